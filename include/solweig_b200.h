@@ -1,0 +1,223 @@
+/*
+ * solweig_b200.h -- C ABI of libsolweig_b200.so, the sm_100a SOLWEIG engine.
+ *
+ * Every entry point takes device pointers that the caller allocated, plain
+ * sizes and a CUDA stream (as void*; NULL = default stream), launches its
+ * kernels on that stream, performs no hidden synchronisation and returns an
+ * int status (SOLWEIG_OK = 0).  On failure solweig_last_error() returns a
+ * message for the calling thread.  Nothing here allocates device memory.
+ *
+ * Raster layout: row-major [rows][cols]; "rows" is axis 0 of the reference's
+ * numpy arrays.  Per-patch visibility is bit-packed: two planes (S, V) of
+ * SOLWEIG_MASK_WORDS uint32 words per pixel, stored plane-major as
+ * masks[(plane * SOLWEIG_MASK_WORDS + word) * pixels + pixel]; bit k of word
+ * w is patch 32*w + k.  S = no building in that direction (the reference's
+ * shmat == 1), V = vegetation seen (vegshmat == 0 or vbshvegshmat == 0).
+ * The four states of a (pixel, patch) pair are then
+ *   sky  = S & ~V,  vegetation = S & V,  building = ~S & ~V,
+ *   building behind vegetation = ~S & V.
+ *
+ * Reference interfaces replaced (paths relative to the reference root):
+ *   solweig_wall_heights      src/walls.py:59-69, src/kernels/geometry.cu:15-34
+ *   solweig_wall_aspect       src/walls.py:83-121, src/kernels/geometry.cu:36-63
+ *   solweig_shadow            src/model.py:689-708 (cast_shadow),
+ *                             src/kernels/geometry.cu:185-253
+ *   solweig_svf               src/svf.py:81-114, src/kernels/geometry.cu:77-159
+ *   solweig_svf_unpack        src/svf.py:113-114 (the three [rows,cols,P] cubes)
+ *   solweig_diffsh            src/svf.py:117-131, src/kernels/geometry.cu:161-172
+ *   solweig_gvf               src/model.py:569-622, src/kernels/gvf.cu:79-292
+ *   solweig_step              src/model.py:15-256 (Solweig_2022a_calc, device part)
+ *   solweig_day               src/series.py:445-491 (the hour loop of _run_day)
+ *   solweig_utci              src/utci.py:6-33, src/kernels/utci.cu
+ */
+#ifndef SOLWEIG_B200_H
+#define SOLWEIG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOLWEIG_OK 0
+#define SOLWEIG_ERR_INVALID 1
+#define SOLWEIG_ERR_CUDA 2
+#define SOLWEIG_ERR_TIMEOUT 3
+
+#define SOLWEIG_MAX_PATCHES 160
+#define SOLWEIG_MASK_WORDS 5
+#define SOLWEIG_MAX_BANDS 8
+#define SOLWEIG_GVF_DIRECTIONS 18
+#define SOLWEIG_GVF_MAX_STEPS 64
+
+/* Static per-scene device arrays (all [rows*cols] unless noted). */
+typedef struct SolweigScene {
+    int32_t rows, cols;
+    double scale;             /* 1 / pixel size */
+    /* geometry, float64 (exact comparisons in the shadow sweep) */
+    const double* dsm;        /* building DSM raised to >= 0 */
+    const double* vegdem;     /* canopy top (0 where no vegetation) */
+    const double* vegdem2;    /* trunk-zone top (0 where none) */
+    const double* walls;      /* wall height, m (0 = no wall) */
+    const double* aspect;     /* wall aspect, radians */
+    const uint8_t* flags;     /* bit0 ground (buildings==1), bit1 bush>1, bit2 water (lc==3) */
+    /* land cover and radiation statics, float32 */
+    const float* alb;         /* ground albedo */
+    const float* emis;        /* ground emissivity */
+    const float* tgk;         /* TgK */
+    const float* tstart;      /* Tstart */
+    const float* tmaxlst;     /* TmaxLST */
+    const float* svfbuveg;    /* svf - (1 - svfveg)(1 - transVeg) */
+    const double* svfalfa;    /* asin(exp(log(1 - max(svf + svfveg - 1, 0)) / 2)) */
+    const double* tan_asvf;   /* tan(acos(sqrt(svf))) */
+    const uint32_t* masks;    /* SOLWEIG_MASK_WORDS * 2 planes, see above */
+    const float* veg_sums;    /* [4][pixels]: sum over V of omega*cos, omega*sin; over
+                                 obstructed (~sky) of omega*cos, omega*sin */
+    const uint8_t* sky_band_counts; /* [nbands][pixels]: sky patches per band */
+    const uint32_t* gvf_face;  /* bit j: wall face turned away from GVF direction j (facesh==0) */
+    /* isotropic / box variants read these directional SVFs (may be NULL otherwise) */
+    const float* svf_dir;     /* [12][pixels]: E,S,W,N x (svf, svfveg, svfaveg) */
+    int32_t patches;          /* number of sky patches (153 for option 2) */
+    int32_t nbands;
+    int32_t landcover;        /* 1 = land-cover maps in use (enables Tg clamp / water) */
+    int32_t has_water;        /* any flags bit2 set */
+    double hmax;              /* max over the raster of dsm, vegdem, vegdem2 */
+} SolweigScene;
+
+/* Per-patch constants of the sky-vault layout (host arrays, copied per call). */
+typedef struct SolweigSkyLayout {
+    int32_t patches, nbands;
+    int32_t band_of_patch[SOLWEIG_MAX_PATCHES];
+    float omega[SOLWEIG_MAX_PATCHES];       /* steradian */
+    float cos_alt[SOLWEIG_MAX_PATCHES];
+    float sin_alt[SOLWEIG_MAX_PATCHES];
+    float band_omega[SOLWEIG_MAX_BANDS];
+    float band_cos[SOLWEIG_MAX_BANDS];
+    float band_sin[SOLWEIG_MAX_BANDS];
+    double sunlit_below[SOLWEIG_MAX_PATCHES]; /* x < t  <=> atan(x)*180/pi < patch altitude */
+    double shaded_above[SOLWEIG_MAX_PATCHES]; /* x > t  <=> atan(x)*180/pi > patch altitude */
+    float cardinal[4][SOLWEIG_MAX_PATCHES];  /* E,S,W,N longwave direction cosines (0 = off) */
+} SolweigSkyLayout;
+
+/* One hour: FP64 host scalars and the device ray table of the sun. */
+typedef struct SolweigHour {
+    int32_t daytime;          /* altitude > 0 */
+    double altitude, azimuth; /* degrees */
+    double zen;               /* radians */
+    double ta, rh, ws;        /* deg C, %, m/s */
+    double rad_g, rad_d, rad_i;
+    double psi;               /* 1 - vegetation transmissivity */
+    double cos_alt, sin_alt;  /* of the solar altitude */
+    double tan_zen;
+    double esky;              /* after the CI < 0.95 blend */
+    double ci_tgg;            /* CI_TgG */
+    double tg_phase;          /* sin(...) factor of Tg for ground (per pixel TmaxLST => see tgk) */
+    double altmax, dectime_frac, snup;
+    double tgwall;            /* wall temperature amplitude after CI scaling and clamp */
+    double twater;
+    int32_t firstdaytime;     /* TsWaveDelay flags */
+    int32_t wave_update;      /* timeadd >= 59/1440 */
+    double wave_weight;       /* exp(-33.27 * timeadd') */
+    /* shadow ray (device arrays, steps entries) */
+    int32_t steps;
+    const int32_t* ray_dxdy;  /* [steps][2] (row offset, col offset) */
+    const double* ray_dz;     /* [steps] */
+    double ray_low, ray_high; int32_t ray_middle;  /* self-shadow azimuth window */
+    /* per-patch hour weights (host arrays) */
+    float lum[SOLWEIG_MAX_PATCHES];      /* Perez luminance lv_k */
+    double yi[SOLWEIG_MAX_PATCHES];      /* min(2 cos(dAzi) tan(alt), 0) */
+    uint8_t lw_sun_test[SOLWEIG_MAX_PATCHES]; /* 90 < dAzi < 270 and daytime */
+    float band_lsky[SOLWEIG_MAX_BANDS];  /* emissivity * SBC * Tk^4 / pi per band */
+    double rad_tot;           /* sum lv * omega * sin(alt) */
+    /* UTCI as a polynomial in (Tmrt - Ta), 7 coefficients (scalar weather) */
+    double utci[7];
+    int32_t utci_valid;       /* 0 -> -999 sentinel */
+} SolweigHour;
+
+/* Output planes of one hour; any pointer may be NULL (not written). */
+typedef struct SolweigOutputs {
+    float* tmrt;
+    float* utci;
+    float* kdown; float* kup; float* ldown; float* lup;
+    float* shadow; float* tg;
+    float* keast; float* ksouth; float* kwest; float* knorth;
+    float* least; float* lsouth; float* lwest; float* lnorth;
+    float* kside_i; float* kside_d; float* kside; float* lside;
+    float* d_rad; float* tg_out;
+} SolweigOutputs;
+
+/* Thermal state carried from hour to hour (6 planes [pixels], float32). */
+typedef struct SolweigState {
+    float* tgmap1; float* tgmap1e; float* tgmap1s; float* tgmap1w; float* tgmap1n;
+    float* tgout1;
+} SolweigState;
+
+const char* solweig_last_error(void);
+int solweig_version(void);
+
+/* Walls ------------------------------------------------------------------ */
+int solweig_wall_heights(const double* dsm, double* walls, int rows, int cols,
+                         double threshold, void* stream);
+/* Best template angle (or -1) and template direction (deg; 0 = unresolved)
+ * for every wall pixel; the gradient fallback for unresolved pixels is done
+ * by the caller on the host.  Templates: line/side1/side2 offset lists
+ * (dr, dc) concatenated over 180 angles, with starts[181] per list. */
+int solweig_wall_aspect(const double* dsm, const double* walls, double* aspect,
+                        int rows, int cols, int radius,
+                        const int32_t* line_off, const int32_t* line_start,
+                        const int32_t* side1_off, const int32_t* side1_start,
+                        const int32_t* side2_off, const int32_t* side2_start,
+                        void* stream);
+
+/* Shadows ---------------------------------------------------------------- */
+/* out: 8 planes [8][pixels] float64 in the reference order
+ * (vegsh, sh, vbshvegsh, wallsh, wallsun, wallshve, facesh, facesun);
+ * vegetation = 0 runs the building-only variant (planes 1,3,4,6,7 valid). */
+int solweig_shadow(const SolweigScene* scene, const int32_t* ray_dxdy, const double* ray_dz,
+                   int steps, double low, double high, int middle, int vegetation,
+                   double* out, void* stream);
+
+/* Sky view factor -------------------------------------------------------- */
+/* Ray tables: per patch p, lengths[p] steps of (dx, dy) and dz in
+ * ray_dxdy[p*capacity + n], ray_dz[p*capacity + n].  Writes the packed masks
+ * (scene-owned buffer) and planes[16][pixels] float64 in the reference's
+ * reduce order (all,E,S,W,N x sh,veg,vb; svftotal). */
+int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
+                const uint8_t* flags, int rows, int cols,
+                int patches, int capacity, const int32_t* ray_dxdy, const double* ray_dz,
+                const int32_t* lengths, double hmax,
+                const SolweigSkyLayout* layout, const double* band_weights /* [nbands][2] */,
+                const uint8_t* sectors /* [patches] bit d: E,S,W,N */,
+                double transmissivity, uint32_t* masks, double* planes,
+                float* veg_sums, uint8_t* sky_band_counts, void* stream);
+/* Expand packed masks to the reference's float cubes [rows][cols][patches]. */
+int solweig_svf_unpack(const uint32_t* masks, int64_t pixels, int patches,
+                       float* shmat, float* vegmat, float* vbmat, void* stream);
+/* diffsh = shmat - (1 - vegshmat)(1 - transmissivity), float32, any layout. */
+int solweig_diffsh(const float* shmat, const float* vegshmat, float* diffsh, int64_t n,
+                   float transmissivity, void* stream);
+
+/* Ground view factor ----------------------------------------------------- */
+/* Planes [17][pixels] float32 in the reference order. */
+int solweig_gvf(const SolweigScene* scene, const float* shadow, const double* wallsun,
+                const float* tg, double tgwall, double ta, double ewall, double albedo_b,
+                double twater, const int32_t* gvf_dxdy /* [18][steps][2] */, int first_steps,
+                int second_steps, float* scratch /* [5][pixels] */, float* planes, void* stream);
+
+/* The hourly step ---------------------------------------------------------- */
+int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                 const SolweigHour* hour, SolweigState* state, const SolweigOutputs* out,
+                 const int32_t* gvf_dxdy, int first_steps, int second_steps,
+                 float* scratch /* [5][pixels] */, void* stream);
+
+/* UTCI ------------------------------------------------------------------- */
+/* Per-pixel weather (any of ta/rh/va may be a 1-element array when its
+ * *_scalar flag is set). */
+int solweig_utci(const float* ta, const float* rh, const float* tmrt, const float* va,
+                 int ta_scalar, int rh_scalar, int va_scalar, float* out, int64_t n,
+                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOLWEIG_B200_H */

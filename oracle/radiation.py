@@ -72,7 +72,7 @@ def _steradians(alt):
     uniq, counts = np.unique(alt, return_counts=True)
     out = np.zeros(alt.size)
     for i in range(alt.size):
-        n = counts[uniq == alt[i]]
+        n = int(counts[uniq == alt[i]][0])
         if n > 1:
             out[i] = ((360 / n) * _D2R) * (np.sin((alt[i] + alt[0]) * _D2R) - np.sin((alt[i] - alt[0]) * _D2R))
         else:

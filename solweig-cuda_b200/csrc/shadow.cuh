@@ -1,0 +1,103 @@
+// The shadow sweep: building and vegetation shadows along one sun ray.
+//
+// For every pixel p and ray step k the reference (src/umep_solweig.py:2201-2406)
+// shifts the DSM / canopy / trunk rasters by the step offset, subtracts the
+// step height dz_k (all float64) and accumulates:
+//   f      = max(dsm_p, max_k(dsm[p+off_k] - dz_k))          building top seen
+//   topmax = max(vegdem_p, max_k(vegdem[p+off_k] - dz_k))    canopy top seen
+//   shadowed_k = f > dsm_p
+//   veg    |= 1 <= #{top-dz_k, bot-dz_k, top-dz_{k-1}, bot-dz_{k-1} > dsm_p} <= 3,
+//             cleared whenever shadowed_k
+//   ever   |= veg
+// Samples outside the raster read as exactly 0 (no dz subtracted).
+//
+// The per-pixel loop below evaluates these recurrences in the same float64
+// operations, so every mask is bit-identical to the reference, and stops early
+// when the remaining steps provably change nothing:
+//   * hmax - dz_{k-1} <= dsm_p   -> no later sample can rise above the pixel
+//     (and, for wall pixels, hmax - dz_k <= topmax so the canopy top is final);
+//     only taken when dsm_p >= 0 (and topmax >= 0), so the zero-valued samples
+//     beyond the raster edge could not change anything either;
+//   * shadowed and not a wall pixel -> every output is final;
+//   * shadowed wall pixel with f - dsm_p >= wall -> wallsun is already 0.
+// Once a sample leaves the raster it never re-enters (the offsets grow
+// monotonically), so the first outside step is applied and the loop ends.
+#pragma once
+#include "common.cuh"
+
+namespace solweig {
+
+struct ShadowResult {
+    double f, topmax;
+    bool shadowed, veg, ever;
+};
+
+// Walk the ray for pixel (r, c).  `is_wall` enables the wall-specific
+// continuation rules; `hmax` = max over the raster of dsm, vegdem and vegdem2.
+__device__ __forceinline__ ShadowResult shadow_walk(
+    const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
+    int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,
+    const int2* __restrict__ ray, const double* __restrict__ dz, int steps, double hmax,
+    bool vegetation) {
+    ShadowResult s;
+    s.f = a;
+    s.topmax = top_p;
+    s.shadowed = false;
+    s.veg = bush;
+    s.ever = false;
+    const bool is_wall = wall > 0.0;
+    double dz_prev = 0.0;
+    int k = 0;
+    for (; k < steps; ++k) {
+        const int2 o = __ldg(&ray[k]);
+        const double dzk = __ldg(&dz[k]);
+        const int rr = r + o.x, cc = c + o.y;
+        if (!in_raster(rr, cc, rows, cols)) break;
+        // Early exits that cannot change any output.
+        if (a >= 0.0 && hmax - dz_prev <= a && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
+            k = steps;  // nothing further can change; no outside fix-up needed
+            break;
+        }
+        const long long q = (long long)rr * cols + cc;
+        const double aq = __ldg(&dsm[q]) - dzk;
+        s.f = fmax(s.f, aq);
+        s.shadowed = s.f > a;
+        if (vegetation) {
+            const double tq = __ldg(&top[q]), bq = __ldg(&bot[q]);
+            s.topmax = fmax(s.topmax, tq - dzk);
+            if (s.shadowed) {
+                s.veg = false;
+            } else {
+                const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
+                              (int)(bq - dz_prev > a);
+                s.veg = s.veg || (n > 0 && n < 4);
+                s.ever = s.ever || s.veg;
+            }
+        }
+        if (s.shadowed && (!is_wall || s.f - a >= wall)) {
+            k = steps;
+            break;
+        }
+        dz_prev = dzk;
+    }
+    if (k < steps) {
+        // First step whose sample is outside the raster: all shifted values are 0.
+        s.f = fmax(s.f, 0.0);
+        s.shadowed = s.f > a;
+        if (vegetation) {
+            s.topmax = fmax(s.topmax, 0.0);
+            if (s.shadowed) s.veg = false;
+            s.ever = s.ever || s.veg;
+        }
+    }
+    return s;
+}
+
+// Self-shadowed wall faces (facesh) for the sun window (low, high, middle).
+__device__ __forceinline__ double self_shadow_face(double aspect, double wallbol, double low,
+                                                   double high, int middle) {
+    return middle ? (double)(aspect < low || aspect >= high) - wallbol + 1.0
+                  : 1.0 - (double)(aspect > low || aspect <= high);
+}
+
+}  // namespace solweig

@@ -1,0 +1,357 @@
+// The hourly SOLWEIG step: two kernels per daytime hour, one per night hour.
+//
+//  K1 step_shadow_kernel   shadow sweep + per-pixel GVF inputs -> float4 quad
+//                          (shadow, Lup, albedo, ground|sunwall bits)
+//  K2 step_radiation_kernel<Day>
+//                          GVF over a shared-memory quad tile, wave delay of
+//                          the thermal state, F_sh, K/L fluxes with the
+//                          anisotropic patch sums, Tmrt and UTCI
+//
+// Per-pixel arithmetic outside the GVF walk and the patch loop is float64
+// (B200 runs FP64 at half the FP32 rate, and it is a few hundred operations
+// per pixel-hour); stored planes are float32.
+#include "gvf.cuh"
+#include "radiation.cuh"
+#include "shadow.cuh"
+
+namespace solweig {
+
+constexpr int kStepBX = 32, kStepBY = 8;
+
+// Ground temperature amplitude wave of the hour (before the water override).
+__device__ __forceinline__ double ground_tg(const SolweigScene& S, const SolweigHour& h,
+                                            long long p) {
+    const double amp = (double)S.tgk[p] * h.altmax + (double)S.tstart[p];
+    const double phase =
+        ((h.dectime_frac - h.snup / 24.0) / ((double)S.tmaxlst[p] / 24.0 - h.snup / 24.0)) * kPi / 2.0;
+    double tg = amp * sin(phase) * h.ci_tgg;
+    if (S.landcover == 1 && tg < 0.0) tg = 0.0;
+    return tg;
+}
+
+__device__ __forceinline__ double lup_excess(double emis, double tg, double shadow, double ta) {
+    return kSBC * emis * pow4(tg * shadow + ta + 273.15) - kSBC * emis * pow4(ta + 273.15);
+}
+
+__global__ void __launch_bounds__(kStepBX* kStepBY) step_shadow_kernel(
+    SolweigScene S, SolweigHour h, float4* __restrict__ quad, float* __restrict__ lup_first) {
+    const int c = blockIdx.x * kStepBX + threadIdx.x;
+    const int r = blockIdx.y * kStepBY + threadIdx.y;
+    if (r >= S.rows || c >= S.cols) return;
+    const long long p = (long long)r * S.cols + c;
+    const double a = S.dsm[p];
+    const double wall = S.walls[p];
+    const uint8_t fl = S.flags[p];
+    const ShadowResult s =
+        shadow_walk(S.dsm, S.vegdem, S.vegdem2, S.rows, S.cols, r, c, a, S.vegdem[p], (fl & 2) != 0,
+                    wall, reinterpret_cast<const int2*>(h.ray_dxdy), h.ray_dz, h.steps, S.hmax, true);
+    // Wall sunlit height (only needed for the sunlit-wall bit of the GVF).
+    const double wallbol = wall > 0.0 ? 1.0 : 0.0;
+    const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);
+    double wallsun = wall - (s.f - a);
+    if (wallsun < 0.0) wallsun = 0.0;
+    if (facesh == 1.0) wallsun = 0.0;
+    const double wallsh = wall - wallsun;
+    double wallshve = (s.topmax - a) * (s.veg ? 1.0 : 0.0) * wallbol - wallsh;
+    if (wallshve < 0.0) wallshve = 0.0;
+    if (wallshve > wall) wallshve = wall;
+    wallsun = wallsun - wallshve;
+    if (wallsun < 0.0) wallsun = 0.0;
+    const double ground = (fl & 1) ? 1.0 : 0.0;
+    const bool sunwall = (wallsun / wall * ground) == 1.0;
+    const double sh = s.shadowed ? 0.0 : 1.0;
+    const double vegsh = s.veg ? 0.0 : 1.0;
+    const double shadow = (double)(float)(sh - (1.0 - vegsh) * (1.0 - h.psi));
+    double tg = ground_tg(S, h, p);
+    const double emis = S.emis[p];
+    if (lup_first) lup_first[p] = (float)lup_excess(emis, tg, shadow, h.ta);
+    if (S.has_water && (fl & 4)) tg = h.twater - h.ta;
+    const float lup = (float)lup_excess(emis, tg, shadow, h.ta);
+    quad[p] = make_float4((float)shadow, lup, S.alb[p],
+                          (float)((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+}
+
+struct StepGvfArgs {
+    const int2* offs;  // [18][second]
+    int first, second, halo;
+};
+
+template <bool Day, bool Cardinal>
+__global__ void __launch_bounds__(kStepBX* kStepBY) step_radiation_kernel(
+    SolweigScene S, SolweigSkyLayout L, SolweigHour h, SolweigState st, SolweigOutputs out,
+    StepGvfArgs ga, const float4* __restrict__ quad, const float* __restrict__ lup_first) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PatchSmem& ps = *reinterpret_cast<PatchSmem*>(smem_raw);
+    int2* offs = reinterpret_cast<int2*>(smem_raw + sizeof(PatchSmem));
+    float4* tile = reinterpret_cast<float4*>(
+        smem_raw + ((sizeof(PatchSmem) + sizeof(int2) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS + 15) & ~size_t(15)));
+    const int H = ga.halo;
+    const int pitch = kStepBX + 2 * H;
+    const int row0 = blockIdx.y * kStepBY - H, col0 = blockIdx.x * kStepBX - H;
+    stage_patches(ps, L, h);
+    if (Day) {
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+        for (int i = tid; i < SOLWEIG_GVF_DIRECTIONS * ga.second; i += blockDim.x * blockDim.y)
+            offs[i] = ga.offs[i];
+        load_quad_tile(tile, pitch, kStepBY + 2 * H, quad, S.rows, S.cols, row0, col0);
+    }
+    __syncthreads();
+    const int c = blockIdx.x * kStepBX + threadIdx.x;
+    const int r = blockIdx.y * kStepBY + threadIdx.y;
+    if (r >= S.rows || c >= S.cols) return;
+    const long long n = (long long)S.rows * S.cols;
+    const long long p = (long long)r * S.cols + c;
+    const uint8_t fl = S.flags[p];
+    const bool ground = fl & 1;
+    const double ta = h.ta;
+    const double tk = ta + 273.15;
+    const double emis = S.emis[p];
+    const double ambient = kSBC * emis * pow4(tk);
+    const double ewall = 0.9, albedo_b = 0.2;
+    const double absK = 0.7, absL = 0.95, Fside = 0.22, Fup = 0.06, Fcyl = 0.28;
+
+    double lup5[5], kup5[5] = {0, 0, 0, 0, 0};
+    double kdown = 0.0, kside = 0.0, kside_i = 0.0, kside_d = 0.0, d_rad = 0.0;
+    double shadow = 0.0, tg = 0.0, tg_out = ta;
+    if (Day) {
+        const float4 own = tile[(threadIdx.y + H) * pitch + threadIdx.x + H];
+        shadow = own.x;
+        GvfScalars gs;
+        gs.lwall = (float)(kSBC * ewall * pow4(h.tgwall + ta + 273.15) - kSBC * ewall * pow4(tk));
+        gs.albedo_b = (float)albedo_b;
+        gs.first = ga.first;
+        gs.second = ga.second;
+        auto sample = [&](int rr, int cc) -> float4 {
+            return tile[(rr - row0) * pitch + (cc - col0)];
+        };
+        auto lfirst = [&](int rr, int cc) -> float {
+            return __ldg(&lup_first[(long long)rr * S.cols + cc]);
+        };
+        const GvfSums g = gvf_walk(sample, lfirst, S.has_water != 0 && lup_first != nullptr, r, c,
+                                   S.rows, S.cols, offs, S.gvf_face[p], own, gs);
+        double gvf_lup[5], gvf_alb[5], gvf_nosh[5];
+        for (int d = 0; d < 5; ++d) {
+            const double div = d == 0 ? 18.0 : 9.0;
+            gvf_lup[d] = (double)g.lup[d] / div + ambient;
+            gvf_alb[d] = (double)g.alb[d] / div;
+            gvf_nosh[d] = (double)g.nosh[d] / div;
+        }
+        // Thermal lag of the upwelling longwave (state: Tgmap1, E, S, W, N).
+        float* state[5] = {st.tgmap1, st.tgmap1e, st.tgmap1s, st.tgmap1w, st.tgmap1n};
+        for (int d = 0; d < 5; ++d) {
+            const double cur = gvf_lup[d];
+            const double prev = h.firstdaytime ? cur : (double)state[d][p];
+            const double delayed = cur * (1.0 - h.wave_weight) + prev * h.wave_weight;
+            lup5[d] = delayed;
+            state[d][p] = (float)(h.wave_update ? delayed : prev);
+        }
+        tg = ground_tg(S, h, p);
+        if (S.has_water && (fl & 4)) tg = h.twater - ta;
+        {
+            const double cur = tg * shadow + ta;
+            const double prev = h.firstdaytime ? cur : (double)st.tgout1[p];
+            const double delayed = cur * (1.0 - h.wave_weight) + prev * h.wave_weight;
+            tg_out = delayed;
+            st.tgout1[p] = (float)(h.wave_update ? delayed : prev);
+        }
+        const double fsh = wedge_fsh(S.svfalfa[p], h.tan_zen);
+        const double svfbuveg = S.svfbuveg[p];
+        const double reflected = albedo_b * (1.0 - svfbuveg) * (h.rad_g * (1.0 - fsh) + h.rad_d * fsh);
+        const double sin_alt = h.sin_alt;
+        const double base_up = h.rad_d * svfbuveg + reflected;
+        for (int d = 0; d < 5; ++d) kup5[d] = gvf_alb[d] * h.rad_i * sin_alt + base_up * gvf_nosh[d];
+        (void)gvf_nosh;
+        uint32_t Sw[SOLWEIG_MASK_WORDS], Vw[SOLWEIG_MASK_WORDS];
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            Sw[w] = S.masks[(long long)w * n + p];
+            Vw[w] = S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + p];
+        }
+        const double tan_asvf = S.tan_asvf[p];
+        const PatchSums pz = patch_loop<Cardinal>(ps, Sw, Vw, tan_asvf, true);
+        const double dsh_veg = 1.0 - (1.0 - 0.03);
+        d_rad = h.rad_d * ((double)pz.lum_sky + dsh_veg * (double)pz.lum_veg);
+        kdown = h.rad_i * shadow * sin_alt + d_rad + reflected;
+        kside_i = shadow * h.rad_i * h.cos_alt;
+        kside_d = (h.rad_d / h.rad_tot) * ((double)pz.cw_sky + dsh_veg * (double)pz.cw_veg);
+        const double sw_shade = (0.2 * h.rad_d * 0.5) / kPi;
+        const double sw_sun = (0.2 * (h.rad_i * h.cos_alt) + h.rad_d * 0.5) / kPi;
+        const double kref_veg = sw_shade * (double)S.veg_sums[p];
+        kside = kside_i + kside_d + sw_sun * (double)pz.sw_sun + sw_shade * (double)pz.sw_shade + kref_veg;
+        // Longwave (daytime)
+        const double lw_shade = (ewall * kSBC * pow4(tk)) / kPi;
+        const double lw_sun = (ewall * kSBC * pow4(ta + h.tgwall + 273.15)) / kPi;
+        double ld_sky = 0.0, ls_sky = 0.0;
+        for (int b = 0; b < L.nbands; ++b) {
+            const double cnt = S.sky_band_counts[(long long)b * n + p];
+            ld_sky += (double)ps.band_down[b] * cnt;
+            ls_sky += (double)ps.band_side[b] * cnt;
+        }
+        const double refl = ((ld_sky + lup5[0]) * (1.0 - ewall) * 0.5) / kPi;
+        const double vc = S.veg_sums[p], vs = S.veg_sums[n + p];
+        const double oc = S.veg_sums[2 * n + p], os = S.veg_sums[3 * n + p];
+        const double ldown = ld_sky + lw_shade * vs + lw_shade * (double)pz.lw_shade_s +
+                             lw_sun * (double)pz.lw_sun_s + refl * os;
+        const double lside = ls_sky + lw_shade * vc + lw_shade * (double)pz.lw_shade_c +
+                             lw_sun * (double)pz.lw_sun_c + refl * oc;
+        // Tmrt (cylinder, anisotropic sky): Keast.. = KupE..*0.5, Least.. = LupE..*0.5
+        const double ksum = 0.5 * (kup5[1] + kup5[2] + kup5[3] + kup5[4]);
+        const double lsum = 0.5 * (lup5[1] + lup5[2] + lup5[3] + lup5[4]);
+        const double sstr = absK * (kside * Fcyl + (kdown + kup5[0]) * Fup + ksum * Fside) +
+                            absL * ((ldown + lup5[0]) * Fup + lside * Fcyl + lsum * Fside);
+        const double tmrt = sqrt(sqrt(sstr / (absL * kSBC))) - 273.2;
+        if (out.tmrt) out.tmrt[p] = (float)tmrt;
+        if (out.utci) out.utci[p] = ground ? utci_eval(h.utci, tmrt, ta, h.utci_valid) : __int_as_float(0x7fc00000);
+        if (out.ldown) out.ldown[p] = (float)ldown;
+        if (out.lside) out.lside[p] = (float)lside;
+        if (Cardinal) {
+            float* card_out[4] = {out.least, out.lsouth, out.lwest, out.lnorth};
+            for (int d = 0; d < 4; ++d)
+                if (card_out[d])
+                    card_out[d][p] = (float)(lup5[d + 1] * 0.5 + (double)pz.card_sky[d] +
+                                             lw_shade * (double)pz.card_veg[d] +
+                                             lw_sun * (double)pz.card_sun[d] +
+                                             lw_shade * (double)pz.card_shade[d] +
+                                             refl * (double)pz.card_obst[d]);
+        } else {
+            float* card_out[4] = {out.least, out.lsouth, out.lwest, out.lnorth};
+            for (int d = 0; d < 4; ++d)
+                if (card_out[d]) card_out[d][p] = (float)(lup5[d + 1] * 0.5);
+        }
+    } else {
+        // Night: no shortwave, Lup from air temperature, state untouched.
+        double lup = kSBC * emis * pow4(ta + 0.0 + 273.15);
+        if (S.landcover == 1 && (fl & 4)) lup = kSBC * 0.98 * pow4(h.twater + 273.15);
+        for (int d = 0; d < 5; ++d) lup5[d] = lup;
+        uint32_t Sw[SOLWEIG_MASK_WORDS], Vw[SOLWEIG_MASK_WORDS];
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            Sw[w] = S.masks[(long long)w * n + p];
+            Vw[w] = S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + p];
+        }
+        const PatchSums pz = patch_loop<Cardinal>(ps, Sw, Vw, S.tan_asvf[p], false);
+        const double lw_shade = (ewall * kSBC * pow4(tk)) / kPi;
+        const double lw_sun = (ewall * kSBC * pow4(ta + 0.0 + 273.15)) / kPi;
+        double ld_sky = 0.0, ls_sky = 0.0;
+        for (int b = 0; b < L.nbands; ++b) {
+            const double cnt = S.sky_band_counts[(long long)b * n + p];
+            ld_sky += (double)ps.band_down[b] * cnt;
+            ls_sky += (double)ps.band_side[b] * cnt;
+        }
+        const double refl = ((ld_sky + lup) * (1.0 - ewall) * 0.5) / kPi;
+        const double vc = S.veg_sums[p], vs = S.veg_sums[n + p];
+        const double oc = S.veg_sums[2 * n + p], os = S.veg_sums[3 * n + p];
+        const double ldown = ld_sky + lw_shade * vs + lw_shade * (double)pz.lw_shade_s + refl * os;
+        const double lside = ls_sky + lw_shade * vc + lw_shade * (double)pz.lw_shade_c + refl * oc;
+        const double lsum = 0.5 * 4.0 * lup;
+        const double sstr = absL * ((ldown + lup) * Fup + lside * Fcyl + lsum * Fside);
+        const double tmrt = sqrt(sqrt(sstr / (absL * kSBC))) - 273.2;
+        if (out.tmrt) out.tmrt[p] = (float)tmrt;
+        if (out.utci) out.utci[p] = ground ? utci_eval(h.utci, tmrt, ta, h.utci_valid) : __int_as_float(0x7fc00000);
+        if (out.ldown) out.ldown[p] = (float)ldown;
+        if (out.lside) out.lside[p] = (float)lside;
+        float* card_out[4] = {out.least, out.lsouth, out.lwest, out.lnorth};
+        for (int d = 0; d < 4; ++d)
+            if (card_out[d])
+                card_out[d][p] = (float)(lup * 0.5 + (Cardinal ? (double)pz.card_sky[d] +
+                                                                     lw_shade * (double)pz.card_veg[d] +
+                                                                     lw_shade * (double)pz.card_shade[d] +
+                                                                     refl * (double)pz.card_obst[d]
+                                                               : 0.0));
+        (void)lw_sun;
+    }
+    if (out.lup) out.lup[p] = (float)lup5[0];
+    if (out.kdown) out.kdown[p] = (float)kdown;
+    if (out.kup) out.kup[p] = (float)kup5[0];
+    if (out.keast) out.keast[p] = (float)(kup5[1] * 0.5);
+    if (out.ksouth) out.ksouth[p] = (float)(kup5[2] * 0.5);
+    if (out.kwest) out.kwest[p] = (float)(kup5[3] * 0.5);
+    if (out.knorth) out.knorth[p] = (float)(kup5[4] * 0.5);
+    if (out.kside_i) out.kside_i[p] = (float)kside_i;
+    if (out.kside_d) out.kside_d[p] = (float)kside_d;
+    if (out.kside) out.kside[p] = (float)kside;
+    if (out.d_rad) out.d_rad[p] = (float)d_rad;
+    if (out.shadow) out.shadow[p] = (float)shadow;
+    if (out.tg) out.tg[p] = (float)tg;
+    if (out.tg_out) out.tg_out[p] = (float)tg_out;
+}
+
+size_t radiation_smem_bytes(int halo) {
+    const size_t head = (sizeof(PatchSmem) + sizeof(int2) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS + 15) & ~size_t(15);
+    return head + sizeof(float4) * (size_t)(kStepBX + 2 * halo) * (kStepBY + 2 * halo);
+}
+
+}  // namespace solweig
+
+using namespace solweig;
+
+static int check_scene(const SolweigScene* S) {
+    SOLWEIG_CHECK_ARG(S, "null scene");
+    SOLWEIG_CHECK_ARG(S->rows > 0 && S->cols > 0 && S->rows < (1 << 20) && S->cols < (1 << 20),
+                      "bad scene shape %dx%d", S->rows, S->cols);
+    SOLWEIG_CHECK_ARG(S->dsm && S->vegdem && S->vegdem2 && S->walls && S->aspect && S->flags &&
+                          S->alb && S->emis && S->tgk && S->tstart && S->tmaxlst && S->svfbuveg &&
+                          S->svfalfa && S->tan_asvf && S->masks && S->veg_sums &&
+                          S->sky_band_counts && S->gvf_face,
+                      "scene has a null array");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                            const SolweigHour* hour, SolweigState* state, const SolweigOutputs* out,
+                            const int32_t* gvf_dxdy, int first_steps, int second_steps,
+                            float* scratch, void* stream) {
+    int rc = check_scene(scene);
+    if (rc) return rc;
+    SOLWEIG_CHECK_ARG(layout && hour && state && out, "solweig_step: null argument");
+    SOLWEIG_CHECK_ARG(layout->patches > 0 && layout->patches <= SOLWEIG_MAX_PATCHES &&
+                          layout->patches == scene->patches,
+                      "solweig_step: layout has %d patches, scene %d", layout->patches, scene->patches);
+    SOLWEIG_CHECK_ARG(state->tgmap1 && state->tgmap1e && state->tgmap1s && state->tgmap1w &&
+                          state->tgmap1n && state->tgout1,
+                      "solweig_step: state has a null plane");
+    const SolweigScene& S = *scene;
+    cudaStream_t st = as_stream(stream);
+    const bool full = out->least || out->lsouth || out->lwest || out->lnorth;
+    dim3 block(kStepBX, kStepBY);
+    dim3 grid(blocks_for(S.cols, kStepBX), blocks_for(S.rows, kStepBY));
+    StepGvfArgs ga{reinterpret_cast<const int2*>(gvf_dxdy), first_steps, second_steps,
+                   second_steps > 0 ? second_steps - 1 : 0};
+    const size_t smem = radiation_smem_bytes(ga.halo);
+    if (hour->daytime) {
+        SOLWEIG_CHECK_ARG(scratch && gvf_dxdy && hour->ray_dxdy && hour->ray_dz,
+                          "solweig_step: daytime needs scratch, GVF offsets and the sun ray");
+        SOLWEIG_CHECK_ARG(second_steps >= 1 && second_steps <= SOLWEIG_GVF_MAX_STEPS &&
+                              first_steps >= 1 && first_steps <= second_steps,
+                          "solweig_step: GVF steps first=%d second=%d", first_steps, second_steps);
+        SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "solweig_step: GVF halo %d too large for shared memory",
+                          ga.halo);
+        float4* quad = reinterpret_cast<float4*>(scratch);
+        float* lup_first = S.has_water ? scratch + 4 * (long long)S.rows * S.cols : nullptr;
+        step_shadow_kernel<<<grid, block, 0, st>>>(S, *hour, quad, lup_first);
+        SOLWEIG_CHECK_LAUNCH("step_shadow_kernel");
+        if (full) {
+            auto k = step_radiation_kernel<true, true>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k<<<grid, block, smem, st>>>(S, *layout, *hour, *state, *out, ga, quad, lup_first);
+        } else {
+            auto k = step_radiation_kernel<true, false>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k<<<grid, block, smem, st>>>(S, *layout, *hour, *state, *out, ga, quad, lup_first);
+        }
+        SOLWEIG_CHECK_LAUNCH("step_radiation_kernel<day>");
+    } else {
+        const size_t smem_night = radiation_smem_bytes(0);
+        if (full) {
+            auto k = step_radiation_kernel<false, true>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_night);
+            k<<<grid, block, smem_night, st>>>(S, *layout, *hour, *state, *out, ga, nullptr, nullptr);
+        } else {
+            auto k = step_radiation_kernel<false, false>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_night);
+            k<<<grid, block, smem_night, st>>>(S, *layout, *hour, *state, *out, ga, nullptr, nullptr);
+        }
+        SOLWEIG_CHECK_LAUNCH("step_radiation_kernel<night>");
+    }
+    return SOLWEIG_OK;
+}

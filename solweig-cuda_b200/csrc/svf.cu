@@ -1,0 +1,250 @@
+// Sky view factor: per-patch visibility rays, bit-packed, and the annulus sums.
+//
+// Visibility (src/kernels/geometry.cu:77-119, src/svf.py:81-106): for every
+// pixel and sky patch the shadow sweep toward the patch centre decides whether
+// a building blocks the patch (S = 0) and whether vegetation was seen in front
+// of the first building hit (V = 1).  The reference stores three float32
+// cubes [rows, cols, 153] (7.3 GB at 2000^2); here each (pixel, patch) keeps
+// 2 bits, 40 bytes per pixel, in the layout described in solweig_b200.h.
+//
+// Reduce (geometry.cu:121-159): annulus-weighted sums over bands and the four
+// half-sky sectors become per-band popcounts of the packed words, summed in
+// the reference's band order so the float64 planes agree to the last bit.
+#include "shadow.cuh"
+
+namespace solweig {
+
+constexpr int kSvfWarps = 8;        // warps per block
+constexpr int kSvfPatchGroup = 32;  // patches per packed word
+
+struct SvfRayParams {
+    int rows, cols, patches, capacity;
+    double hmax;
+};
+
+// grid.x: chunks of 32 consecutive pixels; grid.y: patch word (32 patches).
+__global__ void __launch_bounds__(32 * kSvfWarps) svf_visibility_kernel(
+    const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
+    const uint8_t* __restrict__ flags, SvfRayParams prm, const int2* __restrict__ ray,
+    const double* __restrict__ dz, const int32_t* __restrict__ lengths,
+    uint32_t* __restrict__ masks) {
+    __shared__ uint8_t state[kSvfPatchGroup][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long pixels = (long long)prm.rows * prm.cols;
+    const long long p = (long long)blockIdx.x * 32 + lane;
+    const int word = blockIdx.y;
+    const bool valid = p < pixels;
+    const int r = valid ? (int)(p / prm.cols) : 0, c = valid ? (int)(p % prm.cols) : 0;
+    const double a = valid ? dsm[p] : 0.0;
+    const double top_p = valid ? top[p] : 0.0;
+    const bool bush = valid && (flags[p] & 2);
+    for (int j = warp; j < kSvfPatchGroup; j += kSvfWarps) {
+        const int patch = word * kSvfPatchGroup + j;
+        uint8_t st = 0;
+        if (valid && patch < prm.patches) {
+            const long long base = (long long)patch * prm.capacity;
+            ShadowResult s = shadow_walk(dsm, top, bot, prm.rows, prm.cols, r, c, a, top_p, bush,
+                                         0.0, ray + base, dz + base, lengths[patch], prm.hmax, true);
+            st = (s.shadowed ? 0 : 1) | (s.ever ? 2 : 0);
+        }
+        state[j][lane] = st;
+    }
+    __syncthreads();
+    if (warp < 2 && valid) {
+        uint32_t bits = 0;
+#pragma unroll
+        for (int j = 0; j < kSvfPatchGroup; ++j) bits |= (uint32_t)((state[j][lane] >> warp) & 1u) << j;
+        masks[((long long)warp * SOLWEIG_MASK_WORDS + word) * pixels + p] = bits;
+    }
+}
+
+struct SvfReduceParams {
+    long long pixels;
+    int nbands;
+    double trans;
+    uint32_t band_mask[SOLWEIG_MAX_BANDS][SOLWEIG_MASK_WORDS];
+    uint32_t sector_mask[4][SOLWEIG_MASK_WORDS];
+    double wf[SOLWEIG_MAX_BANDS], wa[SOLWEIG_MAX_BANDS];
+    double w_cos[SOLWEIG_MAX_BANDS], w_sin[SOLWEIG_MAX_BANDS];  // omega*cos, omega*sin per band
+};
+
+__global__ void __launch_bounds__(256) svf_reduce_kernel(const uint32_t* __restrict__ masks,
+                                                         const double* __restrict__ bot,
+                                                         SvfReduceParams prm,
+                                                         double* __restrict__ planes,
+                                                         float* __restrict__ veg_sums,
+                                                         uint8_t* __restrict__ sky_counts) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= prm.pixels) return;
+    const long long n = prm.pixels;
+    uint32_t S[SOLWEIG_MASK_WORDS], V[SOLWEIG_MASK_WORDS];
+#pragma unroll
+    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+        S[w] = masks[(long long)w * n + p];
+        V[w] = masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + p];
+    }
+    double v[15];
+#pragma unroll
+    for (int i = 0; i < 15; ++i) v[i] = 0.0;
+    double vc = 0.0, vs = 0.0, oc = 0.0, os = 0.0;
+    for (int b = 0; b < prm.nbands; ++b) {
+        int cnt[15];
+#pragma unroll
+        for (int i = 0; i < 15; ++i) cnt[i] = 0;
+        int nveg = 0, nobst = 0, nsky = 0;
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            const uint32_t bm = prm.band_mask[b][w];
+            const uint32_t sh = S[w] & bm;                // shmat == 1
+            const uint32_t vg = ~(S[w] & V[w]) & bm;      // vegmat == 1
+            const uint32_t vb = ~(~S[w] & V[w]) & bm;     // vbmat == 1
+            cnt[0] += __popc(sh);
+            cnt[5] += __popc(vg);
+            cnt[10] += __popc(vb);
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                const uint32_t sm = prm.sector_mask[d][w];
+                cnt[1 + d] += __popc(sh & sm);
+                cnt[6 + d] += __popc(vg & sm);
+                cnt[11 + d] += __popc(vb & sm);
+            }
+            nveg += __popc(V[w] & bm);
+            nobst += __popc(~(S[w] & ~V[w]) & bm);
+            nsky += __popc(S[w] & ~V[w] & bm);
+        }
+#pragma unroll
+        for (int g = 0; g < 3; ++g) {
+            v[g * 5] += prm.wf[b] * cnt[g * 5];
+#pragma unroll
+            for (int d = 1; d < 5; ++d) v[g * 5 + d] += prm.wa[b] * cnt[g * 5 + d];
+        }
+        vc += prm.w_cos[b] * nveg;
+        vs += prm.w_sin[b] * nveg;
+        oc += prm.w_cos[b] * nobst;
+        os += prm.w_sin[b] * nobst;
+        sky_counts[(long long)b * n + p] = (uint8_t)nsky;
+    }
+    const double eps = 3.0459e-4;
+    v[2] += eps;
+    v[3] += eps;
+    const double last = bot[p] == 0.0 ? eps : 0.0;
+    v[7] += last;
+    v[8] += last;
+    v[12] += last;
+    v[13] += last;
+#pragma unroll
+    for (int i = 0; i < 15; ++i) {
+        if (v[i] > 1.0) v[i] = 1.0;
+        planes[(long long)i * n + p] = v[i];
+    }
+    planes[15 * n + p] = v[0] - (1.0 - v[5]) * (1.0 - prm.trans);
+    veg_sums[p] = (float)vc;
+    veg_sums[n + p] = (float)vs;
+    veg_sums[2 * n + p] = (float)oc;
+    veg_sums[3 * n + p] = (float)os;
+}
+
+// Packed masks -> the reference's float cubes [pixels][patches].
+__global__ void __launch_bounds__(256) svf_unpack_kernel(const uint32_t* __restrict__ masks,
+                                                         long long pixels, int patches,
+                                                         float* __restrict__ shm,
+                                                         float* __restrict__ vegm,
+                                                         float* __restrict__ vbm) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixels * patches) return;
+    const long long p = i / patches;
+    const int k = (int)(i % patches);
+    const int w = k >> 5, b = k & 31;
+    const bool S = (masks[(long long)w * pixels + p] >> b) & 1u;
+    const bool V = (masks[(long long)(SOLWEIG_MASK_WORDS + w) * pixels + p] >> b) & 1u;
+    if (shm) shm[i] = S ? 1.f : 0.f;
+    if (vegm) vegm[i] = (S && V) ? 0.f : 1.f;
+    if (vbm) vbm[i] = (!S && V) ? 0.f : 1.f;
+}
+
+__global__ void __launch_bounds__(256) diffsh_kernel(const float* __restrict__ sh,
+                                                     const float* __restrict__ veg,
+                                                     float* __restrict__ out, long long n,
+                                                     float trans) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = __fsub_rn(sh[i], __fmul_rn(__fsub_rn(1.0f, veg[i]), __fsub_rn(1.0f, trans)));
+}
+
+}  // namespace solweig
+
+using namespace solweig;
+
+extern "C" int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
+                           const uint8_t* flags, int rows, int cols, int patches, int capacity,
+                           const int32_t* ray_dxdy, const double* ray_dz, const int32_t* lengths,
+                           double hmax, const SolweigSkyLayout* layout,
+                           const double* band_weights, const uint8_t* sectors,
+                           double transmissivity, uint32_t* masks, double* planes,
+                           float* veg_sums, uint8_t* sky_band_counts, void* stream) {
+    SOLWEIG_CHECK_ARG(dsm && vegdem && vegdem2 && flags && ray_dxdy && ray_dz && lengths && layout &&
+                          band_weights && sectors && masks && planes && veg_sums && sky_band_counts,
+                      "solweig_svf: null pointer");
+    SOLWEIG_CHECK_ARG(rows > 0 && cols > 0 && capacity > 0, "solweig_svf: bad shape");
+    SOLWEIG_CHECK_ARG(patches > 0 && patches <= SOLWEIG_MASK_WORDS * 32 && patches == layout->patches,
+                      "solweig_svf: %d patches (max %d, layout %d)", patches,
+                      SOLWEIG_MASK_WORDS * 32, layout->patches);
+    SOLWEIG_CHECK_ARG(layout->nbands > 0 && layout->nbands <= SOLWEIG_MAX_BANDS,
+                      "solweig_svf: bad band count %d", layout->nbands);
+    const long long pixels = (long long)rows * cols;
+    cudaStream_t st = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(masks, 0, sizeof(uint32_t) * 2 * SOLWEIG_MASK_WORDS * pixels, st);
+    if (e != cudaSuccess) {
+        set_error("solweig_svf: memset: %s", cudaGetErrorString(e));
+        return SOLWEIG_ERR_CUDA;
+    }
+    SvfRayParams rp{rows, cols, patches, capacity, hmax};
+    const int words = (patches + 31) / 32;
+    dim3 grid(blocks_for(pixels, 32), words);
+    svf_visibility_kernel<<<grid, 32 * kSvfWarps, 0, st>>>(
+        dsm, vegdem, vegdem2, flags, rp, reinterpret_cast<const int2*>(ray_dxdy), ray_dz, lengths,
+        masks);
+    SOLWEIG_CHECK_LAUNCH("svf_visibility_kernel");
+    SvfReduceParams q{};
+    q.pixels = pixels;
+    q.nbands = layout->nbands;
+    q.trans = transmissivity;
+    for (int k = 0; k < patches; ++k) {
+        const int b = layout->band_of_patch[k];
+        SOLWEIG_CHECK_ARG(b >= 0 && b < layout->nbands, "solweig_svf: bad band of patch %d", k);
+        q.band_mask[b][k >> 5] |= 1u << (k & 31);
+        for (int d = 0; d < 4; ++d)
+            if (sectors[k] & (1u << d)) q.sector_mask[d][k >> 5] |= 1u << (k & 31);
+    }
+    for (int b = 0; b < layout->nbands; ++b) {
+        q.wf[b] = band_weights[2 * b];
+        q.wa[b] = band_weights[2 * b + 1];
+        q.w_cos[b] = (double)layout->band_omega[b] * (double)layout->band_cos[b];
+        q.w_sin[b] = (double)layout->band_omega[b] * (double)layout->band_sin[b];
+    }
+    svf_reduce_kernel<<<blocks_for(pixels, 256), 256, 0, st>>>(masks, vegdem2, q, planes, veg_sums,
+                                                               sky_band_counts);
+    SOLWEIG_CHECK_LAUNCH("svf_reduce_kernel");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_svf_unpack(const uint32_t* masks, int64_t pixels, int patches, float* shmat,
+                                  float* vegmat, float* vbmat, void* stream) {
+    SOLWEIG_CHECK_ARG(masks && pixels > 0 && patches > 0 && patches <= SOLWEIG_MASK_WORDS * 32,
+                      "solweig_svf_unpack: bad arguments");
+    const long long n = (long long)pixels * patches;
+    svf_unpack_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(masks, pixels, patches,
+                                                                         shmat, vegmat, vbmat);
+    SOLWEIG_CHECK_LAUNCH("svf_unpack_kernel");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_diffsh(const float* shmat, const float* vegshmat, float* diffsh, int64_t n,
+                              float transmissivity, void* stream) {
+    SOLWEIG_CHECK_ARG(shmat && vegshmat && diffsh && n >= 0, "solweig_diffsh: bad arguments");
+    if (n == 0) return SOLWEIG_OK;
+    diffsh_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(shmat, vegshmat, diffsh, n,
+                                                                     transmissivity);
+    SOLWEIG_CHECK_LAUNCH("diffsh_kernel");
+    return SOLWEIG_OK;
+}

@@ -1,0 +1,562 @@
+"""Host orchestration of the B200 SOLWEIG engine.
+
+``Scene``      static geometry of one raster tile on the device: walls and
+               aspect, the bit-packed 153-patch visibility, SVF planes and the
+               derived per-pixel statics (``src/series.py:197-382``);
+``hour_plan``  the FP64 host scalars of one forcing hour turned into the
+               ``SolweigHour`` struct (``src/model.py:79-216``);
+``DayRunner``  the hour loop of one calendar day with the thermal state
+               carried on the device (``src/series.py:396-495``).
+
+Device memory is owned by torch tensors; kernels are launched through the C
+ABI on torch's current CUDA stream.  There is no CPU fallback: without the
+CUDA library or a GPU every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import rays
+from . import sky as _sky
+from . import sun as _sun
+
+__all__ = ["Scene", "SkyLayout", "hour_plan", "DayRunner", "LANDCOVER_CLASSES", "CONSTANTS",
+           "stream_handle", "device_ptr"]
+
+SBC = 5.67051e-8
+
+# src/landcoverclasses_2016a.txt: code, albedo, emissivity, TgK, Tstart, TmaxLST
+LANDCOVER_CLASSES = np.array([
+    [2, 0.18, 0.95, 0.58, -9.78, 15.0],
+    [1, 0.18, 0.95, 0.58, -9.78, 15.0],
+    [0, 0.20, 0.95, 0.37, -3.41, 15.0],
+    [7, 0.05, 0.98, 0.00, 0.00, 12.0],
+    [5, 0.16, 0.94, 0.21, -3.38, 14.0],
+    [6, 0.25, 0.94, 0.33, -3.01, 14.0],
+    [99, 0.20, 0.90, 0.58, -3.41, 15.0],
+])
+
+# src/series.py:35-55, :318-325
+CONSTANTS = dict(albedo_b=0.2, albedo_g=0.15, ewall=0.9, eground=0.95, absK=0.7, absL=0.95,
+                 Fside=0.22, Fup=0.06, Fcyl=0.28, transVeg=0.03, firstdayleaf=97, lastdayleaf=300,
+                 elvis=0.0)
+
+
+def stream_handle(stream=None):
+    s = torch.cuda.current_stream() if stream is None else stream
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def device_ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("solweig_cuda_b200 needs a CUDA device (sm_100a); none is available")
+
+
+class SkyLayout:
+    """Host + ABI view of one sky-vault layout (``patch_option``)."""
+
+    def __init__(self, patch_option=2):
+        L = _sky.patch_layout(patch_option)
+        self.host = L
+        s = _lib.SolweigSkyLayout()
+        s.patches = L.count
+        s.nbands = L.band_counts.size
+        if L.count > _lib.MAX_PATCHES or s.nbands > _lib.MAX_BANDS:
+            raise ValueError(f"patch_option {patch_option}: {L.count} patches / {s.nbands} bands "
+                             f"exceed the library limits")
+        for k in range(L.count):
+            s.band_of_patch[k] = int(L.band_of_patch[k])
+            s.omega[k] = L.steradian[k]
+            s.cos_alt[k] = L.cos_alt[k]
+            s.sin_alt[k] = L.sin_alt[k]
+            s.sunlit_below[k] = L.sunlit_below[k]
+            s.shaded_above[k] = L.shaded_above[k]
+            for d in range(4):
+                s.cardinal[d][k] = L.cardinal[k, d]
+        self.band_omega = np.zeros(s.nbands)
+        for b in range(s.nbands):
+            k = int(L.band_offsets[b])
+            s.band_omega[b] = L.steradian[k]
+            s.band_cos[b] = L.cos_alt[k]
+            s.band_sin[b] = L.sin_alt[k]
+            self.band_omega[b] = L.steradian[k]
+        self.struct = s
+        # SVF annulus weights and sector bits (src/svf.py:36-46)
+        azimuth, altitude, counts = rays.svf_patch_directions(patch_option)
+        edges = (0, 12, 24, 36, 48, 60, 72, 84, 90)
+        w = np.zeros((len(counts), 2))
+        for b, n in enumerate(counts):
+            for k in np.arange(edges[b] + 1, edges[b + 1] + 1):
+                ring = 91. - k
+                x = (1. / (2. * np.pi)) * np.sin(np.pi / 180.) * np.sin((np.pi * (2. * ring - 1.)) / 180.)
+                w[b, 0] += ((360. / n) * (np.pi / 180.)) * x
+                w[b, 1] += ((360. / np.ceil(n / 2.)) * (np.pi / 180.)) * x
+        self.band_weights = np.ascontiguousarray(w)
+        sec = ((azimuth >= 0) & (azimuth < 180)).astype(np.uint8)
+        sec |= (((azimuth >= 90) & (azimuth < 270)).astype(np.uint8) << 1)
+        sec |= (((azimuth >= 180) & (azimuth < 360)).astype(np.uint8) << 2)
+        sec |= (((azimuth >= 270) | (azimuth < 90)).astype(np.uint8) << 3)
+        self.sectors = np.ascontiguousarray(sec)
+
+
+def _upload(arr, dtype, device):
+    return torch.from_numpy(np.ascontiguousarray(arr, dtype=dtype)).to(device, non_blocking=False)
+
+
+def _aspect_templates(pixel_size):
+    """Flattened template offset lists for ``solweig_wall_aspect`` (``src/walls.py:24-56``)."""
+    from scipy.ndimage import rotate
+    size = int(np.floor((1.0 / pixel_size + 1e-10) * 9))
+    if size <= 2:
+        size = 3
+    elif size != 9 and size % 2 == 0:
+        size += 1
+    radius = size // 2
+    line = np.zeros((size, size))
+    line[:, radius] = 1
+    sides = np.zeros((size, size))
+    sides[radius, :radius] = 1
+    sides[radius, radius + 1:] = 2
+    lists = ([], [], [])
+    for angle in range(180):
+        rl = np.round(rotate(line, angle, order=1, reshape=False, mode="nearest"))
+        rs = np.round(rotate(sides, angle, order=0, reshape=False, mode="nearest"))
+        if angle in (150, 30):
+            rs[:, size - 1] = 0
+        if 270 - angle == 225:
+            rl[0, 0] = rl[size - 1, size - 1] = 1
+        if 270 - angle == 135:
+            rl[0, size - 1] = rl[size - 1, 0] = 1
+        for lst, m in zip(lists, (rl != 0, rs == 1, rs == 2)):
+            lst.append(np.argwhere(m).astype(np.int32) - radius)
+    packed = []
+    for lst in lists:
+        starts = np.concatenate(([0], np.cumsum([a.shape[0] for a in lst]))).astype(np.int32)
+        offs = np.concatenate(lst).astype(np.int32).reshape(-1, 2)
+        packed.append((np.ascontiguousarray(offs), starts))
+    return radius, size, packed
+
+
+_TEMPLATE_CACHE = {}
+
+
+def wall_heights_device(dsm_dev, threshold, stream=None):
+    rows, cols = dsm_dev.shape
+    walls = torch.empty_like(dsm_dev)
+    _lib.check(_lib.lib().solweig_wall_heights(device_ptr(dsm_dev), device_ptr(walls), rows, cols,
+                                                float(threshold), stream_handle(stream)),
+               "solweig_wall_heights")
+    return walls
+
+
+def wall_aspect(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
+    """Wall aspect (degrees, float64 host array), ``src/walls.py:83-129``."""
+    rows, cols = dsm_host.shape
+    key = float(pixel_size)
+    if key not in _TEMPLATE_CACHE:
+        _TEMPLATE_CACHE[key] = _aspect_templates(pixel_size)
+    radius, size, packed = _TEMPLATE_CACHE[key]
+    walls = walls_dev.cpu().numpy()
+    mask = walls > 0
+    aspect = np.zeros((rows, cols))
+    if not mask.any():
+        return aspect, walls
+    if rows > 2 * radius + 2 and cols > 2 * radius + 2:
+        dev = dsm_dev.device
+        t = [(_upload(o, np.int32, dev), _upload(s, np.int32, dev)) for o, s in packed]
+        out = torch.empty_like(dsm_dev)
+        _lib.check(_lib.lib().solweig_wall_aspect(
+            device_ptr(dsm_dev), device_ptr(walls_dev), device_ptr(out), rows, cols, radius,
+            device_ptr(t[0][0]), device_ptr(t[0][1]), device_ptr(t[1][0]), device_ptr(t[1][1]),
+            device_ptr(t[2][0]), device_ptr(t[2][1]), stream_handle(stream)), "solweig_wall_aspect")
+        aspect = out.cpu().numpy()
+    unresolved = np.flatnonzero(mask & (aspect == 0))
+    if unresolved.size:
+        aspect.ravel()[unresolved] += _gradient_aspect(dsm_host, pixel_size, unresolved)
+    return aspect, walls
+
+
+def _gradient_aspect(dsm, pixel_size, flat_idx):
+    """``-arctan2(fx, fy)`` in degrees at selected pixels, numpy.gradient semantics."""
+    rows, cols = dsm.shape
+    step = 1.0 / (1.0 / pixel_size)
+    r, c = np.divmod(flat_idx, cols)
+
+    def grad(axis_len, idx, get):
+        out = np.empty(idx.size)
+        if axis_len < 2:
+            out[:] = 0.0
+            return out
+        inner = (idx > 0) & (idx < axis_len - 1)
+        lo = idx == 0
+        hi = idx == axis_len - 1
+        out[inner] = (get(idx[inner] + 1, inner) - get(idx[inner] - 1, inner)) / (2. * step)
+        out[lo] = (get(idx[lo] + 1, lo) - get(idx[lo], lo)) / step
+        out[hi] = (get(idx[hi], hi) - get(idx[hi] - 1, hi)) / step
+        return out
+
+    fy = grad(rows, r, lambda ri, sel: dsm[ri, c[sel]])
+    fx = grad(cols, c, lambda ci, sel: dsm[r[sel], ci])
+    g = -np.arctan2(fx, fy)
+    g[g < 0] += 2 * np.pi
+    return 1 * (g / (math.pi / 180.0))
+
+
+class Scene:
+    """Static geometry and per-pixel statics of one tile, resident on the device."""
+
+    def __init__(self, dsm, trees, dem, pixel_size=1.0, landcover=None, wall_threshold=3.0,
+                 patch_option=2, device="cuda", walls=None, aspect=None, stream=None,
+                 keep_planes=False):
+        _require_cuda()
+        dsm = np.asarray(dsm, dtype=np.float64)
+        trees = np.asarray(trees, dtype=np.float64)
+        dem = np.asarray(dem, dtype=np.float64)
+        if dsm.ndim != 2 or dsm.shape != trees.shape or dsm.shape != dem.shape:
+            raise ValueError("dsm, trees and dem must be 2-D arrays of the same shape")
+        if landcover is not None and np.shape(landcover) != dsm.shape:
+            raise ValueError("landcover must have the raster's shape")
+        self.device = torch.device(device)
+        self.shape = dsm.shape
+        self.rows, self.cols = dsm.shape
+        self.pixels = dsm.size
+        self.pixel_size = float(pixel_size)
+        self.scale = 1 / self.pixel_size
+        self.layout = SkyLayout(patch_option)
+        self.patch_option = int(patch_option)
+        L = _lib.lib()
+        st = stream_handle(stream)
+        dev = self.device
+        n = self.pixels
+        dsm_in = _upload(dsm, np.float64, dev)
+        # Walls from the unraised DSM, rounded through float32 (src/series.py:213-236).
+        if walls is None:
+            walls_dev = wall_heights_device(dsm_in, wall_threshold, stream)
+            aspect, walls = wall_aspect(dsm, dsm_in, walls_dev, pixel_size, stream)
+        walls = np.asarray(walls, dtype=np.float64).astype(np.float32).astype(np.float64)
+        aspect = np.asarray(aspect, dtype=np.float64).astype(np.float32).astype(np.float64)
+        self.walls_host = walls
+        self.aspect_host = aspect
+        self.walls = _upload(walls, np.float64, dev)
+        self.aspect = _upload(aspect * np.pi / 180., np.float64, dev)
+        # Raise / clip semantics of src/series.py:252-291, computed on the host copy.
+        raise_dsm = max(0.0, -float(dsm.min()))
+        raise_dem = max(0.0, -float(dem.min()))
+        a = dsm + raise_dsm if raise_dsm else dsm
+        t1 = np.where(trees < 0., 0., trees)
+        self.amaxvalue = float(max(a.max() - a.min(), t1.max()))
+        self.dsm_max = float(a.max())
+        self.hmax = float(a.max() + max(t1.max(), 0.0))
+        trees_in = _upload(trees, np.float64, dev)
+        dem_in = _upload(dem, np.float64, dev)
+        lc_in = _upload(landcover, np.float64, dev) if landcover is not None else None
+        self.landcover = 1 if landcover is not None else 0
+        f64 = dict(dtype=torch.float64, device=dev)
+        f32 = dict(dtype=torch.float32, device=dev)
+        self.dsm = torch.empty(self.shape, **f64)
+        self.vegdem = torch.empty(self.shape, **f64)
+        self.vegdem2 = torch.empty(self.shape, **f64)
+        self.flags = torch.empty(self.shape, dtype=torch.uint8, device=dev)
+        self.alb = torch.empty(self.shape, **f32)
+        self.emis = torch.empty(self.shape, **f32)
+        self.tgk = torch.empty(self.shape, **f32)
+        self.tstart = torch.empty(self.shape, **f32)
+        self.tmaxlst = torch.empty(self.shape, **f32)
+        self.lc_grid = torch.empty(self.shape, **f32)
+        classes = np.ascontiguousarray(LANDCOVER_CLASSES, dtype=np.float64)
+        defaults = np.array([CONSTANTS["albedo_g"], CONSTANTS["eground"], 0.37, -3.41, 15.0])
+        _lib.check(L.solweig_scene_build(
+            device_ptr(dsm_in), device_ptr(trees_in), device_ptr(dem_in), device_ptr(lc_in), n,
+            raise_dsm, raise_dem, classes.ctypes.data_as(ctypes.c_void_p), classes.shape[0],
+            defaults.ctypes.data_as(ctypes.c_void_p), device_ptr(self.dsm), device_ptr(self.vegdem),
+            device_ptr(self.vegdem2), device_ptr(self.flags), device_ptr(self.alb),
+            device_ptr(self.emis), device_ptr(self.tgk), device_ptr(self.tstart),
+            device_ptr(self.tmaxlst), device_ptr(self.lc_grid), st), "solweig_scene_build")
+        if landcover is not None:
+            wall_row = LANDCOVER_CLASSES[LANDCOVER_CLASSES[:, 0] == 99][0]
+            self.tgk_wall, self.tstart_wall, self.tmaxlst_wall = (float(wall_row[3]),
+                                                                  float(wall_row[4]),
+                                                                  float(wall_row[5]))
+        else:
+            self.tgk_wall, self.tstart_wall, self.tmaxlst_wall = 0.37, -3.41, 15.
+        del dsm_in, trees_in, dem_in, lc_in
+        self.has_water = int(bool(((self.flags & 4) != 0).any().item())) if landcover is not None else 0
+        # Sky view factor: bit-packed visibility + the 16 reduce planes.
+        dxdy, dz, lengths, cap = rays.svf_rays(patch_option, self.shape, self.amaxvalue, self.scale)
+        self.svf_steps = int(lengths.sum())
+        t_dxdy = _upload(dxdy, np.int32, dev)
+        t_dz = _upload(dz, np.float64, dev)
+        t_len = _upload(lengths, np.int32, dev)
+        nb = self.layout.struct.nbands
+        self.masks = torch.empty((2 * _lib.MASK_WORDS, self.rows, self.cols), dtype=torch.int32,
+                                 device=dev)
+        planes = torch.empty((16, self.rows, self.cols), **f64)
+        self.veg_sums = torch.empty((4, self.rows, self.cols), **f32)
+        self.sky_band_counts = torch.empty((nb, self.rows, self.cols), dtype=torch.uint8, device=dev)
+        lay = self.layout
+        _lib.check(L.solweig_svf(
+            device_ptr(self.dsm), device_ptr(self.vegdem), device_ptr(self.vegdem2),
+            device_ptr(self.flags), self.rows, self.cols, lay.struct.patches, cap,
+            device_ptr(t_dxdy), device_ptr(t_dz), device_ptr(t_len), self.hmax,
+            ctypes.byref(lay.struct), lay.band_weights.ctypes.data_as(ctypes.c_void_p),
+            lay.sectors.ctypes.data_as(ctypes.c_void_p), CONSTANTS["transVeg"],
+            device_ptr(self.masks), device_ptr(planes), device_ptr(self.veg_sums),
+            device_ptr(self.sky_band_counts), st), "solweig_svf")
+        del t_dxdy, t_dz, t_len
+        # Derived statics after the float32 round trip of the SVF planes.
+        self.svf32 = torch.empty((15, self.rows, self.cols), **f32)
+        self.svfbuveg = torch.empty(self.shape, **f32)
+        self.svfalfa = torch.empty(self.shape, **f64)
+        self.tan_asvf = torch.empty(self.shape, **f64)
+        self.gvf_face = torch.empty(self.shape, dtype=torch.int32, device=dev)
+        lo, hi, mid = rays.gvf_face_windows()
+        _lib.check(L.solweig_scene_finalize(
+            device_ptr(planes), device_ptr(self.walls), device_ptr(self.aspect), n,
+            CONSTANTS["transVeg"], lo.ctypes.data_as(ctypes.c_void_p),
+            hi.ctypes.data_as(ctypes.c_void_p), mid.ctypes.data_as(ctypes.c_void_p),
+            device_ptr(self.svf32), device_ptr(self.svfbuveg), device_ptr(self.svfalfa),
+            device_ptr(self.tan_asvf), device_ptr(self.gvf_face), st), "solweig_scene_finalize")
+        self.planes = planes if keep_planes else None
+        self.gvf_dxdy_host, self.first_steps, self.second_steps = rays.gvf_offsets(self.scale)
+        self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
+        self.struct = self._make_struct()
+
+    def _make_struct(self):
+        s = _lib.SolweigScene()
+        s.rows, s.cols, s.scale = self.rows, self.cols, self.scale
+        for name in ("dsm", "vegdem", "vegdem2", "walls", "aspect", "flags", "alb", "emis", "tgk",
+                     "tstart", "tmaxlst", "svfbuveg", "svfalfa", "tan_asvf", "masks", "veg_sums",
+                     "sky_band_counts", "gvf_face"):
+            setattr(s, name, getattr(self, name).data_ptr())
+        s.svf_dir = None
+        s.patches = self.layout.struct.patches
+        s.nbands = self.layout.struct.nbands
+        s.landcover = self.landcover
+        s.has_water = self.has_water
+        s.hmax = self.hmax
+        return s
+
+    # The 15 SVF planes in the reference's svf_calculator order, float32-rounded.
+    SVF_ORDER = ("svf", "svfE", "svfS", "svfW", "svfN", "svfveg", "svfEveg", "svfSveg", "svfWveg",
+                 "svfNveg", "svfaveg", "svfEaveg", "svfSaveg", "svfWaveg", "svfNaveg")
+
+    def svf_plane(self, name):
+        return self.svf32[self.SVF_ORDER.index(name)]
+
+
+def _leaf_psi(doy):
+    first, last = CONSTANTS["firstdayleaf"], CONSTANTS["lastdayleaf"]
+    if first > last:
+        leaf = (doy > first) | (doy < last)
+    else:
+        leaf = (doy > first) & (doy < last)
+    return 3. / 100. if leaf else .5
+
+
+@dataclass
+class HourScalars:
+    """Host-side FP64 results of one hour that the step also returns."""
+    ea: float
+    esky: float
+    I0: float
+    CI: float
+    radI: float
+    radD: float
+    CI_Tg: float
+    CI_TgG: float
+    Tgwall: float
+    lv: object
+
+
+def hour_plan(scene, latitude, altitude, azimuth, zen, jday, dectime, altmax, ta, rh, rad_g, rad_d,
+              rad_i, p_kpa, ws, psi, ci_prev, firstdaytime, timeadd, timestepdec, twater):
+    """FP64 host scalars of one hour (``src/umep_solweig.py:122-232``).
+
+    Returns ``(SolweigHour, ShadowRay or None, HourScalars, next_state)`` where
+    next_state = (firstdaytime, timeadd, CI).
+    """
+    L = scene.layout.host
+    h = _lib.SolweigHour()
+    _, _, _, snup = _sun.daylen(jday, latitude)
+    ea = 6.107 * 10 ** ((7.5 * ta) / (237.3 + ta)) * (rh / 100.)
+    msteg = 46.5 * (ea / (ta + 273.15))
+    esky = (1 - (1 + msteg) * np.exp(-((1.2 + 3.0 * msteg) ** 0.5))) + CONSTANTS["elvis"]
+    day = altitude > 0
+    CI = ci_prev
+    ray = None
+    lv = None
+    I0 = 0
+    CI_Tg = CI_TgG = None
+    tgwall = 0.0
+    if day:
+        I0, CI, Kt, _, _ = _sun.clearness_index(zen, jday, ta, rh / 100., rad_g, latitude, p_kpa)
+        if CI > 1 or CI == np.inf:
+            CI = 1
+        rad_i, rad_d = _sun.diffuse_fraction(rad_g, altitude, Kt, ta, rh)
+        lv = _sky.perez(zen * (180 / np.pi), azimuth, rad_d, rad_i, jday, L)
+        tgamp_wall = scene.tgk_wall * altmax + scene.tstart_wall
+        frac = dectime - np.floor(dectime)
+        tgwall = tgamp_wall * np.sin((((frac) - snup / 24) / (scene.tmaxlst_wall / 24 - snup / 24)) * np.pi / 2)
+        if tgwall < 0:
+            tgwall = 0
+        radI0, radD0 = _sun.diffuse_fraction(I0, altitude, 1., ta, rh)
+        corr = 0.1473 * np.log(90 - (zen / np.pi * 180)) + 0.3454
+        CI_Tg = (rad_g / radI0) + (1 - corr)
+        if CI_Tg > 1 or CI_Tg == np.inf:
+            CI_Tg = 1
+        radG0 = radI0 * (np.sin(altitude * (np.pi / 180))) + radD0
+        CI_TgG = (rad_g / radG0) + (1 - corr)
+        if CI_TgG > 1 or CI_TgG == np.inf:
+            CI_TgG = 1
+        tgwall = tgwall * CI_TgG
+        ray = rays.shadow_ray(azimuth, altitude, scene.scale, scene.amaxvalue, scene.shape, True)
+        # wave delay flags (all six TsWaveDelay calls share them)
+        if timeadd >= (59 / 1440):
+            weight = math.exp(-33.27 * timeadd)
+            update = 1
+            next_timeadd = timestepdec if timestepdec > (59 / 1440) else 0
+        else:
+            next_timeadd = timeadd + timestepdec
+            weight = math.exp(-33.27 * next_timeadd)
+            update = 0
+        h.firstdaytime = int(firstdaytime)
+        h.wave_update = update
+        h.wave_weight = weight
+        next_state = (0, next_timeadd, CI)
+    else:
+        CI_Tg = CI_TgG = CI
+        next_state = (1, 0, CI)
+    if CI < 0.95:
+        esky = CI * esky + (1 - CI) * 1.
+    h.daytime = int(day)
+    h.altitude, h.azimuth, h.zen = altitude, azimuth, zen
+    h.ta, h.rh, h.ws = ta, rh, ws
+    h.rad_g, h.rad_d, h.rad_i = rad_g, rad_d, rad_i
+    h.psi = psi
+    h.cos_alt = np.cos(altitude * (np.pi / 180))
+    h.sin_alt = np.sin(altitude * (np.pi / 180))
+    h.tan_zen = np.tan(zen)
+    h.esky = esky
+    h.ci_tgg = CI_TgG if day else 0.0
+    h.altmax = altmax
+    h.dectime_frac = dectime - math.floor(dectime)
+    h.snup = snup
+    h.tgwall = tgwall
+    h.twater = twater if twater is not None else 0.0
+    if ray is not None:
+        h.steps = ray.steps
+        h.ray_low, h.ray_high, h.ray_middle = ray.low, ray.high, ray.middle
+    # per-patch weights
+    band_e = _sky.band_emissivity(esky, L)
+    base = SBC * ((ta + 273.15) ** 4)
+    for b in range(L.band_counts.size):
+        k = int(L.band_offsets[b])
+        h.band_lsky[b] = (band_e[k] * base) / np.pi
+    if day:
+        lum = lv[:, 2]
+        rad_tot = 0.0
+        for k in range(L.count):
+            rad_tot += lum[k] * L.steradian[k] * np.sin(L.altitude[k] * (np.pi / 180))
+        h.rad_tot = float(np.asarray(rad_tot).item())
+        tan_alt = np.tan(altitude * (np.pi / 180))
+        for k in range(L.count):
+            h.lum[k] = lum[k]
+            diff = np.abs(azimuth - L.azimuth[k])
+            yi = 2 * np.cos(diff * (np.pi / 180)) * tan_alt
+            h.yi[k] = 0.0 if yi > 0 else yi
+            h.lw_sun_test[k] = 1 if (90 < diff < 270) else 0
+    else:
+        h.rad_tot = 1.0
+    coef = (ctypes.c_double * 7)()
+    _lib.check(_lib.lib().solweig_utci_collapse(float(np.float32(ta)), float(np.float32(rh)),
+                                                float(np.float32(ws)), coef), "solweig_utci_collapse")
+    for i in range(7):
+        h.utci[i] = coef[i]
+    h.utci_valid = int(not (np.float32(ta) <= -999 or np.float32(rh) <= -999 or np.float32(ws) <= -999))
+    scal = HourScalars(ea=ea, esky=esky, I0=I0, CI=CI, radI=rad_i, radD=rad_d, CI_Tg=CI_Tg,
+                       CI_TgG=CI_TgG, Tgwall=tgwall, lv=lv)
+    return h, ray, scal, next_state
+
+
+STEP_OUTPUTS = ("tmrt", "utci", "kdown", "kup", "ldown", "lup", "shadow", "tg", "keast", "ksouth",
+                "kwest", "knorth", "least", "lsouth", "lwest", "lnorth", "kside_i", "kside_d",
+                "kside", "lside", "d_rad", "tg_out")
+
+
+class DayRunner:
+    """Hour loop of one day (plain form: one host plan + kernel pair per hour)."""
+
+    def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0):
+        self.scene = scene
+        self.latitude, self.longitude, self.site_altitude, self.utc = latitude, longitude, site_altitude, utc
+        dev = scene.device
+        shape = scene.shape
+        self.state = {k: torch.zeros(shape, dtype=torch.float32, device=dev) for k in _lib.STATE_FIELDS}
+        self.scratch = torch.empty((5, scene.rows, scene.cols), dtype=torch.float32, device=dev)
+
+    def state_struct(self):
+        s = _lib.SolweigState()
+        for k in _lib.STATE_FIELDS:
+            setattr(s, k, self.state[k].data_ptr())
+        return s
+
+    def reset_state(self):
+        for t in self.state.values():
+            t.zero_()
+
+    def step(self, hour, ray, outputs, stream=None):
+        """Launch one hour.  ``outputs`` maps ABI output names to float32 device tensors."""
+        sc = self.scene
+        ray_t = None
+        if ray is not None:
+            ray_t = (_upload(ray.dxdy, np.int32, sc.device), _upload(ray.dz, np.float64, sc.device))
+            hour.ray_dxdy = ray_t[0].data_ptr()
+            hour.ray_dz = ray_t[1].data_ptr()
+        out = _lib.SolweigOutputs()
+        for k, t in outputs.items():
+            setattr(out, k, t.data_ptr())
+        st = self.state_struct()
+        _lib.check(_lib.lib().solweig_step(
+            ctypes.byref(sc.struct), ctypes.byref(sc.layout.struct), ctypes.byref(hour),
+            ctypes.byref(st), ctypes.byref(out), device_ptr(sc.gvf_dxdy), sc.first_steps,
+            sc.second_steps, device_ptr(self.scratch), stream_handle(stream)), "solweig_step")
+        return ray_t  # keep the ray tensors alive until the caller syncs
+
+    def run_day(self, met, outputs=("tmrt", "utci"), hours=None, stream=None):
+        """Run the rows of one calendar day; returns {name: tensor [H, rows, cols]}."""
+        met = np.asarray(met, dtype=np.float64)
+        sol = _sun.metdata(met, self.latitude, self.longitude, self.site_altitude, self.utc)
+        dectime = sol.dectime
+        timestepdec = (dectime[1] - dectime[0]) if len(met) > 1 else 1 / 24.
+        twater = float(np.mean(met[:, 11])) if self.scene.landcover else None
+        idx = list(range(len(met))) if hours is None else list(hours)
+        res = {k: torch.empty((len(idx),) + self.scene.shape, dtype=torch.float32,
+                              device=self.scene.device) for k in outputs}
+        self.reset_state()
+        firstdaytime, timeadd, CI = 1, 0.0, 1.0
+        keep = []
+        scalars = []
+        for j, i in enumerate(idx):
+            if dectime[i] - np.floor(dectime[i]) == 0:
+                CI = 1.
+            psi = _leaf_psi(met[i, 1])
+            h, ray, scal, (firstdaytime, timeadd, CI) = hour_plan(
+                self.scene, self.latitude, sol.altitude[i], sol.azimuth[i], sol.zen[i], sol.jday[i],
+                dectime[i], sol.altmax[i], met[i, 11], met[i, 10], met[i, 14], met[i, 21],
+                met[i, 22], met[i, 12], met[i, 9], psi, CI, firstdaytime, timeadd, timestepdec,
+                twater)
+            keep.append(self.step(h, ray, {k: res[k][j] for k in outputs}, stream))
+            scalars.append(scal)
+        self.last_scalars = scalars
+        self._keep = keep
+        return res

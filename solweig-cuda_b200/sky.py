@@ -78,7 +78,7 @@ class PatchLayout:
         uniq, uniq_counts = np.unique(alt, return_counts=True)
         omega = np.zeros(alt.size)
         for i in range(alt.size):
-            n = uniq_counts[uniq == alt[i]]
+            n = int(uniq_counts[uniq == alt[i]][0])
             if n > 1:
                 omega[i] = ((360 / n) * _D2R) * (np.sin((alt[i] + alt[0]) * _D2R)
                                                   - np.sin((alt[i] - alt[0]) * _D2R))
