@@ -1,0 +1,329 @@
+"""Benchmark: pixel-hours/s of Tmrt + UTCI on a seeded 2000 x 2000 scene (1 m).
+
+One step = one calendar day (24 hourly steps: shadow sweep, ground view
+factors, anisotropic K/L fluxes, Tmrt, UTCI) over the whole raster, with the
+static geometry (walls, 153-patch SVF) prepared once before timing.  The
+timed number is the chosen form (``--form``); the plain form is timed beside
+it.  ``e2e`` is the same metric through the public API from host rasters:
+rasters uploaded, walls + SVF prepared, the day computed and every hour's
+Tmrt and UTCI copied back to host memory.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl solweig|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs its own day of the
+same tile (days are independent: the thermal state resets daily), so the
+work per GPU is fixed ("weak" scaling) and there is no data-path collective.
+``--impl reference`` times the float64 CPU port of the reference path on the
+host cores (a process pool over independent tiles) and prints its own line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "pixel-hours/s Tmrt+UTCI at 2000² px: chosen vs plain form on 1 B200 at ≤0.1 K"
+UNIT = "pixel-hours/s"
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("solweig", "reference"), default="solweig")
+    p.add_argument("--size", type=int, default=2000)
+    p.add_argument("--form", choices=("plain", "batched"), default="batched")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# CPU reference arm: the float64 port of the reference path on host cores
+# ----------------------------------------------------------------------------
+
+CPU_TILE = 96
+
+
+def _cpu_tile(seed):
+    import numpy as np
+    from oracle import step as ST
+    from solweig_cuda_b200 import synthetic
+    sc = synthetic.make_scene(CPU_TILE, seed=seed)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    t0 = time.perf_counter()
+    s = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    ST.run_day(s, met, dict(latitude=53.0, longitude=0.0, altitude=3.0), 0.0)
+    return CPU_TILE * CPU_TILE * 24, time.perf_counter() - t0, float(np.float64(0))
+
+
+def cpu_port_throughput(workers, tiles):
+    """pixel-hours/s of the oracle port over ``tiles`` independent tiles on ``workers`` processes."""
+    import multiprocessing as mp
+    t0 = time.perf_counter()
+    if workers <= 1:
+        res = [_cpu_tile(s) for s in range(tiles)]
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(workers) as pool:
+            res = pool.map(_cpu_tile, range(tiles))
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    return work / wall, wall
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    workers = os.cpu_count() or 1
+    vals = []
+    for i in range(a.warmup + a.steps):
+        v, wall = cpu_port_throughput(workers, workers)
+        if i >= a.warmup:
+            vals.append((v, wall))
+    value = sum(v for v, _ in vals) / len(vals)
+    ms = 1000.0 * sum(w for _, w in vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"float64 CPU port of the reference path: {workers} tiles of "
+                               f"{CPU_TILE}x{CPU_TILE} px x 24 h (walls, 153-patch SVF, hourly "
+                               f"Tmrt+UTCI) per step, one tile per host process",
+                   "size": CPU_TILE, "hours": 24},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                         "sample": f"{workers} x ({CPU_TILE}^2 px x 24 h) per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, throttle reasons) while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        import statistics
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def _traffic(kernel):
+    """Per-launch DRAM bytes of ``kernel`` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith(kernel + "="):
+                    return float(line.split("=", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def main():
+    a = _args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return 0
+    import numpy as np
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from solweig_cuda_b200 import batched, engine, synthetic
+    dev = torch.device("cuda", local)
+    n = a.size
+    sc = synthetic.make_scene(n, seed=0)
+    doy = 172 + rank
+    met = synthetic.make_met(doy=doy, latitude=53.0, longitude=0.0)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, device=dev)
+    torch.cuda.synchronize()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+
+    plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    chosen = batched.BatchedDay(scene, 53.0, 0.0, 3.0, 0.0) if a.form == "batched" else plain
+
+    def day(runner):
+        return runner.run_day(met, outputs=("tmrt", "utci"))
+
+    def timed(runner, steps, warmup):
+        for _ in range(warmup):
+            day(runner)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(steps):
+            flush.zero_()
+            if dist is not None:
+                dist.barrier()
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            day(runner)
+            e.record()
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+        return times
+
+    launches_per_day = sum(2 if x > 0 else 1 for x in
+                           __import__("solweig_cuda_b200.sun", fromlist=["metdata"]).metdata(
+                               met, 53.0, 0.0, 3.0, 0.0).altitude)
+    plain_times = timed(plain, max(1, min(a.steps, 3)), 1)
+    with ClockSampler(local) as clocks:
+        chosen_times = timed(chosen, a.steps, a.warmup)
+    ms = float(np.mean(chosen_times))
+    ms_plain = float(np.mean(plain_times))
+    if dist is not None:
+        t = torch.tensor([ms, ms_plain], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_plain = float(t[0]), float(t[1])
+    work = n * n * 24
+    value = world * work / (ms / 1000.0)
+    value_plain = world * work / (ms_plain / 1000.0)
+
+    # Per-kernel timing of one instrumented day (events on the launching stream).
+    kern = plain.profile_day(met) if hasattr(plain, "profile_day") else {}
+    roof = None
+    if kern:
+        dom = max(kern, key=lambda k: kern[k]["ms"])
+        info = kern[dom]
+        peak, peak_kind = _peaks()
+        achieved = info["bytes_per_launch"] / (info["ms"] / info["launches"] / 1000.0) / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                "traffic": _traffic(dom), "launch_ms": info["ms"] / info["launches"],
+                "share": {k: round(v["ms"] / sum(x["ms"] for x in kern.values()), 4) for k, v in kern.items()}}
+
+    # End to end through the public API with host buffers.
+    from solweig_cuda_b200 import api
+    e2e_times, h2d, d2h = [], 0, 0
+    for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = api.simulate_day(sc.dsm, sc.trees, sc.dem, met, latitude=53.0, longitude=0.0,
+                               landcover=sc.landcover, pixel_size=1.0, device=dev,
+                               form=a.form)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_times.append(dt)
+        h2d, d2h = res["h2d_bytes"], res["d2h_bytes"]
+    e2e_s = float(np.mean(e2e_times)) if e2e_times else float("nan")
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    e2e_value = world * work / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, wall = cpu_port_throughput(1, 1)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"one {CPU_TILE}x{CPU_TILE} px tile x 24 h (walls, SVF, hourly step, UTCI), "
+                         f"float64 numpy port of the reference path, {wall:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{n}x{n} px at 1 m, 24 hourly steps (one day, DOY 172, 53N), "
+                                   f"static walls + 153-patch SVF prepared before timing",
+                       "form": a.form, "size": n, "hours": 24, "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"days over {world} GPU(s)"},
+            "plain": {"value": value_plain, "ms_per_step": ms_plain},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_s,
+                    "includes": "H2D rasters, walls, 153-patch SVF, 24 h, D2H Tmrt+UTCI"},
+            "gpu_launches": launches_per_day * a.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

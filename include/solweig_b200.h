@@ -26,8 +26,10 @@
  *   solweig_svf_unpack        src/svf.py:113-114 (the three [rows,cols,P] cubes)
  *   solweig_diffsh            src/svf.py:117-131, src/kernels/geometry.cu:161-172
  *   solweig_gvf               src/model.py:569-622, src/kernels/gvf.cu:79-292
- *   solweig_step              src/model.py:15-256 (Solweig_2022a_calc, device part)
+ *   solweig_step(_shadow,_radiation)
+ *                             src/model.py:15-256 (Solweig_2022a_calc, device part)
  *   solweig_day               src/series.py:445-491 (the hour loop of _run_day)
+ *   solweig_scene_build/finalize src/series.py:252-349 (_prepare_spatial, per pixel)
  *   solweig_utci              src/utci.py:6-33, src/kernels/utci.cu
  */
 #ifndef SOLWEIG_B200_H
@@ -205,10 +207,44 @@ int solweig_gvf(const SolweigScene* scene, const float* shadow, const double* wa
                 int second_steps, float* scratch /* [5][pixels] */, float* planes, void* stream);
 
 /* The hourly step ---------------------------------------------------------- */
+/* Hour records and the sky layout live in DEVICE memory (hours[hour]), so a
+ * captured launch sequence replays for any forcing.  scratch: [5][pixels]
+ * float32 (the per-pixel GVF field quad and, with water pixels, the Lup of the
+ * first search direction).  Night hours: the shadow kernel returns at once. */
+int solweig_step_shadow(const SolweigScene* scene, const SolweigHour* hours, int hour,
+                        float* scratch, void* stream);
+int solweig_step_radiation(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                           const SolweigHour* hours, int hour, const SolweigState* state,
+                           const SolweigOutputs* out, const int32_t* gvf_dxdy, int first_steps,
+                           int second_steps, const float* scratch, void* stream);
+/* Both kernels of one hour. */
 int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
-                 const SolweigHour* hour, SolweigState* state, const SolweigOutputs* out,
-                 const int32_t* gvf_dxdy, int first_steps, int second_steps,
-                 float* scratch /* [5][pixels] */, void* stream);
+                 const SolweigHour* hours, int hour, const SolweigState* state,
+                 const SolweigOutputs* out, const int32_t* gvf_dxdy, int first_steps,
+                 int second_steps, float* scratch, void* stream);
+/* All hours of a day: output plane of hour h at base pointer + h * hour_stride. */
+int solweig_day(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                const SolweigHour* hours, int nhours, const SolweigState* state,
+                const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                int first_steps, int second_steps, float* scratch, void* stream);
+
+/* Static scene preparation (src/series.py:252-349) ------------------------- */
+/* classes: [nclasses][6] (code, albedo, emissivity, TgK, Tstart, TmaxLST);
+ * defaults: albedo, emissivity, TgK, Tstart, TmaxLST without land cover;
+ * landcover_in may be NULL. */
+int solweig_scene_build(const double* dsm_in, const double* trees_in, const double* dem_in,
+                        const double* landcover_in, int64_t pixels, double raise_dsm,
+                        double raise_dem, const double* classes, int nclasses,
+                        const double* defaults, double* dsm, double* vegdem, double* vegdem2,
+                        uint8_t* flags, float* alb, float* emis, float* tgk, float* tstart,
+                        float* tmaxlst, float* lc_out, void* stream);
+/* From the 16 SVF planes: float32 copies of the 15 SVF planes, svfbuveg,
+ * svfalfa, tan(asvf) and the 18 GVF wall-face bits (face windows from the host). */
+int solweig_scene_finalize(const double* planes, const double* walls, const double* aspect_rad,
+                           int64_t pixels, double transmissivity, const double* face_low,
+                           const double* face_high, const int32_t* face_middle, float* svf32,
+                           float* svfbuveg, double* svfalfa, double* tan_asvf, uint32_t* gvf_face,
+                           void* stream);
 
 /* UTCI ------------------------------------------------------------------- */
 /* Per-pixel weather (any of ta/rh/va may be a 1-element array when its
@@ -216,6 +252,12 @@ int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
 int solweig_utci(const float* ta, const float* rh, const float* tmrt, const float* va,
                  int ta_scalar, int rh_scalar, int va_scalar, float* out, int64_t n,
                  void* stream);
+/* Host function: UTCI as a polynomial in D = Tmrt - Ta for scalar weather,
+ * coefficients[0..6] (all zero when an input is the -999 sentinel). */
+int solweig_utci_collapse(double ta, double rh, double va, double* coefficients);
+
+/* sizeof(SolweigScene, SolweigSkyLayout, SolweigHour, SolweigOutputs, SolweigState). */
+int solweig_struct_sizes(int64_t* out);
 
 #ifdef __cplusplus
 }

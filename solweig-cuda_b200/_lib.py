@@ -91,7 +91,8 @@ EXPORTED_SYMBOLS = (
     "solweig_last_error", "solweig_version", "solweig_wall_heights", "solweig_wall_aspect",
     "solweig_shadow", "solweig_svf", "solweig_svf_unpack", "solweig_diffsh", "solweig_gvf",
     "solweig_step", "solweig_utci", "solweig_utci_collapse", "solweig_scene_build",
-    "solweig_scene_finalize", "solweig_struct_sizes",
+    "solweig_scene_finalize", "solweig_struct_sizes", "solweig_step_shadow",
+    "solweig_step_radiation", "solweig_day",
 )
 
 _lock = threading.Lock()
@@ -115,13 +116,16 @@ def _declare(lib):
         "solweig_svf_unpack": (i32, [P, i64, i32, P, P, P, P]),
         "solweig_diffsh": (i32, [P, P, P, i64, fl, P]),
         "solweig_gvf": (i32, [P, P, P, P, dbl, dbl, dbl, dbl, dbl, P, i32, i32, P, P, P]),
-        "solweig_step": (i32, [P, P, P, P, P, P, i32, i32, P, P]),
+        "solweig_step": (i32, [P, P, P, i32, P, P, P, i32, i32, P, P]),
+        "solweig_day": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, P]),
         "solweig_utci": (i32, [P, P, P, P, i32, i32, i32, P, i64, P]),
         "solweig_utci_collapse": (i32, [dbl, dbl, dbl, P]),
         "solweig_scene_build": (i32, [P, P, P, P, i64, dbl, dbl, P, i32, P, P, P, P, P, P, P, P, P,
                                       P, P, P]),
         "solweig_scene_finalize": (i32, [P, P, P, i64, dbl, P, P, P, P, P, P, P, P, P]),
         "solweig_struct_sizes": (i32, [P]),
+        "solweig_step_shadow": (i32, [P, P, i32, P, P]),
+        "solweig_step_radiation": (i32, [P, P, P, i32, P, P, P, i32, i32, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -158,3 +162,8 @@ def check(status, what="solweig"):
     if status != 0:
         msg = lib().solweig_last_error()
         raise RuntimeError(f"{what} failed ({status}): {msg.decode() if msg else ''}")
+
+
+def struct_bytes(obj):
+    """Raw bytes of a ctypes struct (for upload to device memory)."""
+    return ctypes.string_at(ctypes.addressof(obj), ctypes.sizeof(obj))

@@ -1,0 +1,44 @@
+"""Public end-to-end call: host rasters and forcing in, host Tmrt and UTCI out.
+
+``simulate_day`` is the whole per-tile workflow of ``run_timeseries`` for one
+calendar day without file I/O: rasters uploaded, walls and the 153-patch SVF
+prepared on the device, the 24 hourly steps run, and every hour's Tmrt and
+UTCI copied back into pinned host memory.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import engine
+from .batched import BatchedDay
+
+__all__ = ["simulate_day"]
+
+
+def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixel_size=1.0,
+                 site_altitude=3.0, utc=0.0, device="cuda", form="batched"):
+    """Returns {"tmrt": [H, rows, cols] float32, "utci": ..., "h2d_bytes", "d2h_bytes"}."""
+    arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in (dsm, trees, dem)]
+    lc = None if landcover is None else np.ascontiguousarray(landcover, dtype=np.float64)
+    h2d = sum(a.nbytes for a in arrays) + (lc.nbytes if lc is not None else 0)
+    scene = engine.Scene(arrays[0], arrays[1], arrays[2], pixel_size, landcover=lc, device=device)
+    met = np.asarray(met, dtype=np.float64)
+    if form == "batched":
+        runner = BatchedDay(scene, latitude, longitude, site_altitude, utc, hours=len(met),
+                            use_graph=False)
+    else:
+        runner = engine.DayRunner(scene, latitude, longitude, site_altitude, utc)
+    res = runner.run_day(met, outputs=("tmrt", "utci"))
+    out = {}
+    d2h = 0
+    for k in ("tmrt", "utci"):
+        host = torch.empty(res[k].shape, dtype=torch.float32, pin_memory=True)
+        host.copy_(res[k], non_blocking=True)
+        out[k] = host
+        d2h += host.numel() * 4
+    torch.cuda.current_stream().synchronize()
+    out = {k: v.numpy() for k, v in out.items()}
+    out["h2d_bytes"] = h2d
+    out["d2h_bytes"] = d2h
+    return out

@@ -34,7 +34,10 @@ __device__ __forceinline__ double lup_excess(double emis, double tg, double shad
 }
 
 __global__ void __launch_bounds__(kStepBX* kStepBY) step_shadow_kernel(
-    SolweigScene S, SolweigHour h, float4* __restrict__ quad, float* __restrict__ lup_first) {
+    SolweigScene S, const SolweigHour* __restrict__ hours, int hour, float4* __restrict__ quad,
+    float* __restrict__ lup_first) {
+    const SolweigHour& h = hours[hour];
+    if (!h.daytime) return;
     const int c = blockIdx.x * kStepBX + threadIdx.x;
     const int r = blockIdx.y * kStepBY + threadIdx.y;
     if (r >= S.rows || c >= S.cols) return;
@@ -77,9 +80,10 @@ struct StepGvfArgs {
 };
 
 template <bool Day, bool Cardinal>
-__global__ void __launch_bounds__(kStepBX* kStepBY) step_radiation_kernel(
-    SolweigScene S, SolweigSkyLayout L, SolweigHour h, SolweigState st, SolweigOutputs out,
-    StepGvfArgs ga, const float4* __restrict__ quad, const float* __restrict__ lup_first) {
+__device__ __forceinline__ void radiation_body(
+    const SolweigScene& S, const SolweigSkyLayout& L, const SolweigHour& h, const SolweigState& st,
+    const SolweigOutputs& out, const StepGvfArgs& ga, const float4* __restrict__ quad,
+    const float* __restrict__ lup_first) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PatchSmem& ps = *reinterpret_cast<PatchSmem*>(smem_raw);
     int2* offs = reinterpret_cast<int2*>(smem_raw + sizeof(PatchSmem));
@@ -276,6 +280,20 @@ __global__ void __launch_bounds__(kStepBX* kStepBY) step_radiation_kernel(
     if (out.tg_out) out.tg_out[p] = (float)tg_out;
 }
 
+// One kernel for both branches: the day/night choice is read from the hour
+// record in device memory, so a captured day replays for any forcing.
+template <bool Cardinal>
+__global__ void __launch_bounds__(kStepBX* kStepBY) step_radiation_kernel(
+    SolweigScene S, const SolweigSkyLayout* __restrict__ L, const SolweigHour* __restrict__ hours,
+    int hour, SolweigState st, SolweigOutputs out, StepGvfArgs ga, const float4* __restrict__ quad,
+    const float* __restrict__ lup_first) {
+    const SolweigHour& h = hours[hour];
+    if (h.daytime)
+        radiation_body<true, Cardinal>(S, *L, h, st, out, ga, quad, lup_first);
+    else
+        radiation_body<false, Cardinal>(S, *L, h, st, out, ga, quad, lup_first);
+}
+
 size_t radiation_smem_bytes(int halo) {
     const size_t head = (sizeof(PatchSmem) + sizeof(int2) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS + 15) & ~size_t(15);
     return head + sizeof(float4) * (size_t)(kStepBX + 2 * halo) * (kStepBY + 2 * halo);
@@ -297,61 +315,102 @@ static int check_scene(const SolweigScene* S) {
     return SOLWEIG_OK;
 }
 
-extern "C" int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
-                            const SolweigHour* hour, SolweigState* state, const SolweigOutputs* out,
-                            const int32_t* gvf_dxdy, int first_steps, int second_steps,
-                            float* scratch, void* stream) {
+static void set_smem_once(const void* kernel, size_t bytes) {
+    // cudaFuncSetAttribute is not a stream operation; repeating it is harmless
+    // but costs a driver call per launch, so remember the largest size set.
+    static thread_local size_t done[2] = {0, 0};
+    static thread_local const void* which[2] = {nullptr, nullptr};
+    for (int i = 0; i < 2; ++i)
+        if (which[i] == kernel && done[i] >= bytes) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    for (int i = 0; i < 2; ++i)
+        if (which[i] == kernel || which[i] == nullptr) {
+            which[i] = kernel;
+            done[i] = bytes;
+            return;
+        }
+}
+
+extern "C" int solweig_step_shadow(const SolweigScene* scene, const SolweigHour* hours, int hour,
+                                   float* scratch, void* stream) {
     int rc = check_scene(scene);
     if (rc) return rc;
-    SOLWEIG_CHECK_ARG(layout && hour && state && out, "solweig_step: null argument");
-    SOLWEIG_CHECK_ARG(layout->patches > 0 && layout->patches <= SOLWEIG_MAX_PATCHES &&
-                          layout->patches == scene->patches,
-                      "solweig_step: layout has %d patches, scene %d", layout->patches, scene->patches);
+    SOLWEIG_CHECK_ARG(hours && hour >= 0 && scratch, "solweig_step_shadow: bad arguments");
+    const SolweigScene& S = *scene;
+    dim3 block(kStepBX, kStepBY);
+    dim3 grid(blocks_for(S.cols, kStepBX), blocks_for(S.rows, kStepBY));
+    float4* quad = reinterpret_cast<float4*>(scratch);
+    float* lup_first = S.has_water ? scratch + 4 * (long long)S.rows * S.cols : nullptr;
+    step_shadow_kernel<<<grid, block, 0, as_stream(stream)>>>(S, hours, hour, quad, lup_first);
+    SOLWEIG_CHECK_LAUNCH("step_shadow_kernel");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_step_radiation(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                      const SolweigHour* hours, int hour, const SolweigState* state,
+                                      const SolweigOutputs* out, const int32_t* gvf_dxdy,
+                                      int first_steps, int second_steps, const float* scratch,
+                                      void* stream) {
+    int rc = check_scene(scene);
+    if (rc) return rc;
+    SOLWEIG_CHECK_ARG(layout && hours && hour >= 0 && state && out && scratch && gvf_dxdy,
+                      "solweig_step_radiation: null argument");
     SOLWEIG_CHECK_ARG(state->tgmap1 && state->tgmap1e && state->tgmap1s && state->tgmap1w &&
                           state->tgmap1n && state->tgout1,
-                      "solweig_step: state has a null plane");
+                      "solweig_step_radiation: state has a null plane");
+    SOLWEIG_CHECK_ARG(second_steps >= 1 && second_steps <= SOLWEIG_GVF_MAX_STEPS && first_steps >= 1 &&
+                          first_steps <= second_steps,
+                      "solweig_step_radiation: GVF steps first=%d second=%d", first_steps,
+                      second_steps);
     const SolweigScene& S = *scene;
-    cudaStream_t st = as_stream(stream);
     const bool full = out->least || out->lsouth || out->lwest || out->lnorth;
     dim3 block(kStepBX, kStepBY);
     dim3 grid(blocks_for(S.cols, kStepBX), blocks_for(S.rows, kStepBY));
     StepGvfArgs ga{reinterpret_cast<const int2*>(gvf_dxdy), first_steps, second_steps,
-                   second_steps > 0 ? second_steps - 1 : 0};
+                   second_steps - 1};
     const size_t smem = radiation_smem_bytes(ga.halo);
-    if (hour->daytime) {
-        SOLWEIG_CHECK_ARG(scratch && gvf_dxdy && hour->ray_dxdy && hour->ray_dz,
-                          "solweig_step: daytime needs scratch, GVF offsets and the sun ray");
-        SOLWEIG_CHECK_ARG(second_steps >= 1 && second_steps <= SOLWEIG_GVF_MAX_STEPS &&
-                              first_steps >= 1 && first_steps <= second_steps,
-                          "solweig_step: GVF steps first=%d second=%d", first_steps, second_steps);
-        SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "solweig_step: GVF halo %d too large for shared memory",
-                          ga.halo);
-        float4* quad = reinterpret_cast<float4*>(scratch);
-        float* lup_first = S.has_water ? scratch + 4 * (long long)S.rows * S.cols : nullptr;
-        step_shadow_kernel<<<grid, block, 0, st>>>(S, *hour, quad, lup_first);
-        SOLWEIG_CHECK_LAUNCH("step_shadow_kernel");
-        if (full) {
-            auto k = step_radiation_kernel<true, true>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k<<<grid, block, smem, st>>>(S, *layout, *hour, *state, *out, ga, quad, lup_first);
-        } else {
-            auto k = step_radiation_kernel<true, false>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k<<<grid, block, smem, st>>>(S, *layout, *hour, *state, *out, ga, quad, lup_first);
-        }
-        SOLWEIG_CHECK_LAUNCH("step_radiation_kernel<day>");
+    SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "solweig_step_radiation: GVF halo %d too large", ga.halo);
+    const float4* quad = reinterpret_cast<const float4*>(scratch);
+    const float* lup_first = S.has_water ? scratch + 4 * (long long)S.rows * S.cols : nullptr;
+    cudaStream_t st = as_stream(stream);
+    if (full) {
+        set_smem_once((const void*)step_radiation_kernel<true>, smem);
+        step_radiation_kernel<true><<<grid, block, smem, st>>>(S, layout, hours, hour, *state, *out,
+                                                               ga, quad, lup_first);
     } else {
-        const size_t smem_night = radiation_smem_bytes(0);
-        if (full) {
-            auto k = step_radiation_kernel<false, true>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_night);
-            k<<<grid, block, smem_night, st>>>(S, *layout, *hour, *state, *out, ga, nullptr, nullptr);
-        } else {
-            auto k = step_radiation_kernel<false, false>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_night);
-            k<<<grid, block, smem_night, st>>>(S, *layout, *hour, *state, *out, ga, nullptr, nullptr);
-        }
-        SOLWEIG_CHECK_LAUNCH("step_radiation_kernel<night>");
+        set_smem_once((const void*)step_radiation_kernel<false>, smem);
+        step_radiation_kernel<false><<<grid, block, smem, st>>>(S, layout, hours, hour, *state, *out,
+                                                                ga, quad, lup_first);
+    }
+    SOLWEIG_CHECK_LAUNCH("step_radiation_kernel");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                            const SolweigHour* hours, int hour, const SolweigState* state,
+                            const SolweigOutputs* out, const int32_t* gvf_dxdy, int first_steps,
+                            int second_steps, float* scratch, void* stream) {
+    int rc = solweig_step_shadow(scene, hours, hour, scratch, stream);
+    if (rc) return rc;
+    return solweig_step_radiation(scene, layout, hours, hour, state, out, gvf_dxdy, first_steps,
+                                  second_steps, scratch, stream);
+}
+
+extern "C" int solweig_day(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                           const SolweigHour* hours, int nhours, const SolweigState* state,
+                           const SolweigOutputs* base, int64_t hour_stride,
+                           const int32_t* gvf_dxdy, int first_steps, int second_steps,
+                           float* scratch, void* stream) {
+    SOLWEIG_CHECK_ARG(base && nhours > 0 && hour_stride >= 0, "solweig_day: bad arguments");
+    for (int hr = 0; hr < nhours; ++hr) {
+        SolweigOutputs o = *base;
+        float** f = reinterpret_cast<float**>(&o);
+        const int nf = sizeof(SolweigOutputs) / sizeof(float*);
+        for (int i = 0; i < nf; ++i)
+            if (f[i]) f[i] += (long long)hr * hour_stride;
+        int rc = solweig_step(scene, layout, hours, hr, state, &o, gvf_dxdy, first_steps,
+                              second_steps, scratch, stream);
+        if (rc) return rc;
     }
     return SOLWEIG_OK;
 }

@@ -107,6 +107,15 @@ class SkyLayout:
         sec |= (((azimuth >= 180) & (azimuth < 360)).astype(np.uint8) << 2)
         sec |= (((azimuth >= 270) | (azimuth < 90)).astype(np.uint8) << 3)
         self.sectors = np.ascontiguousarray(sec)
+        self._device = {}
+
+    def device(self, dev):
+        """The layout struct in device memory (uploaded once per device)."""
+        key = str(dev)
+        if key not in self._device:
+            raw = np.frombuffer(_lib.struct_bytes(self.struct), dtype=np.uint8)
+            self._device[key] = torch.from_numpy(raw.copy()).to(dev)
+        return self._device[key]
 
 
 def _upload(arr, dtype, device):
@@ -469,12 +478,12 @@ def hour_plan(scene, latitude, altitude, azimuth, zen, jday, dectime, altmax, ta
             rad_tot += lum[k] * L.steradian[k] * np.sin(L.altitude[k] * (np.pi / 180))
         h.rad_tot = float(np.asarray(rad_tot).item())
         tan_alt = np.tan(altitude * (np.pi / 180))
-        for k in range(L.count):
-            h.lum[k] = lum[k]
-            diff = np.abs(azimuth - L.azimuth[k])
-            yi = 2 * np.cos(diff * (np.pi / 180)) * tan_alt
-            h.yi[k] = 0.0 if yi > 0 else yi
-            h.lw_sun_test[k] = 1 if (90 < diff < 270) else 0
+        diff = np.abs(azimuth - L.azimuth)
+        yi = 2 * np.cos(diff * (np.pi / 180)) * tan_alt
+        P = L.count
+        np.ctypeslib.as_array(h.lum)[:P] = lum.astype(np.float32)
+        np.ctypeslib.as_array(h.yi)[:P] = np.where(yi > 0, 0.0, yi)
+        np.ctypeslib.as_array(h.lw_sun_test)[:P] = ((diff > 90) & (diff < 270)).astype(np.uint8)
     else:
         h.rad_tot = 1.0
     coef = (ctypes.c_double * 7)()
@@ -493,16 +502,99 @@ STEP_OUTPUTS = ("tmrt", "utci", "kdown", "kup", "ldown", "lup", "shadow", "tg", 
                 "kside", "lside", "d_rad", "tg_out")
 
 
+class HourBuffers:
+    """Pinned host + device slots for H hour records and their sun rays."""
+
+    def __init__(self, scene, hours=24):
+        self.hours = hours
+        self.kmax = max(scene.shape) + 2
+        self.hsize = ctypes.sizeof(_lib.SolweigHour)
+        dev = scene.device
+        self.h_host = torch.empty(hours * self.hsize, dtype=torch.uint8, pin_memory=True)
+        self.h_dev = torch.empty(hours * self.hsize, dtype=torch.uint8, device=dev)
+        self.r_host = torch.empty((hours, self.kmax, 2), dtype=torch.int32, pin_memory=True)
+        self.z_host = torch.empty((hours, self.kmax), dtype=torch.float64, pin_memory=True)
+        self.r_dev = torch.zeros((hours, self.kmax, 2), dtype=torch.int32, device=dev)
+        self.z_dev = torch.zeros((hours, self.kmax), dtype=torch.float64, device=dev)
+        self.done = None
+
+    def wait_free(self):
+        if self.done is not None:
+            self.done.synchronize()
+            self.done = None
+
+    def put(self, slot, hour, ray):
+        """Write hour record ``slot`` (pointing at its device ray slot) into pinned memory."""
+        if ray is not None and ray.steps:
+            k = ray.steps
+            if k > self.kmax:
+                raise ValueError("sun ray longer than the ray buffer")
+            self.r_host[slot, :k].numpy()[:] = ray.dxdy
+            self.z_host[slot, :k].numpy()[:] = ray.dz
+            hour.ray_dxdy = self.r_dev[slot].data_ptr()
+            hour.ray_dz = self.z_dev[slot].data_ptr()
+        raw = np.frombuffer(_lib.struct_bytes(hour), dtype=np.uint8)
+        self.h_host.numpy()[slot * self.hsize:(slot + 1) * self.hsize] = raw
+
+    def upload(self, first, count, steps):
+        """Async copy of slots [first, first + count) to the device."""
+        hs = self.hsize
+        self.h_dev[first * hs:(first + count) * hs].copy_(self.h_host[first * hs:(first + count) * hs],
+                                                          non_blocking=True)
+        k = max(1, int(steps))
+        self.r_dev[first:first + count, :k].copy_(self.r_host[first:first + count, :k], non_blocking=True)
+        self.z_dev[first:first + count, :k].copy_(self.z_host[first:first + count, :k], non_blocking=True)
+
+    def mark(self):
+        self.done = torch.cuda.Event()
+        self.done.record()
+
+    def ptr(self):
+        return ctypes.c_void_p(self.h_dev.data_ptr())
+
+
+def plan_day(scene, met, latitude, longitude, site_altitude, utc):
+    """FP64 host plan of every row of one day: [(SolweigHour, ShadowRay|None, HourScalars)]."""
+    met = np.asarray(met, dtype=np.float64)
+    sol = _sun.metdata(met, latitude, longitude, site_altitude, utc)
+    dectime = sol.dectime
+    timestepdec = (dectime[1] - dectime[0]) if len(met) > 1 else 1 / 24.
+    twater = float(np.mean(met[:, 11])) if scene.landcover else None
+    firstdaytime, timeadd, CI = 1, 0.0, 1.0
+    out = []
+    for i in range(len(met)):
+        if dectime[i] - np.floor(dectime[i]) == 0:
+            CI = 1.
+        psi = _leaf_psi(met[i, 1])
+        h, ray, scal, (firstdaytime, timeadd, CI) = hour_plan(
+            scene, latitude, sol.altitude[i], sol.azimuth[i], sol.zen[i], sol.jday[i], dectime[i],
+            sol.altmax[i], met[i, 11], met[i, 10], met[i, 14], met[i, 21], met[i, 22], met[i, 12],
+            met[i, 9], psi, CI, firstdaytime, timeadd, timestepdec, twater)
+        out.append((h, ray, scal))
+    return out
+
+
+def outputs_struct(outputs, index=None):
+    out = _lib.SolweigOutputs()
+    for k, t in outputs.items():
+        setattr(out, k, (t[index] if index is not None else t).data_ptr())
+    return out
+
+
 class DayRunner:
-    """Hour loop of one day (plain form: one host plan + kernel pair per hour)."""
+    """Plain form: one host plan, one hour-record upload and one kernel pair
+    per hour, launched as the hours are planned (the host plans hour h+1
+    while the GPU runs hour h)."""
 
     def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0):
         self.scene = scene
         self.latitude, self.longitude, self.site_altitude, self.utc = latitude, longitude, site_altitude, utc
         dev = scene.device
-        shape = scene.shape
-        self.state = {k: torch.zeros(shape, dtype=torch.float32, device=dev) for k in _lib.STATE_FIELDS}
+        self.state = {k: torch.zeros(scene.shape, dtype=torch.float32, device=dev)
+                      for k in _lib.STATE_FIELDS}
         self.scratch = torch.empty((5, scene.rows, scene.cols), dtype=torch.float32, device=dev)
+        self.buffers = HourBuffers(scene, 24)
+        self.layout_dev = scene.layout.device(dev)
 
     def state_struct(self):
         s = _lib.SolweigState()
@@ -514,39 +606,30 @@ class DayRunner:
         for t in self.state.values():
             t.zero_()
 
-    def step(self, hour, ray, outputs, stream=None):
-        """Launch one hour.  ``outputs`` maps ABI output names to float32 device tensors."""
+    def _launch(self, slot, out_struct, stream=None):
         sc = self.scene
-        ray_t = None
-        if ray is not None:
-            ray_t = (_upload(ray.dxdy, np.int32, sc.device), _upload(ray.dz, np.float64, sc.device))
-            hour.ray_dxdy = ray_t[0].data_ptr()
-            hour.ray_dz = ray_t[1].data_ptr()
-        out = _lib.SolweigOutputs()
-        for k, t in outputs.items():
-            setattr(out, k, t.data_ptr())
-        st = self.state_struct()
         _lib.check(_lib.lib().solweig_step(
-            ctypes.byref(sc.struct), ctypes.byref(sc.layout.struct), ctypes.byref(hour),
-            ctypes.byref(st), ctypes.byref(out), device_ptr(sc.gvf_dxdy), sc.first_steps,
-            sc.second_steps, device_ptr(self.scratch), stream_handle(stream)), "solweig_step")
-        return ray_t  # keep the ray tensors alive until the caller syncs
+            ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), slot,
+            ctypes.byref(self.state_struct()), ctypes.byref(out_struct), device_ptr(sc.gvf_dxdy),
+            sc.first_steps, sc.second_steps, device_ptr(self.scratch), stream_handle(stream)),
+            "solweig_step")
 
-    def run_day(self, met, outputs=("tmrt", "utci"), hours=None, stream=None):
+    def run_day(self, met, outputs=("tmrt", "utci"), stream=None):
         """Run the rows of one calendar day; returns {name: tensor [H, rows, cols]}."""
         met = np.asarray(met, dtype=np.float64)
+        if len(met) > self.buffers.hours:
+            raise ValueError(f"at most {self.buffers.hours} rows per day")
         sol = _sun.metdata(met, self.latitude, self.longitude, self.site_altitude, self.utc)
         dectime = sol.dectime
         timestepdec = (dectime[1] - dectime[0]) if len(met) > 1 else 1 / 24.
         twater = float(np.mean(met[:, 11])) if self.scene.landcover else None
-        idx = list(range(len(met))) if hours is None else list(hours)
-        res = {k: torch.empty((len(idx),) + self.scene.shape, dtype=torch.float32,
+        res = {k: torch.empty((len(met),) + self.scene.shape, dtype=torch.float32,
                               device=self.scene.device) for k in outputs}
+        self.buffers.wait_free()
         self.reset_state()
         firstdaytime, timeadd, CI = 1, 0.0, 1.0
-        keep = []
         scalars = []
-        for j, i in enumerate(idx):
+        for i in range(len(met)):
             if dectime[i] - np.floor(dectime[i]) == 0:
                 CI = 1.
             psi = _leaf_psi(met[i, 1])
@@ -555,8 +638,60 @@ class DayRunner:
                 dectime[i], sol.altmax[i], met[i, 11], met[i, 10], met[i, 14], met[i, 21],
                 met[i, 22], met[i, 12], met[i, 9], psi, CI, firstdaytime, timeadd, timestepdec,
                 twater)
-            keep.append(self.step(h, ray, {k: res[k][j] for k in outputs}, stream))
+            self.buffers.put(i, h, ray)
+            self.buffers.upload(i, 1, ray.steps if ray is not None else 1)
+            self._launch(i, outputs_struct(res, i), stream)
             scalars.append(scal)
+        self.buffers.mark()
         self.last_scalars = scalars
-        self._keep = keep
         return res
+
+    def profile_day(self, met):
+        """Per-kernel device time of one day: {kernel: {ms, launches, bytes_per_launch}}."""
+        sc = self.scene
+        plan = plan_day(sc, met, self.latitude, self.longitude, self.site_altitude, self.utc)
+        self.buffers.wait_free()
+        for i, (h, ray, _) in enumerate(plan):
+            self.buffers.put(i, h, ray)
+        self.buffers.upload(0, len(plan), self.buffers.kmax)
+        self.reset_state()
+        out = {k: torch.empty(sc.shape, dtype=torch.float32, device=sc.device) for k in ("tmrt", "utci")}
+        o = outputs_struct(out)
+        st = self.state_struct()
+        L = _lib.lib()
+        times = {"step_shadow_kernel": [], "step_radiation_kernel": []}
+        for i, (h, ray, _) in enumerate(plan):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record()
+            if h.daytime:
+                _lib.check(L.solweig_step_shadow(ctypes.byref(sc.struct), self.buffers.ptr(), i,
+                                                 device_ptr(self.scratch), stream_handle()), "shadow")
+            ev[1].record()
+            _lib.check(L.solweig_step_radiation(
+                ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), i,
+                ctypes.byref(st), ctypes.byref(o), device_ptr(sc.gvf_dxdy), sc.first_steps,
+                sc.second_steps, device_ptr(self.scratch), stream_handle()), "radiation")
+            ev[2].record()
+            times["step_shadow_kernel"].append((ev, 0, 1, bool(h.daytime)))
+            times["step_radiation_kernel"].append((ev, 1, 2, True))
+        self.buffers.mark()
+        torch.cuda.synchronize()
+        n = sc.pixels
+        bytes_per = {"step_shadow_kernel": n * SHADOW_BYTES_PER_PIXEL,
+                     "step_radiation_kernel": n * RADIATION_BYTES_PER_PIXEL}
+        res = {}
+        for k, lst in times.items():
+            ms = sum(e[a].elapsed_time(e[b]) for e, a, b, used in lst if used)
+            launches = sum(1 for *_, used in lst if used)
+            res[k] = {"ms": ms, "launches": launches, "bytes_per_launch": bytes_per[k]}
+        return res
+
+
+# Algorithmic HBM bytes per pixel and launch (each input and output once):
+# shadow: own dsm/vegdem/vegdem2/walls/aspect (40) + flags (1) + tgk/tstart/tmaxlst/emis/alb (20)
+#         + quad written (16);
+# radiation: quad (16) + flags (1) + emis/tgk/tstart/tmaxlst (16) + svfbuveg (4) + svfalfa and
+#         tan(asvf) (16) + masks (40) + vegetation/obstruction sums (16) + sky band counts (8)
+#         + wall-face bits (4) + thermal state read+write (48) + Tmrt and UTCI written (8).
+SHADOW_BYTES_PER_PIXEL = 77
+RADIATION_BYTES_PER_PIXEL = 177

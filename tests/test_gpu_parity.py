@@ -92,3 +92,27 @@ def test_day_tmrt_utci(scene48):
         assert d_t <= 0.1, f"hour {h}: Tmrt error {d_t}"
         assert d_u <= 0.05, f"hour {h}: UTCI error {d_u}"
         assert np.array_equal(np.isnan(ut[h]), ~ok)
+
+
+def test_batched_graph_matches_plain_and_replays(scene48):
+    """The graph-captured day equals the plain per-hour loop bit for bit, and a
+    second replay with another day's forcing still matches the oracle."""
+    import torch
+    from oracle import step as ST
+    from solweig_cuda_b200 import batched, engine, synthetic
+    sc, scene = scene48
+    loc = dict(latitude=53.0, longitude=0.0, altitude=3.0)
+    plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    day = batched.BatchedDay(scene, 53.0, 0.0, 3.0, 0.0)
+    s = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    for doy, seed in ((172, 0), (200, 5)):
+        met = synthetic.make_met(doy=doy, latitude=53.0, longitude=0.0, seed=seed)
+        a = {k: v.clone() for k, v in plain.run_day(met).items()}
+        b = day.run_day(met)
+        torch.cuda.synchronize()
+        assert torch.equal(a["tmrt"], b["tmrt"])
+        assert torch.equal(torch.nan_to_num(a["utci"], nan=-1e9), torch.nan_to_num(b["utci"], nan=-1e9))
+        want = ST.run_day(s, met, loc, 0.0)
+        tm = b["tmrt"].cpu().numpy()
+        for h in range(24):
+            assert np.max(np.abs(tm[h] - want[h]["Tmrt"])) <= 0.1, (doy, h)
