@@ -208,15 +208,19 @@ int solweig_gvf(const SolweigScene* scene, const float* shadow, const double* wa
 
 /* The hourly step ---------------------------------------------------------- */
 /* Hour records and the sky layout live in DEVICE memory (hours[hour]), so a
- * captured launch sequence replays for any forcing.  scratch: [5][pixels]
- * float32 (the per-pixel GVF field quad and, with water pixels, the Lup of the
- * first search direction).  Night hours: the shadow kernel returns at once. */
+ * captured launch sequence replays for any forcing.  scratch: [20][pixels]
+ * float32: the per-pixel GVF field quad (4), the Lup of the first search
+ * direction for water pixels (1) and the 15 GVF planes (15).  Night hours:
+ * the shadow and GVF kernels return at once. */
 int solweig_step_shadow(const SolweigScene* scene, const SolweigHour* hours, int hour,
                         float* scratch, void* stream);
+/* Ground view factors of the hour into scratch (tile_rows: 4, 8 or 16 rows per block). */
+int solweig_step_gvf(const SolweigScene* scene, const SolweigHour* hours, int hour,
+                     const int32_t* gvf_dxdy, int first_steps, int second_steps, float* scratch,
+                     int tile_rows, void* stream);
 int solweig_step_radiation(const SolweigScene* scene, const SolweigSkyLayout* layout,
                            const SolweigHour* hours, int hour, const SolweigState* state,
-                           const SolweigOutputs* out, const int32_t* gvf_dxdy, int first_steps,
-                           int second_steps, const float* scratch, void* stream);
+                           const SolweigOutputs* out, float* scratch, void* stream);
 /* Both kernels of one hour. */
 int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
                  const SolweigHour* hours, int hour, const SolweigState* state,

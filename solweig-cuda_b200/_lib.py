@@ -19,6 +19,7 @@ MASK_WORDS = 5
 MAX_BANDS = 8
 GVF_DIRECTIONS = 18
 GVF_MAX_STEPS = 64
+SCRATCH_PLANES = 20  # quad (4) + first-direction Lup (1) + 15 GVF planes
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -92,7 +93,7 @@ EXPORTED_SYMBOLS = (
     "solweig_shadow", "solweig_svf", "solweig_svf_unpack", "solweig_diffsh", "solweig_gvf",
     "solweig_step", "solweig_utci", "solweig_utci_collapse", "solweig_scene_build",
     "solweig_scene_finalize", "solweig_struct_sizes", "solweig_step_shadow",
-    "solweig_step_radiation", "solweig_day",
+    "solweig_step_radiation", "solweig_day", "solweig_step_gvf",
 )
 
 _lock = threading.Lock()
@@ -125,7 +126,8 @@ def _declare(lib):
         "solweig_scene_finalize": (i32, [P, P, P, i64, dbl, P, P, P, P, P, P, P, P, P]),
         "solweig_struct_sizes": (i32, [P]),
         "solweig_step_shadow": (i32, [P, P, i32, P, P]),
-        "solweig_step_radiation": (i32, [P, P, P, i32, P, P, P, i32, i32, P, P]),
+        "solweig_step_gvf": (i32, [P, P, i32, P, i32, i32, P, i32, P]),
+        "solweig_step_radiation": (i32, [P, P, P, i32, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -31,7 +31,8 @@ class BatchedDay:
         dev = scene.device
         self.state = {k: torch.zeros(scene.shape, dtype=torch.float32, device=dev)
                       for k in _lib.STATE_FIELDS}
-        self.scratch = torch.empty((5, scene.rows, scene.cols), dtype=torch.float32, device=dev)
+        self.scratch = torch.empty((_lib.SCRATCH_PLANES, scene.rows, scene.cols), dtype=torch.float32,
+                                   device=dev)
         self.buffers = HourBuffers(scene, hours)
         self.layout_dev = scene.layout.device(dev)
         self.out_names = tuple(outputs)

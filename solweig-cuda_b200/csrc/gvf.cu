@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(256) gvf_quad_kernel(
     lup_first[p] = (float)(kSBC * e * pow4(t * sh + ta + 273.15) - amb);
     if (has_water && (fl & 4)) t = twater - ta;
     quad[p] = make_float4((float)sh, (float)(kSBC * e * pow4(t * sh + ta + 273.15) - amb), alb[p],
-                          (float)(((fl & 1) ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+                          __int_as_float(((fl & 1) ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
 }
 
 __global__ void __launch_bounds__(kGvfBX* kGvfBY) gvf_planes_kernel(
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kGvfBX* kGvfBY) gvf_planes_kernel(
         planes[(3 * d + 2) * n + p] = g.nosh[d] / div;
     }
     planes[15 * n + p] = g.gvf_sum;
-    planes[16 * n + p] = ((int)own.w & kQuadGround) ? g.gvf_sum / 18.f : 1.f;
+    planes[16 * n + p] = (__float_as_int(own.w) & kQuadGround) ? g.gvf_sum / 18.f : 1.f;
 }
 
 }  // namespace solweig

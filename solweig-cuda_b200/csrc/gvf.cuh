@@ -59,7 +59,7 @@ __device__ __forceinline__ GvfSums gvf_walk(Sample sample, LupFirst lup_first, b
     for (int i = 0; i < 5; ++i) out.lup[i] = out.alb[i] = out.nosh[i] = 0.f;
     out.gvf_sum = 0.f;
     const float second = (float)g.second, first = (float)g.first;
-    const bool own_ground = ((int)own.w & kQuadGround) != 0;
+    const bool own_ground = (__float_as_int(own.w) & kQuadGround) != 0;
     const float own_b = own_ground ? 1.f : 0.f;
     // Per-direction additive corrections of the reference (own pixel).
     const float corr_lup = own.y * (1.f - own_b);
@@ -86,7 +86,7 @@ __device__ __forceinline__ GvfSums gvf_walk(Sample sample, LupFirst lup_first, b
                 t_lup = (use_lup_first && j == 0) ? lup_first(rr, cc) : q.y;
                 t_alb = q.z;
                 t_albsh = q.z * q.x;
-                const int bits = (int)q.w;
+                const int bits = __float_as_int(q.w);
                 t_bu = (bits & kQuadGround) != 0;
                 t_sun = (bits & kQuadSunwall) != 0;
             }

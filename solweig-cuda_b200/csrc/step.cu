@@ -11,6 +11,7 @@
 // (B200 runs FP64 at half the FP32 rate, and it is a few hundred operations
 // per pixel-hour); stored planes are float32.
 #include "gvf.cuh"
+#include "gvf_fields.cuh"
 #include "radiation.cuh"
 #include "shadow.cuh"
 
@@ -71,7 +72,7 @@ __global__ void __launch_bounds__(kStepBX* kStepBY) step_shadow_kernel(
     if (S.has_water && (fl & 4)) tg = h.twater - h.ta;
     const float lup = (float)lup_excess(emis, tg, shadow, h.ta);
     quad[p] = make_float4((float)shadow, lup, S.alb[p],
-                          (float)((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+                          __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
 }
 
 struct StepGvfArgs {
@@ -79,26 +80,108 @@ struct StepGvfArgs {
     int first, second, halo;
 };
 
+// Ground view factors of one daytime hour: the 15 planes [15][pixels]
+// (Lup, albedo, albedo without shadow) x (all, E, S, W, N), ambient and own-pixel
+// corrections included.
+template <int TY>
+__global__ void __launch_bounds__(32 * TY) step_gvf_kernel(
+    SolweigScene S, const SolweigHour* __restrict__ hours, int hour, StepGvfArgs ga,
+    const float4* __restrict__ quad, const float* __restrict__ lup_first, float* __restrict__ gvf) {
+    const SolweigHour& h = hours[hour];
+    if (!h.daytime) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int H = ga.halo, second = ga.second, first = ga.first;
+    const int pitch = 32 + 2 * H;
+    int* delta = reinterpret_cast<int*>(smem_raw);
+    int2* offs = reinterpret_cast<int2*>(smem_raw + sizeof(int) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS);
+    float4* tile = reinterpret_cast<float4*>(smem_raw + (sizeof(int) + sizeof(int2)) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS);
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < SOLWEIG_GVF_DIRECTIONS * second; i += 32 * TY) {
+        const int2 o = ga.offs[i];
+        offs[i] = o;
+        delta[i] = o.x * pitch + o.y;
+    }
+    const int row0 = blockIdx.y * TY - H, col0 = blockIdx.x * 32 - H;
+    load_quad_tile(tile, pitch, TY + 2 * H, quad, S.rows, S.cols, row0, col0);
+    __syncthreads();
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const int r = blockIdx.y * TY + threadIdx.y;
+    if (r >= S.rows || c >= S.cols) return;
+    const long long n = (long long)S.rows * S.cols;
+    const long long p = (long long)r * S.cols + c;
+    const float4* own_cell = tile + (threadIdx.y + H) * pitch + threadIdx.x + H;
+    const float4 own = *own_cell;
+    const double ta = h.ta;
+    const float lwall = (float)(kSBC * 0.9 * pow4(h.tgwall + ta + 273.15) - kSBC * 0.9 * pow4(ta + 273.15));
+    const float albedo_b = 0.2f;
+    const uint32_t face = S.gvf_face[p];
+    float lup[5], alb[5], nosh[5];
+    const bool own_ground = (__float_as_int(own.w) & kQuadGround) != 0;
+    if (S.has_water && lup_first) {
+        // Rare path (water pixels change the first direction's Lup): general walk.
+        GvfScalars gs{lwall, albedo_b, first, second};
+        auto sample = [&](int rr, int cc) -> float4 { return tile[(rr - row0) * pitch + (cc - col0)]; };
+        auto lfirst = [&](int rr, int cc) -> float { return __ldg(&lup_first[(long long)rr * S.cols + cc]); };
+        const GvfSums g = gvf_walk(sample, lfirst, true, r, c, S.rows, S.cols, offs, face, own, gs);
+        for (int d = 0; d < 5; ++d) {
+            lup[d] = g.lup[d];
+            alb[d] = g.alb[d];
+            nosh[d] = g.nosh[d];
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 5; ++d) lup[d] = alb[d] = nosh[d] = 0.f;
+        const float inv_first = 1.f / first, inv_first1 = 1.f / (first + 1);
+        const float inv_second = 1.f / second, inv_second1 = 1.f / (second + 1);
+        const bool interior = row0 >= 0 && col0 >= 0 && row0 + TY + 2 * H <= S.rows &&
+                              col0 + pitch <= S.cols;
+        for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
+            const bool fj = (face >> j) & 1u;
+            const GvfDir d = interior
+                ? gvf_direction<true>(own_cell, delta + j * second, offs + j * second, r, c, S.rows,
+                                      S.cols, own_ground, first, second, inv_first, inv_first1,
+                                      inv_second, inv_second1, lwall, albedo_b, fj)
+                : gvf_direction<false>(own_cell, delta + j * second, offs + j * second, r, c, S.rows,
+                                       S.cols, own_ground, first, second, inv_first, inv_first1,
+                                       inv_second, inv_second1, lwall, albedo_b, fj);
+            const unsigned groups = gvf_direction_groups(j);
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+                if (groups & (1u << k)) {
+                    lup[k] += d.lup;
+                    alb[k] += d.alb;
+                    nosh[k] += d.nosh * (own_ground ? 1.f : 0.f);
+                }
+        }
+        // own-pixel corrections, added once per direction in the reference
+        const float ob = own_ground ? 1.f : 0.f;
+        for (int k = 0; k < 5; ++k) {
+            const float cnt = k == 0 ? 18.f : 9.f;
+            lup[k] += cnt * (own.y * (1.f - ob));
+            alb[k] += cnt * (own.z * (1.f - ob) * own.x);
+            nosh[k] += cnt * (own.z * (1.f - ob));
+        }
+    }
+    const double ambient = kSBC * (double)S.emis[p] * pow4(ta + 273.15);
+    for (int k = 0; k < 5; ++k) {
+        const float div = k == 0 ? 18.f : 9.f;
+        gvf[(long long)k * n + p] = (float)((double)(lup[k] / div) + ambient);
+        gvf[(long long)(5 + k) * n + p] = alb[k] / div;
+        gvf[(long long)(10 + k) * n + p] = nosh[k] / div;
+    }
+}
+
+size_t gvf_smem_bytes(int halo, int ty) {
+    return (sizeof(int) + sizeof(int2)) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS +
+           sizeof(float4) * (size_t)(32 + 2 * halo) * (ty + 2 * halo);
+}
+
 template <bool Day, bool Cardinal>
 __device__ __forceinline__ void radiation_body(
     const SolweigScene& S, const SolweigSkyLayout& L, const SolweigHour& h, const SolweigState& st,
-    const SolweigOutputs& out, const StepGvfArgs& ga, const float4* __restrict__ quad,
-    const float* __restrict__ lup_first) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    PatchSmem& ps = *reinterpret_cast<PatchSmem*>(smem_raw);
-    int2* offs = reinterpret_cast<int2*>(smem_raw + sizeof(PatchSmem));
-    float4* tile = reinterpret_cast<float4*>(
-        smem_raw + ((sizeof(PatchSmem) + sizeof(int2) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS + 15) & ~size_t(15)));
-    const int H = ga.halo;
-    const int pitch = kStepBX + 2 * H;
-    const int row0 = blockIdx.y * kStepBY - H, col0 = blockIdx.x * kStepBX - H;
+    const SolweigOutputs& out, const float4* __restrict__ quad, const float* __restrict__ gvfp) {
+    __shared__ PatchSmem ps;
     stage_patches(ps, L, h);
-    if (Day) {
-        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-        for (int i = tid; i < SOLWEIG_GVF_DIRECTIONS * ga.second; i += blockDim.x * blockDim.y)
-            offs[i] = ga.offs[i];
-        load_quad_tile(tile, pitch, kStepBY + 2 * H, quad, S.rows, S.cols, row0, col0);
-    }
     __syncthreads();
     const int c = blockIdx.x * kStepBX + threadIdx.x;
     const int r = blockIdx.y * kStepBY + threadIdx.y;
@@ -118,27 +201,12 @@ __device__ __forceinline__ void radiation_body(
     double kdown = 0.0, kside = 0.0, kside_i = 0.0, kside_d = 0.0, d_rad = 0.0;
     double shadow = 0.0, tg = 0.0, tg_out = ta;
     if (Day) {
-        const float4 own = tile[(threadIdx.y + H) * pitch + threadIdx.x + H];
-        shadow = own.x;
-        GvfScalars gs;
-        gs.lwall = (float)(kSBC * ewall * pow4(h.tgwall + ta + 273.15) - kSBC * ewall * pow4(tk));
-        gs.albedo_b = (float)albedo_b;
-        gs.first = ga.first;
-        gs.second = ga.second;
-        auto sample = [&](int rr, int cc) -> float4 {
-            return tile[(rr - row0) * pitch + (cc - col0)];
-        };
-        auto lfirst = [&](int rr, int cc) -> float {
-            return __ldg(&lup_first[(long long)rr * S.cols + cc]);
-        };
-        const GvfSums g = gvf_walk(sample, lfirst, S.has_water != 0 && lup_first != nullptr, r, c,
-                                   S.rows, S.cols, offs, S.gvf_face[p], own, gs);
+        shadow = quad[p].x;
         double gvf_lup[5], gvf_alb[5], gvf_nosh[5];
         for (int d = 0; d < 5; ++d) {
-            const double div = d == 0 ? 18.0 : 9.0;
-            gvf_lup[d] = (double)g.lup[d] / div + ambient;
-            gvf_alb[d] = (double)g.alb[d] / div;
-            gvf_nosh[d] = (double)g.nosh[d] / div;
+            gvf_lup[d] = gvfp[(long long)d * n + p];
+            gvf_alb[d] = gvfp[(long long)(5 + d) * n + p];
+            gvf_nosh[d] = gvfp[(long long)(10 + d) * n + p];
         }
         // Thermal lag of the upwelling longwave (state: Tgmap1, E, S, W, N).
         float* state[5] = {st.tgmap1, st.tgmap1e, st.tgmap1s, st.tgmap1w, st.tgmap1n};
@@ -285,19 +353,15 @@ __device__ __forceinline__ void radiation_body(
 template <bool Cardinal>
 __global__ void __launch_bounds__(kStepBX* kStepBY) step_radiation_kernel(
     SolweigScene S, const SolweigSkyLayout* __restrict__ L, const SolweigHour* __restrict__ hours,
-    int hour, SolweigState st, SolweigOutputs out, StepGvfArgs ga, const float4* __restrict__ quad,
-    const float* __restrict__ lup_first) {
+    int hour, SolweigState st, SolweigOutputs out, const float4* __restrict__ quad,
+    const float* __restrict__ gvfp) {
     const SolweigHour& h = hours[hour];
     if (h.daytime)
-        radiation_body<true, Cardinal>(S, *L, h, st, out, ga, quad, lup_first);
+        radiation_body<true, Cardinal>(S, *L, h, st, out, quad, gvfp);
     else
-        radiation_body<false, Cardinal>(S, *L, h, st, out, ga, quad, lup_first);
+        radiation_body<false, Cardinal>(S, *L, h, st, out, quad, gvfp);
 }
 
-size_t radiation_smem_bytes(int halo) {
-    const size_t head = (sizeof(PatchSmem) + sizeof(int2) * SOLWEIG_GVF_DIRECTIONS * SOLWEIG_GVF_MAX_STEPS + 15) & ~size_t(15);
-    return head + sizeof(float4) * (size_t)(kStepBX + 2 * halo) * (kStepBY + 2 * halo);
-}
 
 }  // namespace solweig
 
@@ -346,42 +410,70 @@ extern "C" int solweig_step_shadow(const SolweigScene* scene, const SolweigHour*
     return SOLWEIG_OK;
 }
 
-extern "C" int solweig_step_radiation(const SolweigScene* scene, const SolweigSkyLayout* layout,
-                                      const SolweigHour* hours, int hour, const SolweigState* state,
-                                      const SolweigOutputs* out, const int32_t* gvf_dxdy,
-                                      int first_steps, int second_steps, const float* scratch,
-                                      void* stream) {
+// scratch layout [20][pixels]: quad (4 planes as float4), lup_first (1), gvf (15)
+static inline float4* scratch_quad(float* scratch) { return reinterpret_cast<float4*>(scratch); }
+static inline float* scratch_lup_first(float* scratch, long long n) { return scratch + 4 * n; }
+static inline float* scratch_gvf(float* scratch, long long n) { return scratch + 5 * n; }
+
+extern "C" int solweig_step_gvf(const SolweigScene* scene, const SolweigHour* hours, int hour,
+                                const int32_t* gvf_dxdy, int first_steps, int second_steps,
+                                float* scratch, int tile_rows, void* stream) {
     int rc = check_scene(scene);
     if (rc) return rc;
-    SOLWEIG_CHECK_ARG(layout && hours && hour >= 0 && state && out && scratch && gvf_dxdy,
+    SOLWEIG_CHECK_ARG(hours && hour >= 0 && scratch && gvf_dxdy, "solweig_step_gvf: bad arguments");
+    SOLWEIG_CHECK_ARG(second_steps >= 1 && second_steps <= SOLWEIG_GVF_MAX_STEPS && first_steps >= 1 &&
+                          first_steps <= second_steps,
+                      "solweig_step_gvf: GVF steps first=%d second=%d", first_steps, second_steps);
+    SOLWEIG_CHECK_ARG(tile_rows == 8 || tile_rows == 16 || tile_rows == 4,
+                      "solweig_step_gvf: tile_rows must be 4, 8 or 16");
+    const SolweigScene& S = *scene;
+    const long long n = (long long)S.rows * S.cols;
+    StepGvfArgs ga{reinterpret_cast<const int2*>(gvf_dxdy), first_steps, second_steps,
+                   second_steps - 1};
+    const size_t smem = gvf_smem_bytes(ga.halo, tile_rows);
+    SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "solweig_step_gvf: GVF halo %d too large", ga.halo);
+    const float* lup_first = S.has_water ? scratch_lup_first(scratch, n) : nullptr;
+    cudaStream_t st = as_stream(stream);
+    dim3 grid(blocks_for(S.cols, 32), blocks_for(S.rows, tile_rows));
+    if (tile_rows == 4) {
+        set_smem_once((const void*)step_gvf_kernel<4>, smem);
+        step_gvf_kernel<4><<<grid, dim3(32, 4), smem, st>>>(S, hours, hour, ga, scratch_quad(scratch),
+                                                            lup_first, scratch_gvf(scratch, n));
+    } else if (tile_rows == 8) {
+        set_smem_once((const void*)step_gvf_kernel<8>, smem);
+        step_gvf_kernel<8><<<grid, dim3(32, 8), smem, st>>>(S, hours, hour, ga, scratch_quad(scratch),
+                                                            lup_first, scratch_gvf(scratch, n));
+    } else {
+        set_smem_once((const void*)step_gvf_kernel<16>, smem);
+        step_gvf_kernel<16><<<grid, dim3(32, 16), smem, st>>>(S, hours, hour, ga, scratch_quad(scratch),
+                                                              lup_first, scratch_gvf(scratch, n));
+    }
+    SOLWEIG_CHECK_LAUNCH("step_gvf_kernel");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_step_radiation(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                      const SolweigHour* hours, int hour, const SolweigState* state,
+                                      const SolweigOutputs* out, float* scratch, void* stream) {
+    int rc = check_scene(scene);
+    if (rc) return rc;
+    SOLWEIG_CHECK_ARG(layout && hours && hour >= 0 && state && out && scratch,
                       "solweig_step_radiation: null argument");
     SOLWEIG_CHECK_ARG(state->tgmap1 && state->tgmap1e && state->tgmap1s && state->tgmap1w &&
                           state->tgmap1n && state->tgout1,
                       "solweig_step_radiation: state has a null plane");
-    SOLWEIG_CHECK_ARG(second_steps >= 1 && second_steps <= SOLWEIG_GVF_MAX_STEPS && first_steps >= 1 &&
-                          first_steps <= second_steps,
-                      "solweig_step_radiation: GVF steps first=%d second=%d", first_steps,
-                      second_steps);
     const SolweigScene& S = *scene;
+    const long long n = (long long)S.rows * S.cols;
     const bool full = out->least || out->lsouth || out->lwest || out->lnorth;
     dim3 block(kStepBX, kStepBY);
     dim3 grid(blocks_for(S.cols, kStepBX), blocks_for(S.rows, kStepBY));
-    StepGvfArgs ga{reinterpret_cast<const int2*>(gvf_dxdy), first_steps, second_steps,
-                   second_steps - 1};
-    const size_t smem = radiation_smem_bytes(ga.halo);
-    SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "solweig_step_radiation: GVF halo %d too large", ga.halo);
-    const float4* quad = reinterpret_cast<const float4*>(scratch);
-    const float* lup_first = S.has_water ? scratch + 4 * (long long)S.rows * S.cols : nullptr;
     cudaStream_t st = as_stream(stream);
-    if (full) {
-        set_smem_once((const void*)step_radiation_kernel<true>, smem);
-        step_radiation_kernel<true><<<grid, block, smem, st>>>(S, layout, hours, hour, *state, *out,
-                                                               ga, quad, lup_first);
-    } else {
-        set_smem_once((const void*)step_radiation_kernel<false>, smem);
-        step_radiation_kernel<false><<<grid, block, smem, st>>>(S, layout, hours, hour, *state, *out,
-                                                                ga, quad, lup_first);
-    }
+    if (full)
+        step_radiation_kernel<true><<<grid, block, 0, st>>>(S, layout, hours, hour, *state, *out,
+                                                           scratch_quad(scratch), scratch_gvf(scratch, n));
+    else
+        step_radiation_kernel<false><<<grid, block, 0, st>>>(S, layout, hours, hour, *state, *out,
+                                                            scratch_quad(scratch), scratch_gvf(scratch, n));
     SOLWEIG_CHECK_LAUNCH("step_radiation_kernel");
     return SOLWEIG_OK;
 }
@@ -392,8 +484,9 @@ extern "C" int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* l
                             int second_steps, float* scratch, void* stream) {
     int rc = solweig_step_shadow(scene, hours, hour, scratch, stream);
     if (rc) return rc;
-    return solweig_step_radiation(scene, layout, hours, hour, state, out, gvf_dxdy, first_steps,
-                                  second_steps, scratch, stream);
+    rc = solweig_step_gvf(scene, hours, hour, gvf_dxdy, first_steps, second_steps, scratch, 8, stream);
+    if (rc) return rc;
+    return solweig_step_radiation(scene, layout, hours, hour, state, out, scratch, stream);
 }
 
 extern "C" int solweig_day(const SolweigScene* scene, const SolweigSkyLayout* layout,

@@ -592,9 +592,11 @@ class DayRunner:
         dev = scene.device
         self.state = {k: torch.zeros(scene.shape, dtype=torch.float32, device=dev)
                       for k in _lib.STATE_FIELDS}
-        self.scratch = torch.empty((5, scene.rows, scene.cols), dtype=torch.float32, device=dev)
+        self.scratch = torch.empty((_lib.SCRATCH_PLANES, scene.rows, scene.cols), dtype=torch.float32,
+                                   device=dev)
         self.buffers = HourBuffers(scene, 24)
         self.layout_dev = scene.layout.device(dev)
+        self.gvf_tile_rows = 8
 
     def state_struct(self):
         s = _lib.SolweigState()
@@ -659,25 +661,34 @@ class DayRunner:
         o = outputs_struct(out)
         st = self.state_struct()
         L = _lib.lib()
-        times = {"step_shadow_kernel": [], "step_radiation_kernel": []}
+        names = ("step_shadow_kernel", "step_gvf_kernel", "step_radiation_kernel")
+        times = {k: [] for k in names}
         for i, (h, ray, _) in enumerate(plan):
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             ev[0].record()
             if h.daytime:
                 _lib.check(L.solweig_step_shadow(ctypes.byref(sc.struct), self.buffers.ptr(), i,
                                                  device_ptr(self.scratch), stream_handle()), "shadow")
             ev[1].record()
+            if h.daytime:
+                _lib.check(L.solweig_step_gvf(ctypes.byref(sc.struct), self.buffers.ptr(), i,
+                                              device_ptr(sc.gvf_dxdy), sc.first_steps, sc.second_steps,
+                                              device_ptr(self.scratch), self.gvf_tile_rows,
+                                              stream_handle()), "gvf")
+            ev[2].record()
             _lib.check(L.solweig_step_radiation(
                 ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), i,
-                ctypes.byref(st), ctypes.byref(o), device_ptr(sc.gvf_dxdy), sc.first_steps,
-                sc.second_steps, device_ptr(self.scratch), stream_handle()), "radiation")
-            ev[2].record()
+                ctypes.byref(st), ctypes.byref(o), device_ptr(self.scratch), stream_handle()),
+                "radiation")
+            ev[3].record()
             times["step_shadow_kernel"].append((ev, 0, 1, bool(h.daytime)))
-            times["step_radiation_kernel"].append((ev, 1, 2, True))
+            times["step_gvf_kernel"].append((ev, 1, 2, bool(h.daytime)))
+            times["step_radiation_kernel"].append((ev, 2, 3, True))
         self.buffers.mark()
         torch.cuda.synchronize()
         n = sc.pixels
         bytes_per = {"step_shadow_kernel": n * SHADOW_BYTES_PER_PIXEL,
+                     "step_gvf_kernel": n * GVF_BYTES_PER_PIXEL,
                      "step_radiation_kernel": n * RADIATION_BYTES_PER_PIXEL}
         res = {}
         for k, lst in times.items():
@@ -690,8 +701,10 @@ class DayRunner:
 # Algorithmic HBM bytes per pixel and launch (each input and output once):
 # shadow: own dsm/vegdem/vegdem2/walls/aspect (40) + flags (1) + tgk/tstart/tmaxlst/emis/alb (20)
 #         + quad written (16);
-# radiation: quad (16) + flags (1) + emis/tgk/tstart/tmaxlst (16) + svfbuveg (4) + svfalfa and
-#         tan(asvf) (16) + masks (40) + vegetation/obstruction sums (16) + sky band counts (8)
-#         + wall-face bits (4) + thermal state read+write (48) + Tmrt and UTCI written (8).
+# gvf: quad (16) + wall-face bits (4) + emissivity (4) + 15 planes written (60);
+# radiation: shadow from the quad (4) + 15 GVF planes (60) + flags (1) + emis/tgk/tstart/tmaxlst
+#         (16) + svfbuveg (4) + svfalfa and tan(asvf) (16) + masks (40) + vegetation/obstruction
+#         sums (16) + sky band counts (8) + thermal state read+write (48) + Tmrt and UTCI (8).
 SHADOW_BYTES_PER_PIXEL = 77
-RADIATION_BYTES_PER_PIXEL = 177
+GVF_BYTES_PER_PIXEL = 84
+RADIATION_BYTES_PER_PIXEL = 221

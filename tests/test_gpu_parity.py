@@ -116,3 +116,55 @@ def test_batched_graph_matches_plain_and_replays(scene48):
         tm = b["tmrt"].cpu().numpy()
         for h in range(24):
             assert np.max(np.abs(tm[h] - want[h]["Tmrt"])) <= 0.1, (doy, h)
+
+
+@pytest.mark.parametrize("tile_rows", [4, 8, 16])
+def test_step_gvf_planes_match_oracle(cuda, tile_rows):
+    """The hourly GVF kernel (interior fast path and border path) against the
+    oracle's gvf_2018a restatement for the same shadow and surface temperature."""
+    import ctypes
+    import torch
+    from oracle import geometry as G, ground as GR
+    from solweig_cuda_b200 import _lib, engine, synthetic
+    from solweig_cuda_b200.engine import device_ptr, stream_handle
+    sc = synthetic.make_scene(100, seed=9)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    runner = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    runner.gvf_tile_rows = tile_rows
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    plan = engine.plan_day(scene, met, 53.0, 0.0, 3.0, 0.0)
+    i = 13
+    h, ray, scal = plan[i]
+    runner.buffers.put(0, h, ray)
+    runner.buffers.upload(0, 1, runner.buffers.kmax)
+    L = _lib.lib()
+    _lib.check(L.solweig_step_shadow(ctypes.byref(scene.struct), runner.buffers.ptr(), 0,
+                                     device_ptr(runner.scratch), stream_handle()), "shadow")
+    _lib.check(L.solweig_step_gvf(ctypes.byref(scene.struct), runner.buffers.ptr(), 0,
+                                  device_ptr(scene.gvf_dxdy), scene.first_steps, scene.second_steps,
+                                  device_ptr(runner.scratch), tile_rows, stream_handle()), "gvf")
+    torch.cuda.synchronize()
+    got = runner.scratch[5:20].cpu().numpy()
+    n = scene.pixels
+    quad = runner.scratch.reshape(-1)[:4 * n].reshape(scene.rows, scene.cols, 4).permute(2, 0, 1).cpu().numpy()
+    # oracle with the GPU's own shadow value (float32) and the oracle's Tg
+    s = __import__("oracle.step", fromlist=["prepare_static"]).prepare_static(
+        sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover,
+        walls=scene.walls_host, aspect=scene.aspect_host,
+        svf=None)
+    a = s["dsm"]
+    vegsh, sh, _, wallsh, wallsun, wallshve, _, _ = G.shadow_sweep(
+        a, s["vegdem"], s["vegdem2"], h.azimuth, h.altitude, 1.0, s["amaxvalue"], s["bush"],
+        s["walls"], s["dirwalls"] * np.pi / 180.)
+    shadow = sh - (1 - vegsh) * (1 - h.psi)
+    assert np.max(np.abs(quad[0] - shadow)) < 1e-6
+    frac = h.dectime_frac
+    Tg = (s["TgK"] * h.altmax + s["Tstart"]) * np.sin(((frac - h.snup / 24) / (s["TmaxLST"] / 24 - h.snup / 24)) * np.pi / 2)
+    Tg = Tg * h.ci_tgg
+    Tg[Tg < 0] = 0
+    planes, _ = GR.gvf(wallsun, s["walls"], s["buildings"], 1.0, shadow, 1.0, 22.0, s["dirwalls"], Tg,
+                       h.tgwall, h.ta, s["emis_grid"], 0.9, s["alb_grid"], 5.67051e-8, 0.2)
+    order = [0, 3, 6, 9, 12, 1, 4, 7, 10, 13, 2, 5, 8, 11, 14]
+    for k, j in enumerate(order):
+        err = np.max(np.abs(got[k] - planes[j]) / (np.abs(planes[j]) + 1.0))
+        assert err < 2e-5, (k, err)
