@@ -214,14 +214,16 @@ int solweig_gvf(const SolweigScene* scene, const float* shadow, const double* wa
  * the shadow and GVF kernels return at once. */
 int solweig_step_shadow(const SolweigScene* scene, const SolweigHour* hours, int hour,
                         float* scratch, void* stream);
-/* Ground view factors of the hour into scratch (tile_rows: 4, 8 or 16 rows per block). */
+/* Ground view factors of the hour into scratch (tile_rows: 4, 8 or 16 rows per
+ * block).  gvf_dxdy_host: HOST array [18][second_steps][2] of step offsets; it is
+ * folded into the kernel parameters (uniform constant-bank reads). */
 int solweig_step_gvf(const SolweigScene* scene, const SolweigHour* hours, int hour,
-                     const int32_t* gvf_dxdy, int first_steps, int second_steps, float* scratch,
-                     int tile_rows, void* stream);
+                     const int32_t* gvf_dxdy_host, int first_steps, int second_steps,
+                     float* scratch, int tile_rows, void* stream);
 int solweig_step_radiation(const SolweigScene* scene, const SolweigSkyLayout* layout,
                            const SolweigHour* hours, int hour, const SolweigState* state,
                            const SolweigOutputs* out, float* scratch, void* stream);
-/* Both kernels of one hour. */
+/* All kernels of one hour (gvf_dxdy: host array as for solweig_step_gvf). */
 int solweig_step(const SolweigScene* scene, const SolweigSkyLayout* layout,
                  const SolweigHour* hours, int hour, const SolweigState* state,
                  const SolweigOutputs* out, const int32_t* gvf_dxdy, int first_steps,

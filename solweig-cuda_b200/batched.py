@@ -58,7 +58,7 @@ class BatchedDay:
         stride = sc.pixels
         _lib.check(_lib.lib().solweig_day(
             ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
-            ctypes.byref(self._state_struct()), ctypes.byref(base), stride, device_ptr(sc.gvf_dxdy),
+            ctypes.byref(self._state_struct()), ctypes.byref(base), stride, sc.gvf_host_ptr,
             sc.first_steps, sc.second_steps, device_ptr(self.scratch), stream_handle()),
             "solweig_day")
 

@@ -338,6 +338,7 @@ class Scene:
         self.planes = planes if keep_planes else None
         self.gvf_dxdy_host, self.first_steps, self.second_steps = rays.gvf_offsets(self.scale)
         self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
+        self.gvf_host_ptr = self.gvf_dxdy_host.ctypes.data_as(ctypes.c_void_p)
         self.struct = self._make_struct()
 
     def _make_struct(self):
@@ -612,7 +613,7 @@ class DayRunner:
         sc = self.scene
         _lib.check(_lib.lib().solweig_step(
             ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), slot,
-            ctypes.byref(self.state_struct()), ctypes.byref(out_struct), device_ptr(sc.gvf_dxdy),
+            ctypes.byref(self.state_struct()), ctypes.byref(out_struct), sc.gvf_host_ptr,
             sc.first_steps, sc.second_steps, device_ptr(self.scratch), stream_handle(stream)),
             "solweig_step")
 
@@ -672,7 +673,7 @@ class DayRunner:
             ev[1].record()
             if h.daytime:
                 _lib.check(L.solweig_step_gvf(ctypes.byref(sc.struct), self.buffers.ptr(), i,
-                                              device_ptr(sc.gvf_dxdy), sc.first_steps, sc.second_steps,
+                                              sc.gvf_host_ptr, sc.first_steps, sc.second_steps,
                                               device_ptr(self.scratch), self.gvf_tile_rows,
                                               stream_handle()), "gvf")
             ev[2].record()

@@ -402,37 +402,156 @@ def metdata(met, latitude, longitude, site_altitude, utc):
     forcing time minus half the forcing step; ``altmax`` is the maximum solar
     altitude of the calendar day found by a 15-minute search starting at
     10:15 local time; zenith angles in (89, 90] degrees are clamped to 89.
+    All sun positions of the table (rows and altmax candidates) go through one
+    vectorised SPA evaluation.
     """
     met = np.asarray(met, dtype=np.float64)
     n = met.shape[0]
     dectime = met[:, 1] + met[:, 2] / 24 + met[:, 3] / (60 * 24.)
     half = 0 if n == 1 else (dectime[1] - dectime[0]) / 2.
     out = {k: np.empty(n) for k in ("year", "altitude", "azimuth", "zen", "jday", "leafon", "altmax")}
-    sunmaximum = 0.
+    day0s = [_dt.datetime(int(met[i, 0]), 1, 1) + _dt.timedelta(int(met[i, 1]) - 1) for i in range(n)]
+    starts = [i for i in range(n) if i == 0 or np.mod(dectime[i], np.floor(dectime[i])) == 0]
+    K = 96  # 15-minute candidates after 10:00 (24 h)
+    fields = []
+    for i in starts:
+        fifteen = 0.
+        for _ in range(K):
+            fifteen = fifteen + 15. / 1440.
+            fields.append(_datetime_fields(day0s[i] + _dt.timedelta(days=(60 * 10) / 1440.0 + fifteen)))
     for i in range(n):
-        day0 = _dt.datetime(int(met[i, 0]), 1, 1) + _dt.timedelta(int(met[i, 1]) - 1)
-        if i == 0 or np.mod(dectime[i], np.floor(dectime[i])) == 0:
-            fifteen = 0.
-            sunmaximum = -90.
-            zenith_max = 90.
-            while sunmaximum <= 90. - zenith_max:
-                sunmaximum = 90. - zenith_max
-                fifteen = fifteen + 15. / 1440.
-                stamp = day0 + _dt.timedelta(days=(60 * 10) / 1440.0 + fifteen)
-                zenith_max, _ = sun_position(*_datetime_fields(stamp), 0, utc,
-                                             latitude, longitude, site_altitude)
-        out["altmax"][i] = sunmaximum
-        stamp = (day0 + _dt.timedelta(hours=met[i, 2]) + _dt.timedelta(minutes=met[i, 3])
+        stamp = (day0s[i] + _dt.timedelta(hours=met[i, 2]) + _dt.timedelta(minutes=met[i, 3])
                  - _dt.timedelta(days=half))
-        zenith, azimuth = sun_position(*_datetime_fields(stamp), 0, utc, latitude, longitude, site_altitude)
+        fields.append(_datetime_fields(stamp))
+    f = np.asarray(fields, dtype=np.int64)
+    zen_all, azi_all = sun_positions(f[:, 0], f[:, 1], f[:, 2], f[:, 3], f[:, 4], utc, latitude,
+                                     longitude, site_altitude)
+    altmax_of = {}
+    for s_i, i in enumerate(starts):
+        zc = zen_all[s_i * K:(s_i + 1) * K]
+        sunmaximum, zenith_max = -90., 90.
+        k = 0
+        while sunmaximum <= 90. - zenith_max:
+            sunmaximum = 90. - zenith_max
+            if k < K:
+                zenith_max = float(zc[k])
+            else:  # beyond the precomputed candidates: continue one by one
+                stamp = day0s[i] + _dt.timedelta(days=(60 * 10) / 1440.0 + (k + 1) * 15. / 1440.)
+                zenith_max, _ = sun_position(*_datetime_fields(stamp), 0, utc, latitude, longitude,
+                                             site_altitude)
+            k += 1
+        altmax_of[i] = sunmaximum
+    base = len(starts) * K
+    current = None
+    for i in range(n):
+        if i in altmax_of:
+            current = altmax_of[i]
+        out["altmax"][i] = current
+        zenith = float(zen_all[base + i])
+        azimuth = float(azi_all[base + i])
         if 89.0 < zenith <= 90.0:
             zenith = 89.0
         out["altitude"][i] = 90. - zenith
         out["azimuth"][i] = azimuth
         out["zen"][i] = zenith * (np.pi / 180.)
         out["year"][i] = met[i, 0]
-        doy = day0.timetuple().tm_yday
+        doy = day0s[i].timetuple().tm_yday
         out["jday"][i] = doy
         out["leafon"][i] = 1 if (doy > 97) | (doy < 300) else 0
-        _ = calendar.isleap(stamp.year)
     return SolarHours(dectime=dectime, **out)
+
+
+def _series_rows(table, jme):
+    """Row-wise periodic-term sums for a vector of JME (one row per time)."""
+    return np.sum(table[None, :, 0] * np.cos(table[None, :, 1] + (table[None, :, 2] * jme[:, None])), axis=1)
+
+
+def _wrap_vec(value, period):
+    value = value - period * np.floor(value / period)
+    return np.where(value < 0, value + period, value)
+
+
+def _julian_vec(year, month, day, hour, minute, utc):
+    year = np.asarray(year, dtype=np.int64)
+    month = np.asarray(month, dtype=np.int64)
+    early = (month == 1) | (month == 2)
+    y = np.where(early, year - 1, year).astype(np.float64)
+    m = np.where(early, month + 12, month).astype(np.float64)
+    ut = ((np.asarray(hour, dtype=np.float64) - utc) / 24) + (np.asarray(minute, dtype=np.float64) / (60 * 24)) + (0 / (60 * 60 * 24))
+    d = np.asarray(day, dtype=np.float64) + ut
+    a = np.floor(y / 100)
+    b = 2 - a + np.floor(a / 4)
+    julian_cal = (year < 1582) | ((year == 1582) & ((month < 10) | ((month == 10) & (np.asarray(day) <= 4))))
+    b = np.where(julian_cal, 0.0, b)
+    jd = d + b + np.floor(365.25 * (y + 4716)) + np.floor(30.6001 * (m + 1)) - 1524.5
+    jc = (jd - 2451545) / 36525
+    return jd, jc, jc, jc / 10
+
+
+def sun_positions(year, month, day, hour, minute, utc, latitude, longitude, altitude):
+    """Vectorised :func:`sun_position` over arrays of calendar fields.
+
+    Same operations as the scalar version, row by row; the periodic-term sums
+    reduce along the contiguous axis, so they use the same summation order.
+    """
+    jd, jc, jce, jme = _julian_vec(year, month, day, hour, minute, utc)
+    l_terms = [_series_rows(t, jme) for t in (_L0, _L1, _L2, _L3, _L4)]
+    l5 = _L5[0, 0] * np.cos(_L5[0, 1] + (_L5[0, 2] * jme))
+    helio_lon = (l_terms[0] + (l_terms[1] * jme) + (l_terms[2] * np.power(jme, 2))
+                 + (l_terms[3] * np.power(jme, 3)) + (l_terms[4] * np.power(jme, 4))
+                 + (l5 * np.power(jme, 5))) / 1e8
+    helio_lon = _wrap_vec(helio_lon * 180 / np.pi, 360)
+    b0, b1 = _series_rows(_B0, jme), _series_rows(_B1, jme)
+    helio_lat = _wrap_vec(((b0 + (b1 * jme)) / 1e8) * 180 / np.pi, 360)
+    r_terms = [_series_rows(t, jme) for t in (_R0, _R1, _R2, _R3)]
+    r4 = _R4[0, 0] * np.cos(_R4[0, 1] + (_R4[0, 2] * jme))
+    radius = (r_terms[0] + (r_terms[1] * jme) + (r_terms[2] * np.power(jme, 2))
+              + (r_terms[3] * np.power(jme, 3)) + (r4 * np.power(jme, 4))) / 1e8
+    geo_lon = _wrap_vec(helio_lon + 180, 360)
+    geo_lat = _wrap_vec(-helio_lat, 360)
+    x = np.stack([c3 * np.power(jce, 3) + c2 * np.power(jce, 2) + c1 * jce + c0
+                  for (c3, c2, c1, c0) in _NUT_X], axis=1)          # (T, 5)
+    arg = x.dot(np.transpose(_NUT_Y)) * (np.pi / 180)               # (T, 63)
+    d_psi = np.sum((_NUT_PE[None, :, 0] + (_NUT_PE[None, :, 1] * jce[:, None])) * np.sin(arg), axis=1) / 36000000
+    d_eps = np.sum((_NUT_PE[None, :, 2] + (_NUT_PE[None, :, 3] * jce[:, None])) * np.cos(arg), axis=1) / 36000000
+    u = jme / 10
+    p = _OBLIQUITY
+    eps0 = (p[0] * np.power(u, 10) + p[1] * np.power(u, 9) + p[2] * np.power(u, 8)
+            + p[3] * np.power(u, 7) + p[4] * np.power(u, 6) + p[5] * np.power(u, 5)
+            + p[6] * np.power(u, 4) + p[7] * np.power(u, 3) + p[8] * np.power(u, 2)
+            + p[9] * u + p[10])
+    eps = (eps0 / 3600) + d_eps
+    aberration = -20.4898 / (3600 * radius)
+    lam = geo_lon + d_psi + aberration
+    nu0 = (280.46061837 + (360.98564736629 * (jd - 2451545)) + (0.000387933 * np.power(jc, 2))
+           - (np.power(jc, 3) / 38710000))
+    nu0 = _wrap_vec(nu0, 360)
+    nu = nu0 + (d_psi * np.cos(eps * np.pi / 180))
+    num = (np.sin(lam * np.pi / 180) * np.cos(eps * np.pi / 180)) - \
+          (np.tan(geo_lat * np.pi / 180) * np.sin(eps * np.pi / 180))
+    alpha = _wrap_vec(np.arctan2(num, np.cos(lam * np.pi / 180)) * 180 / np.pi, 360)
+    delta = np.arcsin((np.sin(geo_lat * np.pi / 180) * np.cos(eps * np.pi / 180))
+                      + (np.cos(geo_lat * np.pi / 180) * np.sin(eps * np.pi / 180)
+                         * np.sin(lam * np.pi / 180))) * 180 / np.pi
+    hour_angle = _wrap_vec(nu + longitude - alpha, 360)
+    xi = 8.794 / (3600 * radius)
+    uu = np.arctan(0.99664719 * np.tan(latitude * np.pi / 180))
+    xx = np.cos(uu) + ((altitude / 6378140) * np.cos(latitude * np.pi / 180))
+    yy = (0.99664719 * np.sin(uu)) + ((altitude / 6378140) * np.sin(latitude * np.pi / 180))
+    d_alpha = np.arctan2(-xx * np.sin(xi * np.pi / 180) * np.sin(hour_angle * np.pi / 180),
+                         np.cos(delta * np.pi / 180)
+                         - (xx * np.sin(xi * np.pi / 180) * np.cos(hour_angle * np.pi / 180)))
+    delta_t = np.arctan2((np.sin(delta * np.pi / 180) - (yy * np.sin(xi * np.pi / 180))) * np.cos(d_alpha),
+                         np.cos(delta * np.pi / 180)
+                         - (yy * np.sin(xi * np.pi / 180)) * np.cos(hour_angle * np.pi / 180)) * 180 / np.pi
+    h_t = hour_angle - d_alpha * 180 / np.pi
+    e0 = np.arcsin((np.sin(latitude * np.pi / 180) * np.sin(delta_t * np.pi / 180))
+                   + (np.cos(latitude * np.pi / 180) * np.cos(delta_t * np.pi / 180)
+                      * np.cos(h_t * np.pi / 180))) * 180 / np.pi
+    refraction = 1.02 / (60 * np.tan((e0 + (10.3 / (e0 + 5.11))) * np.pi / 180))
+    zenith = 90 - (e0 + refraction)
+    azimuth = (np.arctan2(np.sin(h_t * np.pi / 180),
+                          (np.cos(h_t * np.pi / 180) * np.sin(latitude * np.pi / 180))
+                          - (np.tan(delta_t * np.pi / 180) * np.cos(latitude * np.pi / 180)))
+               * 180 / np.pi) + 180
+    return zenith, _wrap_vec(azimuth, 360)

@@ -141,7 +141,7 @@ def test_step_gvf_planes_match_oracle(cuda, tile_rows):
     _lib.check(L.solweig_step_shadow(ctypes.byref(scene.struct), runner.buffers.ptr(), 0,
                                      device_ptr(runner.scratch), stream_handle()), "shadow")
     _lib.check(L.solweig_step_gvf(ctypes.byref(scene.struct), runner.buffers.ptr(), 0,
-                                  device_ptr(scene.gvf_dxdy), scene.first_steps, scene.second_steps,
+                                  scene.gvf_host_ptr, scene.first_steps, scene.second_steps,
                                   device_ptr(runner.scratch), tile_rows, stream_handle()), "gvf")
     torch.cuda.synchronize()
     got = runner.scratch[5:20].cpu().numpy()
