@@ -192,6 +192,15 @@ int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
                 const uint8_t* sectors /* [patches] bit d: E,S,W,N */,
                 double transmissivity, uint32_t* masks, double* planes,
                 float* veg_sums, uint8_t* sky_band_counts, void* stream);
+/* Annulus sums of packed masks (the reduce half of solweig_svf). */
+int solweig_svf_reduce(const uint32_t* masks, const double* vegdem2, int64_t pixels,
+                       const SolweigSkyLayout* layout, const double* band_weights,
+                       const uint8_t* sectors, double transmissivity, double* planes,
+                       float* veg_sums, uint8_t* sky_band_counts, void* stream);
+/* Pack the reference's float cubes [rows][cols][patches] (shmat, vegshmat,
+ * vbshvegshmat) into S/V words (src/model.py:273-284 packs them into bytes). */
+int solweig_svf_pack(const float* shmat, const float* vegmat, const float* vbmat, int64_t pixels,
+                     int patches, uint32_t* masks, void* stream);
 /* Expand packed masks to the reference's float cubes [rows][cols][patches]. */
 int solweig_svf_unpack(const uint32_t* masks, int64_t pixels, int patches,
                        float* shmat, float* vegmat, float* vbmat, void* stream);
@@ -258,6 +267,10 @@ int solweig_scene_finalize(const double* planes, const double* walls, const doub
 int solweig_utci(const float* ta, const float* rh, const float* tmrt, const float* va,
                  int ta_scalar, int rh_scalar, int va_scalar, float* out, int64_t n,
                  void* stream);
+/* Scalar weather for the whole raster (src/kernels/utci.cu:243-523): the
+ * polynomial is collapsed on the host and evaluated per pixel in (Tmrt - Ta). */
+int solweig_utci_scalar(double ta, double rh, double va, const float* tmrt, float* out, int64_t n,
+                        void* stream);
 /* Host function: UTCI as a polynomial in D = Tmrt - Ta for scalar weather,
  * coefficients[0..6] (all zero when an input is the -999 sentinel). */
 int solweig_utci_collapse(double ta, double rh, double va, double* coefficients);

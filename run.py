@@ -1,0 +1,120 @@
+"""Command line of the B200 engine, mirroring the reference's ``run.py``.
+
+    python run.py --case case.json [--output DIR] [--dtype float32|float64]
+                  [--output-core ROW COL ROWS COLS] [--output-chunk-steps N]
+                  [--sync-output] [--output-queue-size N] [--no-write] [--progress]
+
+Case keys follow the reference's ``examples/case.json`` (paths relative to the
+case file).  Rasters are ``.npy`` arrays (GeoTIFF where rasterio/GDAL is
+installed).  ``case_type: open_data`` needs network downloads and is not
+supported; ``core_area_m`` / ``buffer_area_m`` tile the rasters with halos.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+from datetime import datetime
+from pathlib import Path
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+PATH_KEYS = {"building_dsm_path", "tree_path", "dem_path", "met_file", "building_geometry_path",
+             "building_height_path", "landcover_path", "output_path"}
+PREPARATION_KEYS = {"case_name", "case_type", "case_size_m", "core_area_m", "buffer_area_m",
+                    "resolution_m", "start_date", "end_date"}
+
+
+def load_case(path):
+    """Case dict and preparation settings (``run.py:70-86`` of the reference)."""
+    path = Path(path).resolve()
+    case = json.loads(path.read_text(encoding="utf-8-sig"))
+    settings = {key: case.pop(key) for key in PREPARATION_KEYS if key in case}
+    settings.setdefault("case_type", "local")
+    settings.setdefault("resolution_m", 1)
+    for key in PATH_KEYS & case.keys():
+        value = case[key]
+        if value is None:
+            continue
+        entries = value if isinstance(value, list) else [value]
+        resolved = [str((path.parent / Path(e).expanduser()).resolve()) for e in entries]
+        case[key] = resolved if isinstance(value, list) else resolved[0]
+    case.setdefault("async_output", True)
+    case.setdefault("output_queue_size", 2)
+    case.setdefault("output_chunk_steps", 24)
+    return case, settings
+
+
+def _tile_jobs(case, settings):
+    if "core_area_m" not in settings:
+        return [(settings.get("case_name", "tile"), dict(case), None)]
+    import numpy as np
+    from solweig_cuda_b200.series import load_raster
+    from solweig_cuda_b200 import tiling
+    res = float(settings.get("resolution_m", 1))
+    core, halo = (int(round(settings[k] / res)) for k in ("core_area_m", "buffer_area_m"))
+    rasters = {k: load_raster(case[k]) for k in ("building_dsm_path", "tree_path", "dem_path")}
+    if case.get("landcover_path"):
+        rasters["landcover_path"] = load_raster(case["landcover_path"])
+    h, w = rasters["building_dsm_path"].shape
+    jobs = []
+    for t in tiling.tile_windows(h, w, core=core, halo=halo):
+        opts = dict(case)
+        for k, arr in rasters.items():
+            opts[k] = np.ascontiguousarray(tiling.extract(arr, t))
+        opts["output_core"] = t["output_core"]
+        jobs.append((t["tile_id"], opts, t))
+    return jobs
+
+
+def main(argv=None):
+    parser = argparse.ArgumentParser(description="Run SOLWEIG on the GPU for the supplied rasters and forcing.")
+    parser.add_argument("--case", type=Path, required=True)
+    parser.add_argument("--output", type=Path)
+    parser.add_argument("--dtype", choices=("float32", "float64"), default="float32")
+    parser.add_argument("--output-core", type=int, nargs=4, metavar=("ROW", "COL", "ROWS", "COLS"))
+    parser.add_argument("--output-chunk-steps", type=int)
+    parser.add_argument("--sync-output", action="store_true")
+    parser.add_argument("--output-queue-size", type=int)
+    parser.add_argument("--no-write", action="store_true")
+    parser.add_argument("--progress", action=argparse.BooleanOptionalAction, default=True)
+    args = parser.parse_args(argv)
+    case_path = args.case.resolve()
+    case, settings = load_case(case_path)
+    if settings["case_type"] == "open_data":
+        missing = [k for k in ("building_dsm_path", "tree_path", "dem_path", "met_file")
+                   if not Path(case[k]).exists()]
+        if missing:
+            raise SystemExit(f"open_data preparation (network download) is not supported; missing: {missing}")
+    if args.output_core is not None:
+        case["output_core"] = args.output_core
+    if args.output_chunk_steps is not None:
+        case["output_chunk_steps"] = args.output_chunk_steps
+    if args.sync_output:
+        case["async_output"] = False
+    if args.output_queue_size is not None:
+        case["output_queue_size"] = args.output_queue_size
+    output = Path(case.pop("output_path", case_path.parent / "output"))
+    output = (args.output or output).resolve()
+    import numpy as np
+    from solweig_cuda_b200.series import load_meteorology, run_timeseries
+    forcing = load_meteorology(case["met_file"])
+    case["met_file"] = forcing
+    for label, options, tile in _tile_jobs(case, settings):
+        dest = output / label if tile is not None else output
+        known = {"building_dsm_path", "tree_path", "dem_path", "met_file", "longitude", "latitude",
+                 "landcover_path", "utc_offset_hours", "site_altitude_m", "output_core",
+                 "output_chunk_steps", "async_output", "output_queue_size"}
+        kwargs = {k: v for k, v in options.items() if k in known}
+        run_timeseries(output_path=dest, dtype=np.dtype(args.dtype), no_write=args.no_write,
+                       progress=args.progress, pixel_size=float(settings.get("resolution_m", 1)), **kwargs)
+    if args.progress and not args.no_write:
+        print(f"[{datetime.now():%H:%M:%S}] Results: {output}", flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -93,7 +93,8 @@ EXPORTED_SYMBOLS = (
     "solweig_shadow", "solweig_svf", "solweig_svf_unpack", "solweig_diffsh", "solweig_gvf",
     "solweig_step", "solweig_utci", "solweig_utci_collapse", "solweig_scene_build",
     "solweig_scene_finalize", "solweig_struct_sizes", "solweig_step_shadow",
-    "solweig_step_radiation", "solweig_day", "solweig_step_gvf",
+    "solweig_step_radiation", "solweig_day", "solweig_step_gvf", "solweig_utci_scalar",
+    "solweig_svf_pack", "solweig_svf_reduce",
 )
 
 _lock = threading.Lock()
@@ -125,6 +126,9 @@ def _declare(lib):
                                       P, P, P]),
         "solweig_scene_finalize": (i32, [P, P, P, i64, dbl, P, P, P, P, P, P, P, P, P]),
         "solweig_struct_sizes": (i32, [P]),
+        "solweig_utci_scalar": (i32, [dbl, dbl, dbl, P, P, i64, P]),
+        "solweig_svf_pack": (i32, [P, P, P, i64, i32, P, P]),
+        "solweig_svf_reduce": (i32, [P, P, i64, P, P, P, dbl, P, P, P, P]),
         "solweig_step_shadow": (i32, [P, P, i32, P, P]),
         "solweig_step_gvf": (i32, [P, P, i32, P, i32, i32, P, i32, P]),
         "solweig_step_radiation": (i32, [P, P, P, i32, P, P, P, P]),

@@ -162,6 +162,28 @@ __global__ void __launch_bounds__(256) svf_unpack_kernel(const uint32_t* __restr
     if (vbm) vbm[i] = (!S && V) ? 0.f : 1.f;
 }
 
+// Reference float cubes [pixels][patches] -> packed S/V words.
+__global__ void __launch_bounds__(256) svf_pack_kernel(const float* __restrict__ shm,
+                                                       const float* __restrict__ vegm,
+                                                       const float* __restrict__ vbm,
+                                                       long long pixels, int patches,
+                                                       uint32_t* __restrict__ masks) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+        uint32_t s = 0, v = 0;
+        for (int b = 0; b < 32; ++b) {
+            const int k = w * 32 + b;
+            if (k >= patches) break;
+            const long long i = p * patches + k;
+            if (shm[i] == 1.0f) s |= 1u << b;
+            if (vegm[i] == 0.0f || vbm[i] == 0.0f) v |= 1u << b;
+        }
+        masks[(long long)w * pixels + p] = s;
+        masks[(long long)(SOLWEIG_MASK_WORDS + w) * pixels + p] = v;
+    }
+}
+
 __global__ void __launch_bounds__(256) diffsh_kernel(const float* __restrict__ sh,
                                                      const float* __restrict__ veg,
                                                      float* __restrict__ out, long long n,
@@ -174,6 +196,52 @@ __global__ void __launch_bounds__(256) diffsh_kernel(const float* __restrict__ s
 }  // namespace solweig
 
 using namespace solweig;
+
+extern "C" int solweig_svf_reduce(const uint32_t* masks, const double* vegdem2, int64_t pixels,
+                                  const SolweigSkyLayout* layout, const double* band_weights,
+                                  const uint8_t* sectors, double transmissivity, double* planes,
+                                  float* veg_sums, uint8_t* sky_band_counts, void* stream) {
+    SOLWEIG_CHECK_ARG(masks && vegdem2 && layout && band_weights && sectors && planes && veg_sums &&
+                          sky_band_counts && pixels > 0,
+                      "solweig_svf_reduce: bad arguments");
+    SOLWEIG_CHECK_ARG(layout->nbands > 0 && layout->nbands <= SOLWEIG_MAX_BANDS &&
+                          layout->patches > 0 && layout->patches <= SOLWEIG_MASK_WORDS * 32,
+                      "solweig_svf_reduce: bad layout");
+    const int patches = layout->patches;
+    cudaStream_t st = as_stream(stream);
+    SvfReduceParams q{};
+    q.pixels = pixels;
+    q.nbands = layout->nbands;
+    q.trans = transmissivity;
+    for (int k = 0; k < patches; ++k) {
+        const int b = layout->band_of_patch[k];
+        SOLWEIG_CHECK_ARG(b >= 0 && b < layout->nbands, "solweig_svf: bad band of patch %d", k);
+        q.band_mask[b][k >> 5] |= 1u << (k & 31);
+        for (int d = 0; d < 4; ++d)
+            if (sectors[k] & (1u << d)) q.sector_mask[d][k >> 5] |= 1u << (k & 31);
+    }
+    for (int b = 0; b < layout->nbands; ++b) {
+        q.wf[b] = band_weights[2 * b];
+        q.wa[b] = band_weights[2 * b + 1];
+        q.w_cos[b] = (double)layout->band_omega[b] * (double)layout->band_cos[b];
+        q.w_sin[b] = (double)layout->band_omega[b] * (double)layout->band_sin[b];
+    }
+    svf_reduce_kernel<<<blocks_for(pixels, 256), 256, 0, st>>>(masks, vegdem2, q, planes, veg_sums,
+                                                               sky_band_counts);
+    SOLWEIG_CHECK_LAUNCH("svf_reduce_kernel");
+    return SOLWEIG_OK;
+}
+
+extern "C" int solweig_svf_pack(const float* shmat, const float* vegmat, const float* vbmat,
+                                int64_t pixels, int patches, uint32_t* masks, void* stream) {
+    SOLWEIG_CHECK_ARG(shmat && vegmat && vbmat && masks && pixels > 0 && patches > 0 &&
+                          patches <= SOLWEIG_MASK_WORDS * 32,
+                      "solweig_svf_pack: bad arguments");
+    svf_pack_kernel<<<blocks_for(pixels, 256), 256, 0, as_stream(stream)>>>(shmat, vegmat, vbmat,
+                                                                           pixels, patches, masks);
+    SOLWEIG_CHECK_LAUNCH("svf_pack_kernel");
+    return SOLWEIG_OK;
+}
 
 extern "C" int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
                            const uint8_t* flags, int rows, int cols, int patches, int capacity,
@@ -205,27 +273,8 @@ extern "C" int solweig_svf(const double* dsm, const double* vegdem, const double
         dsm, vegdem, vegdem2, flags, rp, reinterpret_cast<const int2*>(ray_dxdy), ray_dz, lengths,
         masks);
     SOLWEIG_CHECK_LAUNCH("svf_visibility_kernel");
-    SvfReduceParams q{};
-    q.pixels = pixels;
-    q.nbands = layout->nbands;
-    q.trans = transmissivity;
-    for (int k = 0; k < patches; ++k) {
-        const int b = layout->band_of_patch[k];
-        SOLWEIG_CHECK_ARG(b >= 0 && b < layout->nbands, "solweig_svf: bad band of patch %d", k);
-        q.band_mask[b][k >> 5] |= 1u << (k & 31);
-        for (int d = 0; d < 4; ++d)
-            if (sectors[k] & (1u << d)) q.sector_mask[d][k >> 5] |= 1u << (k & 31);
-    }
-    for (int b = 0; b < layout->nbands; ++b) {
-        q.wf[b] = band_weights[2 * b];
-        q.wa[b] = band_weights[2 * b + 1];
-        q.w_cos[b] = (double)layout->band_omega[b] * (double)layout->band_cos[b];
-        q.w_sin[b] = (double)layout->band_omega[b] * (double)layout->band_sin[b];
-    }
-    svf_reduce_kernel<<<blocks_for(pixels, 256), 256, 0, st>>>(masks, vegdem2, q, planes, veg_sums,
-                                                               sky_band_counts);
-    SOLWEIG_CHECK_LAUNCH("svf_reduce_kernel");
-    return SOLWEIG_OK;
+    return solweig_svf_reduce(masks, vegdem2, pixels, layout, band_weights, sectors, transmissivity,
+                              planes, veg_sums, sky_band_counts, stream);
 }
 
 extern "C" int solweig_svf_unpack(const uint32_t* masks, int64_t pixels, int patches, float* shmat,

@@ -114,9 +114,48 @@ __global__ void __launch_bounds__(256) utci_kernel(const float* __restrict__ ta,
     out[i] = (float)utci_poly(DevTable{}, t, w, m - t, pa);
 }
 
+// Scalar weather: UTCI(Tmrt) = sum_k c_k (Tmrt - Ta)^k by Horner's rule.
+struct UtciPoly {
+    double c[7];
+    double ta;
+    int valid;
+};
+
+__global__ void __launch_bounds__(256) utci_poly_kernel(UtciPoly poly, const float* __restrict__ tmrt,
+                                                        float* __restrict__ out, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double m = tmrt[i];
+    if (!poly.valid || m <= -999.0) {
+        out[i] = -999.0f;
+        return;
+    }
+    const double d = m - poly.ta;
+    double u = poly.c[6];
+#pragma unroll
+    for (int k = 5; k >= 0; --k) u = u * d + poly.c[k];
+    out[i] = (float)u;
+}
+
 }  // namespace solweig
 
 using namespace solweig;
+
+extern "C" int solweig_utci_collapse(double ta, double rh, double va, double* coefficients);
+
+extern "C" int solweig_utci_scalar(double ta, double rh, double va, const float* tmrt, float* out,
+                                   int64_t n, void* stream) {
+    SOLWEIG_CHECK_ARG(tmrt && out && n >= 0, "solweig_utci_scalar: bad arguments");
+    if (n == 0) return SOLWEIG_OK;
+    UtciPoly poly{};
+    poly.ta = ta;
+    poly.valid = !(ta <= -999.0 || rh <= -999.0 || va <= -999.0);
+    int rc = solweig_utci_collapse(ta, rh, va, poly.c);
+    if (rc) return rc;
+    utci_poly_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(poly, tmrt, out, n);
+    SOLWEIG_CHECK_LAUNCH("utci_poly_kernel");
+    return SOLWEIG_OK;
+}
 
 extern "C" int solweig_utci_collapse(double ta, double rh, double va, double* coefficients) {
     SOLWEIG_CHECK_ARG(coefficients, "solweig_utci_collapse: null output");

@@ -122,6 +122,20 @@ def _upload(arr, dtype, device):
     return torch.from_numpy(np.ascontiguousarray(arr, dtype=dtype)).to(device, non_blocking=False)
 
 
+def _as_device(x, dtype, device, shape):
+    """Any array-like (numpy, torch, __cuda_array_interface__, scalar) as a
+    contiguous device tensor of ``shape`` (scalars are broadcast)."""
+    if isinstance(x, torch.Tensor):
+        t = x.to(device=device, dtype=dtype)
+    elif hasattr(x, "__cuda_array_interface__"):
+        t = torch.as_tensor(x, device=device).to(dtype)
+    else:
+        t = torch.as_tensor(np.asarray(x), dtype=dtype).to(device)
+    if t.dim() == 0 or t.numel() == 1:
+        t = t.reshape(()).expand(shape)
+    return t.reshape(shape).contiguous()
+
+
 def _aspect_templates(pixel_size):
     """Flattened template offset lists for ``solweig_wall_aspect`` (``src/walls.py:24-56``)."""
     from scipy.ndimage import rotate
@@ -340,6 +354,101 @@ class Scene:
         self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
         self.gvf_host_ptr = self.gvf_dxdy_host.ctypes.data_as(ctypes.c_void_p)
         self.struct = self._make_struct()
+
+    @classmethod
+    def from_inputs(cls, inputs, device="cuda", stream=None):
+        """Build a scene from the reference's prepared inputs (the ``static``
+        dict of ``src/series.py:350-365`` handed to ``prepare_model``): DSM
+        fields, walls/aspect, land-cover grids, the derived SVF fields and the
+        three [rows, cols, P] visibility cubes."""
+        _require_cuda()
+        self = cls.__new__(cls)
+        dev = torch.device(device)
+        self.device = dev
+        rows, cols = int(inputs["rows"]), int(inputs["cols"])
+        self.shape = (rows, cols)
+        self.rows, self.cols = rows, cols
+        self.pixels = rows * cols
+        self.scale = float(inputs["scale"])
+        self.pixel_size = 1.0 / self.scale
+        self.patch_option = int(inputs.get("patch_option", 2))
+        self.layout = SkyLayout(self.patch_option)
+        L = _lib.lib()
+        st = stream_handle(stream)
+
+        def f64(x):
+            return _as_device(x, torch.float64, dev, self.shape)
+
+        def f32(x):
+            return _as_device(x, torch.float32, dev, self.shape)
+
+        self.dsm = f64(inputs["dsm"])
+        self.vegdem = f64(inputs["vegdem"])
+        self.vegdem2 = f64(inputs["vegdem2"])
+        self.walls = f64(inputs["walls"])
+        dirwalls = f64(inputs["dirwalls"])
+        self.aspect = (dirwalls * np.pi / 180.).contiguous()
+        self.walls_host = self.walls.cpu().numpy()
+        self.aspect_host = dirwalls.cpu().numpy()
+        bush = f64(inputs["bush"])
+        buildings = f64(inputs["buildings"])
+        lc = f64(inputs.get("lc_grid", 0.0))
+        self.flags = ((buildings == 1).to(torch.uint8) | ((bush > 1).to(torch.uint8) << 1)
+                      | ((lc == 3).to(torch.uint8) << 2)).contiguous()
+        self.landcover = int(inputs.get("landcover", 0))
+        self.has_water = int(bool(((self.flags & 4) != 0).any().item())) if self.landcover else 0
+        self.alb = f32(inputs["alb_grid"])
+        self.emis = f32(inputs["emis_grid"])
+        self.tgk = f32(inputs["TgK"])
+        self.tstart = f32(inputs["Tstart"])
+        self.tmaxlst = f32(inputs["TmaxLST"])
+        self.lc_grid = f32(lc)
+        self.tgk_wall = float(inputs["TgK_wall"])
+        self.tstart_wall = float(inputs["Tstart_wall"])
+        self.tmaxlst_wall = float(inputs["TmaxLST_wall"])
+        self.amaxvalue = float(inputs["amaxvalue"])
+        self.dsm_max = float(self.dsm.max().item())
+        self.hmax = float(max(self.dsm_max, self.vegdem.max().item(), self.vegdem2.max().item()))
+        self.svfbuveg = f32(inputs["svfbuveg"])
+        self.svfalfa = f64(inputs["svfalfa"])
+        self.tan_asvf = torch.tan(f64(inputs["asvf"])).contiguous()
+        P = self.layout.struct.patches
+        cubes = [_as_device(inputs[k], torch.float32, dev, self.shape + (P,))
+                 for k in ("shmat", "vegshmat", "vbshvegshmat")]
+        self.masks = torch.empty((2 * _lib.MASK_WORDS, rows, cols), dtype=torch.int32, device=dev)
+        _lib.check(L.solweig_svf_pack(device_ptr(cubes[0]), device_ptr(cubes[1]), device_ptr(cubes[2]),
+                                      self.pixels, P, device_ptr(self.masks), st), "solweig_svf_pack")
+        nb = self.layout.struct.nbands
+        planes = torch.empty((16, rows, cols), dtype=torch.float64, device=dev)
+        self.veg_sums = torch.empty((4, rows, cols), dtype=torch.float32, device=dev)
+        self.sky_band_counts = torch.empty((nb, rows, cols), dtype=torch.uint8, device=dev)
+        lay = self.layout
+        _lib.check(L.solweig_svf_reduce(
+            device_ptr(self.masks), device_ptr(self.vegdem2), self.pixels, ctypes.byref(lay.struct),
+            lay.band_weights.ctypes.data_as(ctypes.c_void_p), lay.sectors.ctypes.data_as(ctypes.c_void_p),
+            CONSTANTS["transVeg"], device_ptr(planes), device_ptr(self.veg_sums),
+            device_ptr(self.sky_band_counts), st), "solweig_svf_reduce")
+        self.planes = None
+        svf_names = cls.SVF_ORDER
+        self.svf32 = torch.stack([f32(inputs[k]) for k in svf_names])
+        # GVF wall-face bits (finalize computes them together with SVF-derived
+        # fields; only the face bits are kept here, the fields come from inputs)
+        scratch = {k: torch.empty(self.shape, dtype=t, device=dev) for k, t in
+                   (("svfbuveg", torch.float32), ("svfalfa", torch.float64), ("tan", torch.float64))}
+        self.gvf_face = torch.empty(self.shape, dtype=torch.int32, device=dev)
+        lo, hi, mid = rays.gvf_face_windows()
+        _lib.check(L.solweig_scene_finalize(
+            device_ptr(planes), device_ptr(self.walls), device_ptr(self.aspect), self.pixels,
+            CONSTANTS["transVeg"], lo.ctypes.data_as(ctypes.c_void_p), hi.ctypes.data_as(ctypes.c_void_p),
+            mid.ctypes.data_as(ctypes.c_void_p), None, device_ptr(scratch["svfbuveg"]),
+            device_ptr(scratch["svfalfa"]), device_ptr(scratch["tan"]), device_ptr(self.gvf_face), st),
+            "solweig_scene_finalize")
+        first, second = float(inputs.get("first", 1.0)), float(inputs.get("second", 22.0))
+        self.gvf_dxdy_host, self.first_steps, self.second_steps = rays.gvf_offsets(self.scale, first, second)
+        self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
+        self.gvf_host_ptr = self.gvf_dxdy_host.ctypes.data_as(ctypes.c_void_p)
+        self.struct = self._make_struct()
+        return self
 
     def _make_struct(self):
         s = _lib.SolweigScene()
