@@ -243,6 +243,26 @@ int solweig_day(const SolweigScene* scene, const SolweigSkyLayout* layout,
                 const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
                 int first_steps, int second_steps, float* scratch, void* stream);
 
+/* solweig_step without a scratch argument -- no counterpart in the reference.
+ * For callers that cannot allocate device memory: a host model that owns its
+ * arrays but no device allocator for temporaries, or that must not call
+ * cudaMalloc/cudaFree inside its time loop (cudaFree synchronises the device).
+ * The [20][pixels] scratch lives in a file-scope static device array of
+ * SOLWEIG_STEP_SCRATCH_PLANES x SOLWEIG_STATIC_SCRATCH_MAX_PIXELS floats
+ * (20 MiB); tiles above SOLWEIG_STATIC_SCRATCH_MAX_PIXELS pixels are rejected
+ * with SOLWEIG_ERR_INVALID.  Nothing is allocated.  The first call on each
+ * device (with that device current) looks the array's address up once; make
+ * that first call before any stream capture.  The array is shared by every
+ * call on a device: two calls that overlap in time (different streams or
+ * host threads) race on it and must be serialised by the caller.  Nothing in
+ * the array has to start at zero. */
+#define SOLWEIG_STEP_SCRATCH_PLANES 20
+#define SOLWEIG_STATIC_SCRATCH_MAX_PIXELS (512 * 512)
+int solweig_step_static_scratch(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                const SolweigHour* hours, int hour, const SolweigState* state,
+                                const SolweigOutputs* out, const int32_t* gvf_dxdy,
+                                int first_steps, int second_steps, void* stream);
+
 /* Static scene preparation (src/series.py:252-349) ------------------------- */
 /* classes: [nclasses][6] (code, albedo, emissivity, TgK, Tstart, TmaxLST);
  * defaults: albedo, emissivity, TgK, Tstart, TmaxLST without land cover;

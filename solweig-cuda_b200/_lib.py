@@ -20,6 +20,7 @@ MAX_BANDS = 8
 GVF_DIRECTIONS = 18
 GVF_MAX_STEPS = 64
 SCRATCH_PLANES = 20  # quad (4) + first-direction Lup (1) + 15 GVF planes
+STATIC_SCRATCH_MAX_PIXELS = 512 * 512  # capacity of solweig_step_static_scratch
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -94,7 +95,7 @@ EXPORTED_SYMBOLS = (
     "solweig_step", "solweig_utci", "solweig_utci_collapse", "solweig_scene_build",
     "solweig_scene_finalize", "solweig_struct_sizes", "solweig_step_shadow",
     "solweig_step_radiation", "solweig_day", "solweig_step_gvf", "solweig_utci_scalar",
-    "solweig_svf_pack", "solweig_svf_reduce",
+    "solweig_svf_pack", "solweig_svf_reduce", "solweig_step_static_scratch",
 )
 
 _lock = threading.Lock()
@@ -119,6 +120,7 @@ def _declare(lib):
         "solweig_diffsh": (i32, [P, P, P, i64, fl, P]),
         "solweig_gvf": (i32, [P, P, P, P, dbl, dbl, dbl, dbl, dbl, P, i32, i32, P, P, P]),
         "solweig_step": (i32, [P, P, P, i32, P, P, P, i32, i32, P, P]),
+        "solweig_step_static_scratch": (i32, [P, P, P, i32, P, P, P, i32, i32, P]),
         "solweig_day": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, P]),
         "solweig_utci": (i32, [P, P, P, P, i32, i32, i32, P, i64, P]),
         "solweig_utci_collapse": (i32, [dbl, dbl, dbl, P]),
