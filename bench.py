@@ -41,7 +41,7 @@ def _args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("solweig", "reference"), default="solweig")
     p.add_argument("--size", type=int, default=2000)
-    p.add_argument("--form", choices=("plain", "batched"), default="batched")
+    p.add_argument("--form", choices=("plain", "batched", "chosen"), default="chosen")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -219,7 +219,12 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
 
     plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
-    chosen = batched.BatchedDay(scene, 53.0, 0.0, 3.0, 0.0) if a.form == "batched" else plain
+    if a.form == "chosen":
+        chosen = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+    elif a.form == "batched":
+        chosen = batched.BatchedDay(scene, 53.0, 0.0, 3.0, 0.0)
+    else:
+        chosen = plain
 
     def day(runner):
         return runner.run_day(met, outputs=("tmrt", "utci"))
@@ -242,7 +247,8 @@ def main():
             times.append(s.elapsed_time(e))
         return times
 
-    launches_per_day = 3 * len(met)  # shadow, GVF and radiation kernel per hour
+    # our kernels per timed day: 7 for the batched form, shadow/GVF/radiation per hour otherwise
+    launches_per_day = 7 if a.form == "chosen" else 3 * len(met)
     plain_times = timed(plain, max(1, min(a.steps, 3)), 1)
     with ClockSampler(local) as clocks:
         chosen_times = timed(chosen, a.steps, a.warmup)

@@ -243,6 +243,37 @@ int solweig_day(const SolweigScene* scene, const SolweigSkyLayout* layout,
                 const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
                 int first_steps, int second_steps, float* scratch, void* stream);
 
+/* Batched day ----------------------------------------------------------------
+ * All nhours (<= 64) hours of one day (src/series.py:445-491) in seven
+ * launches: shadow sweep and ground view factors for every hour (one launch
+ * each), the luminance-weighted sky / vegetation patch sums of all hours as
+ * one BF16 tensor-core contraction (tcgen05, FP32 accumulation, weights split
+ * into BF16 hi + lo), per-hour sunlit/shaded tables, and one radiation launch
+ * whose threads loop over the hours with the wave-delay state in registers.
+ * Outputs as solweig_day (plane of hour h at base + h * hour_stride); the
+ * cardinal planes (keast..lnorth) must be NULL.  State: tgmap1 and tgout1 are
+ * read at the start and written at the end (the four cardinal state planes
+ * are not used: their sum is 4 x tgmap1 for any state the model produces).
+ * Sky layouts with 145 or 153 patches.  work: device buffer of
+ * solweig_day_batched_work_bytes() bytes, 256-byte aligned.  A tensor-core
+ * wait that times out sets a device flag read by solweig_day_batched_error. */
+int64_t solweig_day_batched_work_bytes(int rows, int cols, int nhours, int has_water);
+int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                        const SolweigHour* hours, int nhours, const SolweigState* state,
+                        const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                        int first_steps, int second_steps, void* work, int64_t work_bytes,
+                        void* stream);
+/* Copy the device error flag of the last batched day in `work` to out_device. */
+int solweig_day_batched_error(const void* work, int rows, int cols, int nhours, int has_water,
+                              int* out_device, void* stream);
+/* The patch contraction alone: out[c][p] = sum_k sky(p,k) * weights[c][k] for
+ * c < ncols and out[ncols + c][p] = sum_k veg(p,k) * weights[c][k], with
+ * sky = S & ~V and veg = S & V of the packed masks; weights: device float32
+ * [ncols][160] (ncols <= 256), contracted as BF16 hi + lo with FP32
+ * accumulation.  work: >= 4 * 16*ceil(ncols/16) * 160 + 16 bytes, 16-byte aligned. */
+int solweig_patch_sums(const uint32_t* masks, int64_t pixels, int patches, const float* weights,
+                       int ncols, float* out, void* work, int64_t work_bytes, void* stream);
+
 /* solweig_step without a scratch argument -- no counterpart in the reference.
  * For callers that cannot allocate device memory: a host model that owns its
  * arrays but no device allocator for temporaries, or that must not call

@@ -96,6 +96,8 @@ EXPORTED_SYMBOLS = (
     "solweig_scene_finalize", "solweig_struct_sizes", "solweig_step_shadow",
     "solweig_step_radiation", "solweig_day", "solweig_step_gvf", "solweig_utci_scalar",
     "solweig_svf_pack", "solweig_svf_reduce", "solweig_step_static_scratch",
+    "solweig_day_batched", "solweig_day_batched_work_bytes", "solweig_day_batched_error",
+    "solweig_patch_sums",
 )
 
 _lock = threading.Lock()
@@ -121,6 +123,10 @@ def _declare(lib):
         "solweig_gvf": (i32, [P, P, P, P, dbl, dbl, dbl, dbl, dbl, P, i32, i32, P, P, P]),
         "solweig_step": (i32, [P, P, P, i32, P, P, P, i32, i32, P, P]),
         "solweig_step_static_scratch": (i32, [P, P, P, i32, P, P, P, i32, i32, P]),
+        "solweig_day_batched": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P]),
+        "solweig_day_batched_work_bytes": (i64, [i32, i32, i32, i32]),
+        "solweig_day_batched_error": (i32, [P, i32, i32, i32, i32, P, P]),
+        "solweig_patch_sums": (i32, [P, i64, i32, P, i32, P, P, i64, P]),
         "solweig_day": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, P]),
         "solweig_utci": (i32, [P, P, P, P, i32, i32, i32, P, i64, P]),
         "solweig_utci_collapse": (i32, [dbl, dbl, dbl, P]),

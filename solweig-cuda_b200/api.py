@@ -11,20 +11,26 @@ import numpy as np
 import torch
 
 from . import engine
-from .batched import BatchedDay
+from .batched import BatchedDay, ChosenDay
 
 __all__ = ["simulate_day"]
 
 
 def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixel_size=1.0,
-                 site_altitude=3.0, utc=0.0, device="cuda", form="batched"):
-    """Returns {"tmrt": [H, rows, cols] float32, "utci": ..., "h2d_bytes", "d2h_bytes"}."""
+                 site_altitude=3.0, utc=0.0, device="cuda", form="chosen"):
+    """Returns {"tmrt": [H, rows, cols] float32, "utci": ..., "h2d_bytes", "d2h_bytes"}.
+
+    form: "chosen" (batched day, tensor-core patch sums), "batched" (per-hour
+    kernels in one launch sequence) or "plain" (per-hour loop)."""
     arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in (dsm, trees, dem)]
     lc = None if landcover is None else np.ascontiguousarray(landcover, dtype=np.float64)
     h2d = sum(a.nbytes for a in arrays) + (lc.nbytes if lc is not None else 0)
     scene = engine.Scene(arrays[0], arrays[1], arrays[2], pixel_size, landcover=lc, device=device)
     met = np.asarray(met, dtype=np.float64)
-    if form == "batched":
+    if form == "chosen":
+        runner = ChosenDay(scene, latitude, longitude, site_altitude, utc, hours=len(met),
+                           use_graph=False)
+    elif form == "batched":
         runner = BatchedDay(scene, latitude, longitude, site_altitude, utc, hours=len(met),
                             use_graph=False)
     else:

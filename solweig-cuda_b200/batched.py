@@ -17,7 +17,7 @@ import torch
 from . import _lib
 from .engine import HourBuffers, device_ptr, outputs_struct, plan_day, stream_handle
 
-__all__ = ["BatchedDay"]
+__all__ = ["BatchedDay", "ChosenDay"]
 
 
 class BatchedDay:
@@ -91,3 +91,52 @@ class BatchedDay:
         self.buffers.mark()
         names = self.out_names if outputs is None else outputs
         return {k: self.out[k] for k in names}
+
+
+class ChosenDay(BatchedDay):
+    """The batched form: every hour of a day in seven launches
+    (``solweig_day_batched``: per-launch shadow and GVF over all hours, the
+    BF16 tensor-core patch contraction, hour-looping radiation), replayed as
+    one CUDA graph together with the hour-record uploads.
+
+    Produces the all-direction planes (Tmrt, UTCI, Kdown, Kup, Ldown, Lup,
+    Kside, Lside, shadow, Tg ...); the cardinal E/S/W/N planes are only made
+    by the per-hour form."""
+
+    CARDINAL = ("keast", "ksouth", "kwest", "knorth", "least", "lsouth", "lwest", "lnorth")
+
+    def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0, hours=24,
+                 outputs=("tmrt", "utci"), use_graph=True):
+        bad = [o for o in outputs if o in self.CARDINAL]
+        if bad:
+            raise ValueError(f"the batched form does not produce {bad}")
+        super().__init__(scene, latitude, longitude, site_altitude, utc, hours, outputs, use_graph)
+        self.scratch = None
+        L = _lib.lib()
+        self.work_bytes = int(L.solweig_day_batched_work_bytes(scene.rows, scene.cols, hours,
+                                                               int(scene.struct.has_water)))
+        if self.work_bytes <= 0:
+            raise ValueError("bad batched-day shape")
+        self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=scene.device)
+        self.launches_per_day = 7
+
+    def _sequence(self):
+        self.buffers.upload(0, self.hours, self.buffers.kmax)
+        for t in self.state.values():
+            t.zero_()
+        sc = self.scene
+        base = outputs_struct(self.out, 0)
+        _lib.check(_lib.lib().solweig_day_batched(
+            ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
+            ctypes.byref(self._state_struct()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
+            sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes, stream_handle()),
+            "solweig_day_batched")
+
+    def error_flag(self):
+        """Device error flag of the last day (0 = ok, 1 = a tensor-core wait timed out)."""
+        flag = torch.zeros(1, dtype=torch.int32, device=self.scene.device)
+        sc = self.scene
+        _lib.check(_lib.lib().solweig_day_batched_error(
+            device_ptr(self.work), sc.rows, sc.cols, self.hours, int(sc.struct.has_water),
+            device_ptr(flag), stream_handle()), "solweig_day_batched_error")
+        return int(flag.item())

@@ -1,0 +1,62 @@
+// Per-pixel pieces of one SOLWEIG hour shared by the per-hour step
+// (step.cu) and the batched day (day.cu).
+#pragma once
+#include "gvf.cuh"
+#include "shadow.cuh"
+
+namespace solweig {
+
+// Ground temperature amplitude wave of the hour (before the water override).
+__device__ __forceinline__ double ground_tg(const SolweigScene& S, const SolweigHour& h,
+                                            long long p) {
+    const double amp = (double)S.tgk[p] * h.altmax + (double)S.tstart[p];
+    const double phase =
+        ((h.dectime_frac - h.snup / 24.0) / ((double)S.tmaxlst[p] / 24.0 - h.snup / 24.0)) * kPi / 2.0;
+    double tg = amp * sin(phase) * h.ci_tgg;
+    if (S.landcover == 1 && tg < 0.0) tg = 0.0;
+    return tg;
+}
+
+__device__ __forceinline__ double lup_excess(double emis, double tg, double shadow, double ta) {
+    return kSBC * emis * pow4(tg * shadow + ta + 273.15) - kSBC * emis * pow4(ta + 273.15);
+}
+
+// Shadow sweep of pixel (r, c) for hour h and the per-pixel GVF inputs: the
+// float4 quad (shadow, Lup, albedo, ground|sunwall bits) and, for scenes with
+// water, the Lup of the first GVF search direction.
+__device__ __forceinline__ void shadow_quad_pixel(const SolweigScene& S, const SolweigHour& h, int r, int c,
+                                                  float4* __restrict__ quad, float* __restrict__ lup_first) {
+    const long long p = (long long)r * S.cols + c;
+    const double a = S.dsm[p];
+    const double wall = S.walls[p];
+    const uint8_t fl = S.flags[p];
+    const ShadowResult s =
+        shadow_walk(S.dsm, S.vegdem, S.vegdem2, S.rows, S.cols, r, c, a, S.vegdem[p], (fl & 2) != 0,
+                    wall, reinterpret_cast<const int2*>(h.ray_dxdy), h.ray_dz, h.steps, S.hmax, true);
+    // Wall sunlit height (only needed for the sunlit-wall bit of the GVF).
+    const double wallbol = wall > 0.0 ? 1.0 : 0.0;
+    const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);
+    double wallsun = wall - (s.f - a);
+    if (wallsun < 0.0) wallsun = 0.0;
+    if (facesh == 1.0) wallsun = 0.0;
+    const double wallsh = wall - wallsun;
+    double wallshve = (s.topmax - a) * (s.veg ? 1.0 : 0.0) * wallbol - wallsh;
+    if (wallshve < 0.0) wallshve = 0.0;
+    if (wallshve > wall) wallshve = wall;
+    wallsun = wallsun - wallshve;
+    if (wallsun < 0.0) wallsun = 0.0;
+    const double ground = (fl & 1) ? 1.0 : 0.0;
+    const bool sunwall = (wallsun / wall * ground) == 1.0;
+    const double sh = s.shadowed ? 0.0 : 1.0;
+    const double vegsh = s.veg ? 0.0 : 1.0;
+    const double shadow = (double)(float)(sh - (1.0 - vegsh) * (1.0 - h.psi));
+    double tg = ground_tg(S, h, p);
+    const double emis = S.emis[p];
+    if (lup_first) lup_first[p] = (float)lup_excess(emis, tg, shadow, h.ta);
+    if (S.has_water && (fl & 4)) tg = h.twater - h.ta;
+    const float lup = (float)lup_excess(emis, tg, shadow, h.ta);
+    quad[p] = make_float4((float)shadow, lup, S.alb[p],
+                          __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+}
+
+}  // namespace solweig

@@ -158,9 +158,8 @@ __device__ __forceinline__ float utci_eval(const double* c, double tmrt, double 
     return (float)u;
 }
 
-// Fraction of shaded wall, cylindric_wedge (NaN -> 0.5).
-__device__ __forceinline__ double wedge_fsh(double svfalfa, double tan_zen) {
-    const double ta = tan(svfalfa);
+// Fraction of shaded wall, cylindric_wedge (NaN -> 0.5), from ta = tan(svfalfa).
+__device__ __forceinline__ double wedge_fsh_tan(double ta, double tan_zen) {
     const double xa = 1.0 - 2.0 / (ta * tan_zen);
     const double ha = 2.0 / (ta * tan_zen);
     const double ba = 1.0 / ta;
@@ -175,6 +174,10 @@ __device__ __forceinline__ double wedge_fsh(double svfalfa, double tan_zen) {
     }
     const double fsh = (2.0 * kPi * ba - (hkil + ukil)) / (2.0 * kPi * ba);
     return isnan(fsh) ? 0.5 : fsh;
+}
+
+__device__ __forceinline__ double wedge_fsh(double svfalfa, double tan_zen) {
+    return wedge_fsh_tan(tan(svfalfa), tan_zen);
 }
 
 }  // namespace solweig

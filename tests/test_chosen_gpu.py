@@ -1,0 +1,114 @@
+"""The batched form (``solweig_day_batched``): the BF16 tensor-core patch
+contraction against an FP64 reference of the same sums, and whole days
+against the oracle and the per-hour form."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# Patch sums: BF16 hi + lo weights carry ~16 significant bits, FP32 accumulation.
+SUM_RTOL = 2e-5
+TMRT_TOL = 0.1    # K, against the oracle (UMEP restatement)
+UTCI_TOL = 0.05   # K
+FORM_TOL = 0.02   # K, batched vs per-hour form
+
+
+def _sums_reference(S, V, P, W):
+    """FP64 sums of W over the sky (S & ~V) and vegetation (S & V) patches."""
+    px = S.shape[1]
+    bits = np.zeros((px, 160), dtype=np.float64)
+    vbits = np.zeros((px, 160), dtype=np.float64)
+    for w in range(5):
+        for b in range(32):
+            k = 32 * w + b
+            if k >= P:
+                continue
+            s = (S[w] >> b) & 1
+            v = (V[w] >> b) & 1
+            bits[:, k] = s & (1 - v)
+            vbits[:, k] = s & v
+    return bits @ W.T.astype(np.float64), vbits @ W.T.astype(np.float64)
+
+
+@pytest.mark.parametrize("px,ncols", [(128 * 37, 48), (1000, 16), (5 * 128 + 77, 96)])
+def test_patch_sums_match_fp64(cuda, px, ncols):
+    import torch
+    from solweig_cuda_b200 import _lib
+    from solweig_cuda_b200.engine import device_ptr, stream_handle
+    rng = np.random.default_rng(px + ncols)
+    P = 153
+    words = rng.integers(0, 2**32, size=(10, px), dtype=np.uint64).astype(np.uint32)
+    W = rng.uniform(0.0, 0.02, size=(ncols, 160)).astype(np.float32)
+    W[:, P:] = 0
+    masks = torch.from_numpy(words.view(np.int32)).to(cuda)
+    wt = torch.from_numpy(W).to(cuda)
+    out = torch.full((2 * ncols, px), np.nan, dtype=torch.float32, device=cuda)
+    nb = (ncols + 15) // 16 * 16
+    work = torch.empty(4 * nb * 160 + 16, dtype=torch.uint8, device=cuda)
+    L = _lib.lib()
+    _lib.check(L.solweig_patch_sums(device_ptr(masks), px, P, device_ptr(wt), ncols, device_ptr(out),
+                                    device_ptr(work), work.numel(), stream_handle()), "solweig_patch_sums")
+    torch.cuda.synchronize()
+    err = int(work[4 * nb * 160:4 * nb * 160 + 4].view(torch.int32).item())
+    assert err == 0
+    got = out.cpu().numpy().astype(np.float64)
+    sky, veg = _sums_reference(words[:5].astype(np.int64), words[5:].astype(np.int64), P, W)
+    scale = np.abs(W).sum(axis=1)[None, :]  # bound of every sum
+    assert np.all(np.isfinite(got))
+    assert np.max(np.abs(got[:ncols].T - sky) / scale) < SUM_RTOL
+    assert np.max(np.abs(got[ncols:].T - veg) / scale) < SUM_RTOL
+
+
+@pytest.fixture(scope="module")
+def scene64():
+    from solweig_cuda_b200 import engine, synthetic
+    sc = synthetic.make_scene(64, 56, seed=4)
+    return sc, engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+
+
+def test_chosen_day_matches_oracle_and_plain(scene64):
+    import torch
+    from oracle import step as ST
+    from solweig_cuda_b200 import batched, engine, synthetic
+    sc, scene = scene64
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    outs = ("tmrt", "utci", "kdown", "ldown", "lup", "kup", "kside", "lside")
+    chosen = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, outputs=outs)
+    got = {k: v.clone() for k, v in chosen.run_day(met).items()}
+    torch.cuda.synchronize()
+    assert chosen.error_flag() == 0
+    plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    ref = plain.run_day(met, outputs=outs)
+    for k in outs:
+        a = got[k].cpu().numpy()
+        b = ref[k].cpu().numpy()
+        assert np.array_equal(np.isnan(a), np.isnan(b)), k
+        tol = FORM_TOL if k in ("tmrt", "utci") else 0.05  # W/m2 for the fluxes
+        d = np.nanmax(np.abs(a - b))
+        assert d <= tol, (k, d)
+    s = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    want = ST.run_day(s, met, dict(latitude=53.0, longitude=0.0, altitude=3.0), 0.0, outputs=("Tmrt", "UTCI"))
+    tm = got["tmrt"].cpu().numpy()
+    ut = got["utci"].cpu().numpy()
+    for h in range(24):
+        assert np.max(np.abs(tm[h] - want[h]["Tmrt"])) <= TMRT_TOL, h
+        ok = ~np.isnan(want[h]["UTCI"])
+        assert np.max(np.abs(ut[h][ok] - want[h]["UTCI"][ok])) <= UTCI_TOL, h
+
+
+def test_chosen_day_graph_replays_new_forcing(scene64):
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic
+    sc, scene = scene64
+    chosen = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+    plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    for doy, seed in ((172, 0), (200, 5), (350, 2)):
+        met = synthetic.make_met(doy=doy, latitude=53.0, longitude=0.0, seed=seed)
+        b = {k: v.clone() for k, v in chosen.run_day(met).items()}
+        a = plain.run_day(met)
+        torch.cuda.synchronize()
+        d = torch.max(torch.abs(a["tmrt"] - b["tmrt"])).item()
+        assert d <= FORM_TOL, (doy, d)
+    assert chosen.error_flag() == 0
