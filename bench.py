@@ -44,6 +44,11 @@ def _args():
     p.add_argument("--form", choices=("plain", "batched", "chosen"), default="chosen")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=("day", "month", "tiles", "precision"), default="day",
+                   help="day: the headline 2000^2 x 24 h line; month: 2000^2 x 720 h in one graph; "
+                        "tiles: 64 uneven tiles in one graph; precision: 4000^2 patch-sum error report")
+    p.add_argument("--no-tune", dest="tune", action="store_false",
+                   help="skip the launch-shape autotuner (cached per shape) of the batched form")
     return p.parse_args()
 
 
@@ -191,12 +196,180 @@ def _traffic(kernel):
     return None
 
 
+def _events_ms(fn, steps, warmup, flush):
+    """Mean device ms of fn() over `steps` runs after `warmup`, L2 flushed before each."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e))
+    return sum(times) / len(times)
+
+
+def run_month(a):
+    """2000^2 px x 720 h (30 days, state reset daily) as one CUDA-graph replay."""
+    import numpy as np
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic, tune
+    dev = torch.device("cuda", 0)
+    n = a.size
+    sc = synthetic.make_scene(n, seed=0)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, device=dev)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, days=30)
+    day = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+    cfg = tune.apply(day, met[:24]) if a.tune else day.config
+    del day
+    md = batched.MultiDay(scene, 53.0, 0.0, 3.0, 0.0, days=30, config=cfg)
+    t0 = time.perf_counter()
+    md.plan(met)
+    plan_s = time.perf_counter() - t0
+    md.capture()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    with ClockSampler(0) as clocks:
+        ms = _events_ms(md.replay, a.steps, a.warmup, flush)
+    work = n * n * 720
+    print(json.dumps({
+        "metric": "pixel-hours/s Tmrt+UTCI, 2000^2 px x 720 h (30 days) in one CUDA graph",
+        "value": work / (ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "dtype": "f32+f64+bf16", "data": "synthetic",
+        "config": {"workload": f"{n}x{n} px, DOY 172-201, 53N, thermal state reset daily, batched form",
+                   "launch_config": list(cfg.astuple()), "kernel_launches": md.launches,
+                   "host_plan_s_30_days": plan_s, "l2": "flushed before every replay"},
+        "clocks": clocks.summary()}), flush=True)
+
+
+def _tile_specs(count=64):
+    import numpy as np
+    rng = np.random.default_rng(2024)
+    sides = rng.integers(256, 1537, size=count)
+    lats = rng.uniform(35.0, 60.0, size=count)
+    return [(int(sides[i]), int(i + 1), float(lats[i])) for i in range(count)]
+
+
+def run_tiles(a):
+    """64 tiles, sides U{256..1536}, seeds 1-64, latitudes U[35, 60] N, one day each, one graph."""
+    import numpy as np
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic, tune
+    dev = torch.device("cuda", 0)
+    specs = _tile_specs()
+    scenes, mets, lats = [], [], []
+    for side, seed, lat in specs:
+        sc = synthetic.make_scene(side, seed=seed)
+        scenes.append(engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, device=dev))
+        mets.append(synthetic.make_met(doy=172, latitude=lat, longitude=0.0, seed=seed))
+        lats.append(lat)
+    configs = []
+    tuned = {}
+    for s, met, lat in zip(scenes, mets, lats):
+        day = batched.ChosenDay(s, lat, 0.0, 3.0, 0.0)
+        key = tune.tune_key(day)
+        if a.tune and key not in tuned:
+            tuned[key] = tune.apply(day, met)
+        configs.append(tuned.get(key, day.config))
+        del day
+    tb = batched.TileBatch(scenes, lats, [0.0] * len(scenes), configs=configs)
+    tb.plan(mets)
+    tb.capture()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    with ClockSampler(0) as clocks:
+        ms = _events_ms(tb.replay, a.steps, a.warmup, flush)
+    work = tb.pixels * 24
+    print(json.dumps({
+        "metric": "pixel-hours/s Tmrt+UTCI, 64 uneven tiles x 24 h in one CUDA graph",
+        "value": work / (ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "dtype": "f32+f64+bf16", "data": "synthetic",
+        "config": {"workload": "64 tiles, sides U{256..1536} (seed 2024), generator seeds 1-64, "
+                               "latitudes U[35,60] N, DOY 172, batched form",
+                   "pixels": tb.pixels, "tuned_shapes": {k: list(v.astuple()) for k, v in tuned.items()},
+                   "kernel_launches": tb.launches, "l2": "flushed before every replay"},
+        "clocks": clocks.summary()}), flush=True)
+
+
+def run_precision(a):
+    """4000^2 px: the BF16 patch contraction's error against FP64 sums on a pixel
+    sample, and the batched form's Kdown/Ldown/Tmrt against the per-hour FP32 form."""
+    import numpy as np
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic
+    dev = torch.device("cuda", 0)
+    n = 4000 if a.size == 2000 else a.size
+    sc = synthetic.make_scene(n, seed=0)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, device=dev)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    outs = ("tmrt", "kdown", "ldown")
+    day = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, outputs=outs)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    ms = _events_ms(lambda: day.run_day(met), a.steps, a.warmup, flush)
+    stage = day.profile_day(met)
+    got = {k: v.clone() for k, v in day.run_day(met).items()}
+    torch.cuda.synchronize()
+    sums = day.patch_sums()
+    # FP64 reference of the contraction on a pixel sample, all hours
+    rng = np.random.default_rng(7)
+    idx = torch.from_numpy(rng.choice(scene.pixels, size=65536, replace=False)).to(dev)
+    L = scene.layout.host
+    P = L.count
+    words = scene.masks.view(torch.int32).view(10, -1)[:, idx].to(torch.int64) & 0xFFFFFFFF
+    bit = torch.arange(P, device=dev)
+    Sb = (words[bit // 32] >> (bit % 32)[:, None]) & 1
+    Vb = (words[5 + bit // 32] >> (bit % 32)[:, None]) & 1
+    sky = (Sb * (1 - Vb)).to(torch.float64).T
+    veg = (Sb * Vb).to(torch.float64).T
+    W = np.zeros((2 * 24, P))
+    for h, s_ in enumerate(day.last_scalars):
+        if s_.lv is not None:
+            lum = s_.lv[:, 2]
+            W[2 * h] = lum
+            W[2 * h + 1] = lum * L.cos_alt * L.steradian
+    Wt = torch.from_numpy(W).to(dev)
+    ref_sky, ref_veg = sky @ Wt.T, veg @ Wt.T
+    got_sky = sums[0][:, idx].T.to(torch.float64)
+    got_veg = sums[1][:, idx].T.to(torch.float64)
+    scale = Wt.abs().sum(dim=1).clamp_min(1e-30)
+    err_sky = ((got_sky - ref_sky).abs() / scale).max().item()
+    err_veg = ((got_veg - ref_veg).abs() / scale).max().item()
+    abs_sky = (got_sky - ref_sky).abs().max().item()
+    # the per-hour FP32 form (per-patch loop, no tensor cores) beside it
+    plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    ref = plain.run_day(met, outputs=outs)
+    torch.cuda.synchronize()
+    diffs = {k: float(torch.nan_to_num((got[k] - ref[k]).abs(), nan=0.0).max()) for k in outs}
+    gemm_flops = batched.ChosenDay.gemm_flops(scene.pixels, 24, P)
+    print(json.dumps({
+        "metric": "patch-sum contraction error vs FP64 and batched-vs-FP32 differences, 4000^2 px x 24 h",
+        "value": n * n * 24 / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms,
+        "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+        "config": {"workload": f"{n}x{n} px at 1 m, DOY 172, 53N, BF16 hi/lo weights, FP32 accumulation",
+                   "sample_pixels": 65536},
+        "patch_sums_max_rel_error_vs_fp64": {"sky": err_sky, "vegetation": err_veg},
+        "patch_sums_max_abs_error_vs_fp64": abs_sky,
+        "max_abs_diff_vs_fp32_form": diffs,
+        "stages_ms": stage,
+        "patch_gemm_tflops": gemm_flops / (stage["patch_gemm_kernel"] / 1000.0) / 1e12}), flush=True)
+
+
 def main():
     a = _args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if a.impl == "reference":
         run_reference(a, rank, world)
+        return 0
+    if a.workload != "day":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(0)
+            {"month": run_month, "tiles": run_tiles, "precision": run_precision}[a.workload](a)
         return 0
     import numpy as np
     import torch
@@ -221,6 +394,9 @@ def main():
     plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
     if a.form == "chosen":
         chosen = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+        if a.tune:
+            from solweig_cuda_b200 import tune
+            tune.apply(chosen, met)
     elif a.form == "batched":
         chosen = batched.BatchedDay(scene, 53.0, 0.0, 3.0, 0.0)
     else:
@@ -247,6 +423,7 @@ def main():
             times.append(s.elapsed_time(e))
         return times
 
+    sun_alt = __import__("solweig_cuda_b200.sun", fromlist=["metdata"]).metdata(met, 53.0, 0.0, 3.0, 0.0).altitude
     # our kernels per timed day: 7 for the batched form, shadow/GVF/radiation per hour otherwise
     launches_per_day = 7 if a.form == "chosen" else 3 * len(met)
     plain_times = timed(plain, max(1, min(a.steps, 3)), 1)
@@ -263,15 +440,33 @@ def main():
     value_plain = world * work / (ms_plain / 1000.0)
 
     # Per-kernel timing of one instrumented day (events on the launching stream).
-    kern = plain.profile_day(met) if hasattr(plain, "profile_day") else {}
+    peak, peak_kind = _peaks()
+    peak_src = (peak_kind + " (MEASURED_PEAKS.json hbm_gbs)") if peak_kind == "measured" else "fallback"
     roof = None
-    if kern:
+    if a.form == "chosen":
+        stage_ms = chosen.profile_day(met)
+        day_hours = int(sum(1 for x in sun_alt if x > 0))
+        px = n * n
+        bytes_per = batched.ChosenDay.stage_bytes(px, 24, day_hours)
+        stages = {k: {"ms": v, "launches": 1, "bytes_per_launch": bytes_per[k]} for k, v in stage_ms.items()}
+        dom = max(stages, key=lambda k: stages[k]["ms"])
+        info = stages[dom]
+        achieved = info["bytes_per_launch"] / (info["ms"] / 1000.0) / 1e9
+        total = sum(v["ms"] for v in stages.values())
+        gemm_flops = batched.ChosenDay.gemm_flops(px, 24, scene.layout.host.count)
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": _traffic(dom),
+                "launch_ms": info["ms"],
+                "share": {k: round(v["ms"] / total, 4) for k, v in stages.items()},
+                "stages_ms": {k: round(v["ms"], 4) for k, v in stages.items()},
+                "patch_gemm_tflops": gemm_flops / (stage_ms["patch_gemm_kernel"] / 1000.0) / 1e12}
+    else:
+        kern = plain.profile_day(met)
         dom = max(kern, key=lambda k: kern[k]["ms"])
         info = kern[dom]
-        peak, peak_kind = _peaks()
         achieved = info["bytes_per_launch"] / (info["ms"] / info["launches"] / 1000.0) / 1e9
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                 "traffic": _traffic(dom), "launch_ms": info["ms"] / info["launches"],
                 "share": {k: round(v["ms"] / sum(x["ms"] for x in kern.values()), 4) for k, v in kern.items()}}
 

@@ -29,6 +29,7 @@
  *   solweig_step(_shadow,_radiation)
  *                             src/model.py:15-256 (Solweig_2022a_calc, device part)
  *   solweig_day               src/series.py:445-491 (the hour loop of _run_day)
+ *   solweig_day_batched       src/series.py:445-491 (same loop, batched form)
  *   solweig_scene_build/finalize src/series.py:252-349 (_prepare_spatial, per pixel)
  *   solweig_utci              src/utci.py:6-33, src/kernels/utci.cu
  */
@@ -263,6 +264,34 @@ int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layou
                         const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
                         int first_steps, int second_steps, void* work, int64_t work_bytes,
                         void* stream);
+/* Launch shapes of the batched day (the autotuner's search space).
+ * Defaults (config == NULL): {32, 8, 8, 256, 0}. */
+typedef struct SolweigDayConfig {
+    int32_t shadow_bx, shadow_by;  /* shadow block: <= 256 threads, a multiple of 32 */
+    int32_t gvf_rows;              /* GVF tile rows per block: 4, 8 or 16 (32 columns) */
+    int32_t rad_threads;           /* radiation block: 128 or 256 pixels */
+    int32_t gemm_ctas_per_sm;      /* contraction CTAs per SM: 0 = as many as fit, 1, 2 */
+} SolweigDayConfig;
+int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                           const SolweigHour* hours, int nhours, const SolweigState* state,
+                           const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                           int first_steps, int second_steps, void* work, int64_t work_bytes,
+                           const SolweigDayConfig* config, void* stream);
+/* solweig_day_batched_ex timed with CUDA events on `stream` between its
+ * stages; synchronises on the last event and writes 5 host floats (ms):
+ * shadow, GVF, weights + tables, patch contraction, radiation. */
+int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                              const SolweigHour* hours, int nhours, const SolweigState* state,
+                              const SolweigOutputs* base, int64_t hour_stride,
+                              const int32_t* gvf_dxdy, int first_steps, int second_steps,
+                              void* work, int64_t work_bytes, const SolweigDayConfig* config,
+                              void* stream, float* stage_ms);
+/* Byte offsets inside the batched-day work buffer: quads [H][px] float4,
+ * first-direction Lup [H][px], GVF [H][3][px] (Lup, albedo, shadow),
+ * albedo-without-shadow GVF [px], patch sums [2][2H][px] (sky, vegetation x
+ * (luminance, luminance*cos*omega) per hour), weights f32 [2H][160], BF16
+ * operand, per-hour tables, error flag, total size: offsets[0..9]. */
+int solweig_day_batched_layout(int rows, int cols, int nhours, int has_water, int64_t* offsets);
 /* Copy the device error flag of the last batched day in `work` to out_device. */
 int solweig_day_batched_error(const void* work, int rows, int cols, int nhours, int has_water,
                               int* out_device, void* stream);

@@ -89,6 +89,20 @@ class SolweigState(ctypes.Structure):
     _fields_ = [(name, _vp) for name in STATE_FIELDS]
 
 
+class SolweigDayConfig(ctypes.Structure):
+    """Launch shapes of the batched day (``solweig_day_batched_ex``)."""
+    _fields_ = [("shadow_bx", ctypes.c_int32), ("shadow_by", ctypes.c_int32),
+                ("gvf_rows", ctypes.c_int32), ("rad_threads", ctypes.c_int32),
+                ("gemm_ctas_per_sm", ctypes.c_int32)]
+
+    def astuple(self):
+        return tuple(getattr(self, f) for f, _ in self._fields_)
+
+    @classmethod
+    def default(cls):
+        return cls(32, 8, 8, 256, 0)
+
+
 EXPORTED_SYMBOLS = (
     "solweig_last_error", "solweig_version", "solweig_wall_heights", "solweig_wall_aspect",
     "solweig_shadow", "solweig_svf", "solweig_svf_unpack", "solweig_diffsh", "solweig_gvf",
@@ -97,7 +111,8 @@ EXPORTED_SYMBOLS = (
     "solweig_step_radiation", "solweig_day", "solweig_step_gvf", "solweig_utci_scalar",
     "solweig_svf_pack", "solweig_svf_reduce", "solweig_step_static_scratch",
     "solweig_day_batched", "solweig_day_batched_work_bytes", "solweig_day_batched_error",
-    "solweig_patch_sums",
+    "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex",
+    "solweig_day_batched_layout",
 )
 
 _lock = threading.Lock()
@@ -125,6 +140,9 @@ def _declare(lib):
         "solweig_step_static_scratch": (i32, [P, P, P, i32, P, P, P, i32, i32, P]),
         "solweig_day_batched": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P]),
         "solweig_day_batched_work_bytes": (i64, [i32, i32, i32, i32]),
+        "solweig_day_batched_timed": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P, P]),
+        "solweig_day_batched_ex": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P]),
+        "solweig_day_batched_layout": (i32, [i32, i32, i32, i32, P]),
         "solweig_day_batched_error": (i32, [P, i32, i32, i32, i32, P, P]),
         "solweig_patch_sums": (i32, [P, i64, i32, P, i32, P, P, i64, P]),
         "solweig_day": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, P]),

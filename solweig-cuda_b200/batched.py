@@ -17,7 +17,7 @@ import torch
 from . import _lib
 from .engine import HourBuffers, device_ptr, outputs_struct, plan_day, stream_handle
 
-__all__ = ["BatchedDay", "ChosenDay"]
+__all__ = ["BatchedDay", "ChosenDay", "MultiDay", "TileBatch"]
 
 
 class BatchedDay:
@@ -119,6 +119,14 @@ class ChosenDay(BatchedDay):
             raise ValueError("bad batched-day shape")
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=scene.device)
         self.launches_per_day = 7
+        self.config = _lib.SolweigDayConfig.default()
+
+    def set_config(self, config):
+        """Launch shapes (``SolweigDayConfig`` or a 5-tuple); drops a captured graph."""
+        if not isinstance(config, _lib.SolweigDayConfig):
+            config = _lib.SolweigDayConfig(*config)
+        self.config = config
+        self.graph = None
 
     def _sequence(self):
         self.buffers.upload(0, self.hours, self.buffers.kmax)
@@ -126,11 +134,78 @@ class ChosenDay(BatchedDay):
             t.zero_()
         sc = self.scene
         base = outputs_struct(self.out, 0)
-        _lib.check(_lib.lib().solweig_day_batched(
+        _lib.check(_lib.lib().solweig_day_batched_ex(
             ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
             ctypes.byref(self._state_struct()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
-            sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes, stream_handle()),
-            "solweig_day_batched")
+            sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes,
+            ctypes.byref(self.config), stream_handle()), "solweig_day_batched_ex")
+
+    @staticmethod
+    def stage_bytes(pixels, hours, day_hours):
+        """Algorithmic HBM bytes of each stage of one day.
+
+        shadow: per daytime pixel-hour 40 B float64 geometry + 1 B flags + 20 B
+        float32 fields read, 16 B quad written (77 B); GVF: 16 B quad + 4 B face
+        bits + 4 B emissivity read, 3 planes + the albedo-without-shadow plane
+        written (40 B); tables: per-hour tables (negligible); contraction: 40 B
+        of mask words per pixel read, 2 x 2 sums per pixel-hour written
+        (16 B); radiation: 109 B of per-pixel statics and 16 B of state per
+        day, 28 B per daytime pixel-hour (3 GVF planes, 4 sums) and 8 B per
+        pixel-hour written (Tmrt, UTCI)."""
+        return {
+            "day_shadow_kernel": pixels * day_hours * 77,
+            "day_gvf_kernel": pixels * day_hours * 40,
+            "day_tables_kernel": hours * 9040,
+            "patch_gemm_kernel": pixels * (40 + 16 * hours),
+            "day_radiation_kernel": pixels * (125 + 28 * day_hours + 8 * hours),
+        }
+
+    @staticmethod
+    def gemm_flops(pixels, hours, patches):
+        """Algorithmic FLOPs of the contraction: 2 x pixels x patches x 2 hour
+        columns (luminance, luminance x cos x omega) x 2 masks (sky,
+        vegetation); the BF16 hi/lo duplication is not counted."""
+        return 2 * pixels * patches * (2 * hours) * 2
+
+    STAGES = ("day_shadow_kernel", "day_gvf_kernel", "day_tables_kernel", "patch_gemm_kernel",
+              "day_radiation_kernel")
+
+    def profile_day(self, met):
+        """Device time of each stage of one day, {stage: ms}, from CUDA events
+        recorded on the launching stream between the stages."""
+        self.plan(met)
+        self.buffers.upload(0, self.hours, self.buffers.kmax)
+        for t in self.state.values():
+            t.zero_()
+        sc = self.scene
+        base = outputs_struct(self.out, 0)
+        ms = (ctypes.c_float * len(self.STAGES))()
+        _lib.check(_lib.lib().solweig_day_batched_timed(
+            ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
+            ctypes.byref(self._state_struct()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
+            sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes,
+            ctypes.byref(self.config), stream_handle(), ms), "solweig_day_batched_timed")
+        self.buffers.mark()
+        return dict(zip(self.STAGES, (float(x) for x in ms)))
+
+    WORK_FIELDS = ("quads", "lup_first", "gvf", "nosh", "sums", "wf32", "bw", "tables", "error", "total")
+
+    def work_offsets(self):
+        """{field: byte offset} of the work buffer (``solweig_day_batched_layout``)."""
+        sc = self.scene
+        off = (ctypes.c_int64 * 10)()
+        _lib.check(_lib.lib().solweig_day_batched_layout(sc.rows, sc.cols, self.hours,
+                                                         int(sc.struct.has_water), off),
+                   "solweig_day_batched_layout")
+        return dict(zip(self.WORK_FIELDS, (int(x) for x in off)))
+
+    def patch_sums(self):
+        """The contraction's output of the last day as a [2, 2H, pixels] view:
+        [sky|vegetation][2h + (0: luminance, 1: luminance*cos*omega)]."""
+        o = self.work_offsets()
+        n = 2 * 2 * self.hours * self.scene.pixels
+        return self.work[o["sums"]:o["sums"] + 4 * n].view(torch.float32).view(2, 2 * self.hours,
+                                                                              self.scene.pixels)
 
     def error_flag(self):
         """Device error flag of the last day (0 = ok, 1 = a tensor-core wait timed out)."""
@@ -140,3 +215,161 @@ class ChosenDay(BatchedDay):
             device_ptr(self.work), sc.rows, sc.cols, self.hours, int(sc.struct.has_water),
             device_ptr(flag), stream_handle()), "solweig_day_batched_error")
         return int(flag.item())
+
+
+class MultiDay:
+    """``days`` consecutive days of ``hours`` rows each through ONE captured
+    graph: every hour record and sun ray uploaded once, then per day the state
+    reset (``src/series.py:425-436``) and the batched day
+    (``solweig_day_batched_ex``).  Outputs [days * hours, rows, cols]."""
+
+    def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0, days=30, hours=24,
+                 outputs=("tmrt", "utci"), config=None):
+        self.scene = scene
+        self.latitude, self.longitude, self.site_altitude, self.utc = latitude, longitude, site_altitude, utc
+        self.days, self.hours = days, hours
+        dev = scene.device
+        self.state = {k: torch.zeros(scene.shape, dtype=torch.float32, device=dev)
+                      for k in _lib.STATE_FIELDS}
+        self.buffers = HourBuffers(scene, days * hours)
+        self.layout_dev = scene.layout.device(dev)
+        self.out_names = tuple(outputs)
+        self.out = {k: torch.empty((days * hours,) + scene.shape, dtype=torch.float32, device=dev)
+                    for k in self.out_names}
+        self.work_bytes = int(_lib.lib().solweig_day_batched_work_bytes(scene.rows, scene.cols, hours,
+                                                                        int(scene.struct.has_water)))
+        self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=dev)
+        self.config = config if config is not None else _lib.SolweigDayConfig.default()
+        self.graph = None
+        self.launches = 7 * days
+
+    def plan(self, met):
+        met = np.asarray(met, dtype=np.float64)
+        if len(met) != self.days * self.hours:
+            raise ValueError(f"expected {self.days * self.hours} forcing rows, got {len(met)}")
+        self.buffers.wait_free()
+        H = self.hours
+        for d in range(self.days):
+            plan = plan_day(self.scene, met[d * H:(d + 1) * H], self.latitude, self.longitude,
+                            self.site_altitude, self.utc)
+            for i, (h, ray, _) in enumerate(plan):
+                self.buffers.put(d * H + i, h, ray)
+
+    def _sequence(self):
+        sc = self.scene
+        L = _lib.lib()
+        self.buffers.upload(0, self.days * self.hours, self.buffers.kmax)
+        st = _lib.SolweigState()
+        for k in _lib.STATE_FIELDS:
+            setattr(st, k, self.state[k].data_ptr())
+        hsize = self.buffers.hsize
+        for d in range(self.days):
+            for t in self.state.values():
+                t.zero_()
+            base = outputs_struct(self.out, d * self.hours)
+            hours_ptr = ctypes.c_void_p(self.buffers.h_dev.data_ptr() + d * self.hours * hsize)
+            _lib.check(L.solweig_day_batched_ex(
+                ctypes.byref(sc.struct), device_ptr(self.layout_dev), hours_ptr, self.hours,
+                ctypes.byref(st), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr, sc.first_steps,
+                sc.second_steps, device_ptr(self.work), self.work_bytes, ctypes.byref(self.config),
+                stream_handle()), "solweig_day_batched_ex")
+
+    def capture(self):
+        self._sequence()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._sequence()
+        self.graph = g
+
+    def replay(self):
+        self.graph.replay()
+        self.buffers.mark()
+        return self.out
+
+    def run(self, met):
+        self.plan(met)
+        if self.graph is None:
+            self.capture()
+        return self.replay()
+
+
+class TileBatch:
+    """Independent tiles (own scene, latitude and forcing) for one day each,
+    captured as ONE graph; a single work buffer sized for the largest tile is
+    reused tile after tile on the stream.  Each tile may carry its own launch
+    shapes (from :mod:`tune`)."""
+
+    def __init__(self, scenes, latitudes, longitudes, site_altitude=3.0, utc=0.0, hours=24,
+                 outputs=("tmrt", "utci"), configs=None):
+        self.scenes = list(scenes)
+        n = len(self.scenes)
+        self.latitudes = list(latitudes)
+        self.longitudes = list(longitudes)
+        self.site_altitude, self.utc, self.hours = site_altitude, utc, hours
+        dev = self.scenes[0].device
+        L = _lib.lib()
+        self.work_bytes = max(int(L.solweig_day_batched_work_bytes(s.rows, s.cols, hours,
+                                                                   int(s.struct.has_water)))
+                              for s in self.scenes)
+        self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=dev)
+        self.buffers = [HourBuffers(s, hours) for s in self.scenes]
+        self.layouts = [s.layout.device(dev) for s in self.scenes]
+        self.state = [{k: torch.zeros(s.shape, dtype=torch.float32, device=dev) for k in ("tgmap1", "tgout1")}
+                      for s in self.scenes]
+        self.out_names = tuple(outputs)
+        self.out = [{k: torch.empty((hours,) + s.shape, dtype=torch.float32, device=dev) for k in outputs}
+                    for s in self.scenes]
+        self.configs = list(configs) if configs is not None else [_lib.SolweigDayConfig.default()] * n
+        self.graph = None
+        self.launches = 7 * n
+
+    @property
+    def pixels(self):
+        return sum(s.pixels for s in self.scenes)
+
+    def plan(self, mets):
+        for s, b, met, lat, lon in zip(self.scenes, self.buffers, mets, self.latitudes, self.longitudes):
+            met = np.asarray(met, dtype=np.float64)
+            if len(met) != self.hours:
+                raise ValueError(f"expected {self.hours} forcing rows, got {len(met)}")
+            b.wait_free()
+            for i, (h, ray, _) in enumerate(plan_day(s, met, lat, lon, self.site_altitude, self.utc)):
+                b.put(i, h, ray)
+
+    def _sequence(self):
+        L = _lib.lib()
+        for s, b, lay, state, out, cfg in zip(self.scenes, self.buffers, self.layouts, self.state, self.out,
+                                              self.configs):
+            b.upload(0, self.hours, b.kmax)
+            st = _lib.SolweigState()
+            st.tgmap1 = state["tgmap1"].data_ptr()
+            st.tgout1 = state["tgout1"].data_ptr()
+            for t in state.values():
+                t.zero_()
+            base = outputs_struct(out, 0)
+            _lib.check(L.solweig_day_batched_ex(
+                ctypes.byref(s.struct), device_ptr(lay), b.ptr(), self.hours, ctypes.byref(st),
+                ctypes.byref(base), s.pixels, s.gvf_host_ptr, s.first_steps, s.second_steps,
+                device_ptr(self.work), self.work_bytes, ctypes.byref(cfg), stream_handle()),
+                "solweig_day_batched_ex")
+
+    def capture(self):
+        self._sequence()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._sequence()
+        self.graph = g
+
+    def replay(self):
+        self.graph.replay()
+        for b in self.buffers:
+            b.mark()
+        return self.out
+
+    def run(self, mets):
+        self.plan(mets)
+        if self.graph is None:
+            self.capture()
+        return self.replay()

@@ -150,15 +150,15 @@ __device__ double first_true(Pred pred) {
 
 // ---------------------------------------------------------------- kernels 1, 2
 
-__global__ void __launch_bounds__(kDayBX* kDayBY) day_shadow_kernel(SolweigScene S,
+__global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
                                                                    const SolweigHour* __restrict__ hours,
                                                                    float4* __restrict__ quads,
                                                                    float* __restrict__ lup_first) {
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
-    const int c = blockIdx.x * kDayBX + threadIdx.x;
-    const int r = blockIdx.y * kDayBY + threadIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (r >= S.rows || c >= S.cols) return;
     const long long n = (long long)S.rows * S.cols;
     shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr);
@@ -495,7 +495,6 @@ struct DayRadArgs {
     long long hour_stride;
 };
 
-constexpr int kRadThreads = 256;
 
 struct HourSmem {
     DayTable table;
@@ -520,8 +519,8 @@ __device__ __forceinline__ float* hour_plane(float* base, int hr, long long stri
     return base ? base + hr * stride : nullptr;
 }
 
-template <int OPT>
-__global__ void __launch_bounds__(kRadThreads, 2) day_radiation_kernel(SolweigScene S, DayRadArgs a) {
+template <int OPT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(SolweigScene S, DayRadArgs a) {
     __shared__ HourSmem hsm[2];
     __shared__ float wcos[SOLWEIG_MAX_BANDS], wsin[SOLWEIG_MAX_BANDS];
     const SolweigSkyLayout& L = *a.layout;
@@ -533,7 +532,7 @@ __global__ void __launch_bounds__(kRadThreads, 2) day_radiation_kernel(SolweigSc
     }
     stage_hour(hsm[0], a, 0);
     const long long n = (long long)S.rows * S.cols;
-    const long long p = (long long)blockIdx.x * kRadThreads + threadIdx.x;
+    const long long p = (long long)blockIdx.x * THREADS + threadIdx.x;
     const bool in = p < n;
     const long long q = in ? p : 0;  // a valid pixel for the loads of idle threads
 
@@ -722,11 +721,10 @@ void fill_day_table(GvfTable<TABLE>& tab, const int32_t* dxdy, int second, int p
     }
 }
 
-template <int FIRST, int SECOND, int TABLE>
-void launch_day_gvf(const SolweigScene& S, const SolweigHour* hours, int nhours, const DayGvfArgs& ga,
-                    const GvfTable<TABLE>& tab, const float4* quads, const float* lup_first, float* gvf, float* nosh,
-                    cudaStream_t st) {
-    constexpr int TY = 8;
+template <int TY, int FIRST, int SECOND, int TABLE>
+void launch_day_gvf_ty(const SolweigScene& S, const SolweigHour* hours, int nhours, const DayGvfArgs& ga,
+                       const GvfTable<TABLE>& tab, const float4* quads, const float* lup_first, float* gvf,
+                       float* nosh, cudaStream_t st) {
     const size_t smem = sizeof(float4) * (size_t)(32 + 2 * ga.halo) * (TY + 2 * ga.halo);
     dim3 grid(blocks_for(S.cols, 32), blocks_for(S.rows, TY), nhours);
     if (S.has_water) {
@@ -740,8 +738,17 @@ void launch_day_gvf(const SolweigScene& S, const SolweigHour* hours, int nhours,
     }
 }
 
+template <int FIRST, int SECOND, int TABLE>
+void launch_day_gvf(int ty, const SolweigScene& S, const SolweigHour* hours, int nhours, const DayGvfArgs& ga,
+                    const GvfTable<TABLE>& tab, const float4* quads, const float* lup_first, float* gvf,
+                    float* nosh, cudaStream_t st) {
+    if (ty == 4) launch_day_gvf_ty<4, FIRST, SECOND, TABLE>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+    else if (ty == 16) launch_day_gvf_ty<16, FIRST, SECOND, TABLE>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+    else launch_day_gvf_ty<8, FIRST, SECOND, TABLE>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+}
+
 int launch_gemm(const uint32_t* masks, long long px, int patches, const __nv_bfloat16* b, int ncols, int nb,
-                float* out, int* error, cudaStream_t st) {
+                float* out, int* error, cudaStream_t st, int ctas_per_sm = 0) {
     const size_t smem = gemm_smem_bytes(nb);
     SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "patch contraction: %d weight columns need %zu bytes of shared memory",
                       ncols, smem);
@@ -751,6 +758,7 @@ int launch_gemm(const uint32_t* masks, long long px, int patches, const __nv_bfl
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, patch_gemm_kernel, kARows, smem);
     if (per_sm < 1) per_sm = 1;
+    if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
     const long long ntiles = (px + kARows - 1) / kARows;
     long long grid = (long long)sms * per_sm;
     if (grid > ntiles) grid = ntiles;
@@ -772,6 +780,14 @@ extern "C" int64_t solweig_day_batched_work_bytes(int rows, int cols, int nhours
     return day_work_layout((long long)rows * cols, nhours, has_water != 0).total;
 }
 
+extern "C" int solweig_day_batched_layout(int rows, int cols, int nhours, int has_water, int64_t* offsets) {
+    SOLWEIG_CHECK_ARG(offsets && rows > 0 && cols > 0 && nhours > 0, "solweig_day_batched_layout: bad arguments");
+    const DayWork w = day_work_layout((long long)rows * cols, nhours, has_water != 0);
+    const long long v[10] = {w.quads, w.lup_first, w.gvf, w.nosh, w.sums, w.wf32, w.bw, w.tables, w.error, w.total};
+    for (int i = 0; i < 10; ++i) offsets[i] = v[i];
+    return SOLWEIG_OK;
+}
+
 extern "C" int solweig_patch_sums(const uint32_t* masks, int64_t pixels, int patches, const float* weights,
                                   int ncols, float* out, void* work, int64_t work_bytes, void* stream) {
     SOLWEIG_CHECK_ARG(masks && weights && out && work && pixels > 0, "solweig_patch_sums: null argument");
@@ -791,11 +807,26 @@ extern "C" int solweig_patch_sums(const uint32_t* masks, int64_t pixels, int pat
     return launch_gemm(masks, pixels, patches, b, ncols, nb, out, err, st);
 }
 
-extern "C" int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layout,
-                                   const SolweigHour* hours, int nhours, const SolweigState* state,
-                                   const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
-                                   int first_steps, int second_steps, void* work, int64_t work_bytes,
-                                   void* stream) {
+namespace {
+
+constexpr int kDayStages = 5;  // shadow, GVF, weights + tables, contraction, radiation
+
+int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, const SolweigHour* hours,
+                     int nhours, const SolweigState* state, const SolweigOutputs* base, int64_t hour_stride,
+                     const int32_t* gvf_dxdy, int first_steps, int second_steps, void* work,
+                     int64_t work_bytes, void* stream, cudaEvent_t* ev, const SolweigDayConfig* cfg_in) {
+    SolweigDayConfig cfg{32, 8, 8, 256, 0};
+    if (cfg_in) cfg = *cfg_in;
+    SOLWEIG_CHECK_ARG(cfg.shadow_bx > 0 && cfg.shadow_by > 0 && cfg.shadow_bx * cfg.shadow_by <= 256 &&
+                          (cfg.shadow_bx * cfg.shadow_by) % 32 == 0,
+                      "solweig_day_batched: shadow block %dx%d (at most 256 threads, a multiple of 32)",
+                      cfg.shadow_bx, cfg.shadow_by);
+    SOLWEIG_CHECK_ARG(cfg.gvf_rows == 4 || cfg.gvf_rows == 8 || cfg.gvf_rows == 16,
+                      "solweig_day_batched: gvf_rows must be 4, 8 or 16");
+    SOLWEIG_CHECK_ARG(cfg.rad_threads == 128 || cfg.rad_threads == 256,
+                      "solweig_day_batched: rad_threads must be 128 or 256");
+    SOLWEIG_CHECK_ARG(cfg.gemm_ctas_per_sm >= 0 && cfg.gemm_ctas_per_sm <= 2,
+                      "solweig_day_batched: gemm_ctas_per_sm must be 0 (auto), 1 or 2");
     SOLWEIG_CHECK_ARG(scene && layout && hours && base && work, "solweig_day_batched: null argument");
     const SolweigScene& S = *scene;
     SOLWEIG_CHECK_ARG(S.rows > 0 && S.cols > 0, "solweig_day_batched: bad scene shape %dx%d", S.rows, S.cols);
@@ -837,21 +868,25 @@ extern "C" int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLa
 
     cudaMemsetAsync(err, 0, sizeof(int), st);
     cudaMemsetAsync(nosh, 0, 4 * px, st);
+    if (ev) cudaEventRecord(ev[0], st);
     {
-        dim3 grid(blocks_for(S.cols, kDayBX), blocks_for(S.rows, kDayBY), nhours);
-        day_shadow_kernel<<<grid, dim3(kDayBX, kDayBY), 0, st>>>(S, hours, quads, lup_first);
+        dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nhours);
+        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(S, hours, quads, lup_first);
         SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
     }
+    if (ev) cudaEventRecord(ev[1], st);
     if (first_steps == 1 && second_steps == 22) {
         GvfTable<22> tab;
         fill_day_table(tab, gvf_dxdy, 22, pitch);
-        launch_day_gvf<1, 22, 22>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+        launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
     } else {
         GvfTable<SOLWEIG_GVF_MAX_STEPS> tab;
         fill_day_table(tab, gvf_dxdy, second_steps, pitch);
-        launch_day_gvf<0, 0, SOLWEIG_GVF_MAX_STEPS>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+        launch_day_gvf<0, 0, SOLWEIG_GVF_MAX_STEPS>(cfg.gvf_rows, S, hours, nhours, ga, tab, quads, lup_first, gvf,
+                                                    nosh, st);
     }
     SOLWEIG_CHECK_LAUNCH("day_gvf_kernel");
+    if (ev) cudaEventRecord(ev[2], st);
 
     const int ncols = 2 * nhours;
     const int nb = (ncols + 15) / 16 * 16;
@@ -861,8 +896,10 @@ extern "C" int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLa
     SOLWEIG_CHECK_LAUNCH("split_bf16_kernel");
     day_tables_kernel<<<nhours, kK, 0, st>>>(layout, hours, tables);
     SOLWEIG_CHECK_LAUNCH("day_tables_kernel");
-    int rc = launch_gemm(S.masks, px, S.patches, bw, ncols, nb, sums, err, st);
+    if (ev) cudaEventRecord(ev[3], st);
+    int rc = launch_gemm(S.masks, px, S.patches, bw, ncols, nb, sums, err, st, cfg.gemm_ctas_per_sm);
     if (rc) return rc;
+    if (ev) cudaEventRecord(ev[4], st);
 
     DayRadArgs ra{};
     ra.layout = layout;
@@ -876,13 +913,68 @@ extern "C" int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLa
     if (state) ra.state = *state;
     ra.out = *base;
     ra.hour_stride = hour_stride;
-    const unsigned blocks = blocks_for(px, kRadThreads);
-    if (S.patches == 153)
-        day_radiation_kernel<2><<<blocks, kRadThreads, 0, st>>>(S, ra);
-    else
-        day_radiation_kernel<1><<<blocks, kRadThreads, 0, st>>>(S, ra);
+    const unsigned blocks = blocks_for(px, cfg.rad_threads);
+    if (cfg.rad_threads == 128) {
+        if (S.patches == 153) day_radiation_kernel<2, 128><<<blocks, 128, 0, st>>>(S, ra);
+        else day_radiation_kernel<1, 128><<<blocks, 128, 0, st>>>(S, ra);
+    } else {
+        if (S.patches == 153) day_radiation_kernel<2, 256><<<blocks, 256, 0, st>>>(S, ra);
+        else day_radiation_kernel<1, 256><<<blocks, 256, 0, st>>>(S, ra);
+    }
     SOLWEIG_CHECK_LAUNCH("day_radiation_kernel");
+    if (ev) cudaEventRecord(ev[5], st);
     return SOLWEIG_OK;
+}
+
+}  // namespace
+
+extern "C" int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                   const SolweigHour* hours, int nhours, const SolweigState* state,
+                                   const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                                   int first_steps, int second_steps, void* work, int64_t work_bytes,
+                                   void* stream) {
+    return day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
+                            second_steps, work, work_bytes, stream, nullptr, nullptr);
+}
+
+extern "C" int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                      const SolweigHour* hours, int nhours, const SolweigState* state,
+                                      const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                                      int first_steps, int second_steps, void* work, int64_t work_bytes,
+                                      const SolweigDayConfig* config, void* stream) {
+    return day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
+                            second_steps, work, work_bytes, stream, nullptr, config);
+}
+
+extern "C" int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                         const SolweigHour* hours, int nhours, const SolweigState* state,
+                                         const SolweigOutputs* base, int64_t hour_stride,
+                                         const int32_t* gvf_dxdy, int first_steps, int second_steps, void* work,
+                                         int64_t work_bytes, const SolweigDayConfig* config, void* stream,
+                                         float* stage_ms) {
+    SOLWEIG_CHECK_ARG(stage_ms, "solweig_day_batched_timed: null stage_ms");
+    cudaEvent_t ev[kDayStages + 1];
+    for (int i = 0; i <= kDayStages; ++i) {
+        const cudaError_t e = cudaEventCreate(&ev[i]);
+        if (e != cudaSuccess) {
+            for (int j = 0; j < i; ++j) cudaEventDestroy(ev[j]);
+            set_error("solweig_day_batched_timed: cudaEventCreate: %s", cudaGetErrorString(e));
+            return SOLWEIG_ERR_CUDA;
+        }
+    }
+    int rc = day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
+                              second_steps, work, work_bytes, stream, ev, config);
+    if (rc == SOLWEIG_OK) {
+        const cudaError_t e = cudaEventSynchronize(ev[kDayStages]);
+        if (e != cudaSuccess) {
+            set_error("solweig_day_batched_timed: %s", cudaGetErrorString(e));
+            rc = SOLWEIG_ERR_CUDA;
+        } else {
+            for (int i = 0; i < kDayStages; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+        }
+    }
+    for (int i = 0; i <= kDayStages; ++i) cudaEventDestroy(ev[i]);
+    return rc;
 }
 
 // Device error flag of the last batched day run in `work` (0 = none, 1 = a

@@ -497,6 +497,16 @@ class HourScalars:
     lv: object
 
 
+def _ster_sin(L):
+    """(steradian, sin(altitude)) of every patch as Python floats, cached per layout."""
+    cached = getattr(L, "_ster_sin", None)
+    if cached is None:
+        cached = [(float(L.steradian[k]), float(np.sin(L.altitude[k] * (np.pi / 180))))
+                  for k in range(L.count)]
+        L._ster_sin = cached
+    return cached
+
+
 def hour_plan(scene, latitude, altitude, azimuth, zen, jday, dectime, altmax, ta, rh, rad_g, rad_d,
               rad_i, p_kpa, ws, psi, ci_prev, firstdaytime, timeadd, timestepdec, twater):
     """FP64 host scalars of one hour (``src/umep_solweig.py:122-232``).
@@ -583,10 +593,12 @@ def hour_plan(scene, latitude, altitude, azimuth, zen, jday, dectime, altmax, ta
         h.band_lsky[b] = (band_e[k] * base) / np.pi
     if day:
         lum = lv[:, 2]
+        # sequential float64 sum in patch order, as the reference loop
+        ster_sin = _ster_sin(L)
         rad_tot = 0.0
-        for k in range(L.count):
-            rad_tot += lum[k] * L.steradian[k] * np.sin(L.altitude[k] * (np.pi / 180))
-        h.rad_tot = float(np.asarray(rad_tot).item())
+        for lk, w in zip(lum.tolist(), ster_sin):
+            rad_tot += lk * w[0] * w[1]
+        h.rad_tot = rad_tot
         tan_alt = np.tan(altitude * (np.pi / 180))
         diff = np.abs(azimuth - L.azimuth)
         yi = 2 * np.cos(diff * (np.pi / 180)) * tan_alt

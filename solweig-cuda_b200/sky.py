@@ -159,12 +159,14 @@ def arctan_thresholds(altitudes):
 
 def band_emissivity(esky, layout):
     """Martin & Berdahl per-patch sky emissivity (model2, unnormalised)."""
-    uniq = np.unique(layout.altitude)
-    band = 1 - (1 - esky) * np.exp(0.308 * (1.7 - (1 / np.cos((90 - uniq) * _D2R))))
-    out = np.zeros(layout.count)
-    for a, e in zip(uniq, band):
-        out[layout.altitude == a] = e
-    return out
+    cached = getattr(layout, "_band_index", None)
+    if cached is None:
+        uniq, index = np.unique(layout.altitude, return_inverse=True)
+        cached = (uniq, 1 / np.cos((90 - uniq) * _D2R), index)
+        layout._band_index = cached
+    uniq, inv_cos, index = cached
+    band = 1 - (1 - esky) * np.exp(0.308 * (1.7 - inv_cos))
+    return band[index]
 
 
 _PEREZ = np.array([

@@ -112,3 +112,50 @@ def test_chosen_day_graph_replays_new_forcing(scene64):
         d = torch.max(torch.abs(a["tmrt"] - b["tmrt"])).item()
         assert d <= FORM_TOL, (doy, d)
     assert chosen.error_flag() == 0
+
+
+def test_multiday_graph_equals_day_by_day(scene64):
+    """Two days in one captured graph equal the single-day batched form."""
+    import torch
+    from solweig_cuda_b200 import batched, synthetic
+    sc, scene = scene64
+    met = synthetic.make_met(doy=180, latitude=53.0, longitude=0.0, days=2, seed=3)
+    md = batched.MultiDay(scene, 53.0, 0.0, 3.0, 0.0, days=2)
+    out = {k: v.clone() for k, v in md.run(met).items()}
+    one = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+    for d in range(2):
+        ref = one.run_day(met[24 * d:24 * (d + 1)])
+        torch.cuda.synchronize()
+        assert torch.equal(out["tmrt"][24 * d:24 * (d + 1)], ref["tmrt"]), d
+    # replaying the captured graph again gives the same result
+    again = md.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(again["tmrt"], out["tmrt"])
+
+
+def test_tile_batch_and_autotuner(cuda, tmp_path, monkeypatch):
+    """Uneven tiles in one graph equal each tile run alone; the autotuner picks
+    a config from its search space and caches it."""
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic, tune
+    monkeypatch.setenv("SOLWEIG_TUNE_CACHE", str(tmp_path / "tune.json"))
+    specs = [(40, 33, 1, 40.0), (57, 64, 2, 52.5), (72, 50, 3, 59.0)]
+    scenes, mets, lats = [], [], []
+    for r, c, seed, lat in specs:
+        s = synthetic.make_scene(r, c, seed=seed)
+        scenes.append(engine.Scene(s.dsm, s.trees, s.dem, 1.0, landcover=s.landcover))
+        mets.append(synthetic.make_met(doy=150, latitude=lat, longitude=0.0, seed=seed))
+        lats.append(lat)
+    day = batched.ChosenDay(scenes[2], lats[2], 0.0, 3.0, 0.0)
+    cfg, stages = tune.tune(day, mets[2], repeats=1)
+    assert (cfg.shadow_bx, cfg.shadow_by) in tune.SHADOW_BLOCKS
+    assert cfg.gvf_rows in tune.GVF_ROWS and cfg.rad_threads in tune.RAD_THREADS
+    assert set(stages) >= {"day_shadow_kernel", "day_gvf_kernel", "day_radiation_kernel"}
+    assert tune.lookup(day).astuple() == cfg.astuple()
+    tb = batched.TileBatch(scenes, lats, [0.0] * 3, configs=[cfg] * 3)
+    outs = tb.run(mets)
+    outs = [{k: v.clone() for k, v in o.items()} for o in outs]
+    for s, met, lat, o in zip(scenes, mets, lats, outs):
+        ref = batched.ChosenDay(s, lat, 0.0, 3.0, 0.0).run_day(met)
+        torch.cuda.synchronize()
+        assert torch.equal(o["tmrt"], ref["tmrt"])
