@@ -303,6 +303,41 @@ int solweig_day_batched_error(const void* work, int rows, int cols, int nhours, 
 int solweig_patch_sums(const uint32_t* masks, int64_t pixels, int patches, const float* weights,
                        int ncols, float* out, void* work, int64_t work_bytes, void* stream);
 
+/* Day gradient ---------------------------------------------------------------
+ * Reverse pass of the batched day with the shadow and SVF masks held fixed
+ * (the 1 m GVF walk, first = 1, second = 22; no water pixels; nhours <= 32).
+ * Per-pixel parameters replace the scene's ground albedo and emissivity and
+ * the hour's psi (direct-beam transmissivity of vegetation in
+ * shadow = sh - (1 - vegsh)(1 - t)).  objective: 0 = daily mean UTCI (NaN on
+ * roofs), 1 = daily mean Tmrt.  Both entry points recompute the day from its
+ * inputs (nothing is kept between calls).  The backward pass returns dJ/d
+ * parameter for J = sum_p weights[p] * daily[p], and the partials of J with
+ * respect to the hour scalars the device consumes:
+ * hour_grad[h][SOLWEIG_GRAD_HOUR_FIELDS] = (ta, rad_i, rad_d, rad_tot, ci_tgg,
+ * tgwall, band_lsky[8], utci[7]) and lum_grad[h][4][160] = mask-transposed
+ * sums (sky, sky x cos*omega, vegetation, vegetation x cos*omega) of the
+ * adjoints of the contraction outputs, from which
+ * dJ/dlum_k = lum_grad[h][0][k] + lum_grad[h][2][k]
+ *           + cos_alt_k * omega_k * (lum_grad[h][1][k] + lum_grad[h][3][k]). */
+#define SOLWEIG_GRAD_HOUR_FIELDS 21
+typedef struct SolweigGradParams {
+    const float* albedo;          /* [pixels] */
+    const float* emissivity;      /* [pixels] */
+    const float* transmissivity;  /* [pixels] */
+} SolweigGradParams;
+int64_t solweig_day_grad_work_bytes(int rows, int cols, int nhours);
+int solweig_day_grad_forward(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                             const SolweigHour* hours, int nhours, const int32_t* gvf_dxdy,
+                             int first_steps, int second_steps, const SolweigGradParams* params,
+                             int objective, double* daily /* [pixels] */, void* work,
+                             int64_t work_bytes, void* stream);
+int solweig_day_grad_backward(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                              const SolweigHour* hours, int nhours, const int32_t* gvf_dxdy,
+                              int first_steps, int second_steps, const SolweigGradParams* params,
+                              int objective, const float* weights, float* d_albedo,
+                              float* d_emissivity, float* d_transmissivity, double* hour_grad,
+                              double* lum_grad, void* work, int64_t work_bytes, void* stream);
+
 /* solweig_step without a scratch argument -- no counterpart in the reference.
  * For callers that cannot allocate device memory: a host model that owns its
  * arrays but no device allocator for temporaries, or that must not call

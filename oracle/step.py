@@ -269,17 +269,21 @@ def hour_step(s, location, altitude, azimuth, zen, jday, psi, dectime, altmax, T
     return dict(zip(OUTPUT_NAMES, values))
 
 
-def run_day(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI")):
+def run_day(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI"), psi=None):
     """Hour loop of one calendar day (``src/series.py:396-495``).
 
     ``met`` is the (rows, 24) forcing table of one day.  Returns a list (one
     entry per hour) of dicts with the requested outputs; ``UTCI`` has NaN on
-    roofs (``buildings != 1``).
+    roofs (``buildings != 1``).  ``psi`` (scalar or per-pixel array), when
+    given, replaces the leaf-on/off transmissivity of every hour.
     """
     sol = sun.metdata(met, location["latitude"], location["longitude"], location["altitude"], utc)
     doy = met[:, 1]
     leaf = (doy > CONSTANTS["firstdayleaf"]) & (doy < CONSTANTS["lastdayleaf"])
-    psi = np.where(leaf, 3. / 100., .5)
+    if psi is None:
+        psi = np.where(leaf, 3. / 100., .5)
+    else:
+        psi = [psi] * len(met)
     shape = (s["rows"], s["cols"])
     state = {k: np.zeros(shape) for k in ("Tgmap1", "Tgmap1E", "Tgmap1S", "Tgmap1W", "Tgmap1N", "TgOut1")}
     dectime = sol.dectime

@@ -89,6 +89,11 @@ class SolweigState(ctypes.Structure):
     _fields_ = [(name, _vp) for name in STATE_FIELDS]
 
 
+class SolweigGradParams(ctypes.Structure):
+    """Per-pixel parameters of the day gradient (device float32 pointers)."""
+    _fields_ = [("albedo", _vp), ("emissivity", _vp), ("transmissivity", _vp)]
+
+
 class SolweigDayConfig(ctypes.Structure):
     """Launch shapes of the batched day (``solweig_day_batched_ex``)."""
     _fields_ = [("shadow_bx", ctypes.c_int32), ("shadow_by", ctypes.c_int32),
@@ -112,7 +117,8 @@ EXPORTED_SYMBOLS = (
     "solweig_svf_pack", "solweig_svf_reduce", "solweig_step_static_scratch",
     "solweig_day_batched", "solweig_day_batched_work_bytes", "solweig_day_batched_error",
     "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex",
-    "solweig_day_batched_layout",
+    "solweig_day_batched_layout", "solweig_day_grad_work_bytes", "solweig_day_grad_forward",
+    "solweig_day_grad_backward",
 )
 
 _lock = threading.Lock()
@@ -143,6 +149,9 @@ def _declare(lib):
         "solweig_day_batched_timed": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P, P]),
         "solweig_day_batched_ex": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P]),
         "solweig_day_batched_layout": (i32, [i32, i32, i32, i32, P]),
+        "solweig_day_grad_work_bytes": (i64, [i32, i32, i32]),
+        "solweig_day_grad_forward": (i32, [P, P, P, i32, P, i32, i32, P, i32, P, P, i64, P]),
+        "solweig_day_grad_backward": (i32, [P, P, P, i32, P, i32, i32, P, i32, P, P, P, P, P, P, P, i64, P]),
         "solweig_day_batched_error": (i32, [P, i32, i32, i32, i32, P, P]),
         "solweig_patch_sums": (i32, [P, i64, i32, P, i32, P, P, i64, P]),
         "solweig_day": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, P]),

@@ -1,0 +1,745 @@
+// Kernels and launch helpers of the batched day, shared by the batched
+// entry points (day.cu) and the day gradient (adjoint.cu).  Everything lives
+// in an anonymous namespace: each translation unit instantiates its own copy.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "gvf_fields.cuh"
+#include "hour.cuh"
+#include "radiation.cuh"
+#include "tcgen05.cuh"
+
+namespace solweig {
+
+namespace {
+
+constexpr int kDayBX = 32, kDayBY = 8;
+constexpr int kK = SOLWEIG_MAX_PATCHES;   // contraction depth (patches, padded)
+constexpr int kSBO = (kK / 8) * 128;      // bytes between 8-row groups of an operand
+constexpr int kARows = 128;               // pixels per contraction tile (MMA M)
+constexpr int kABytes = kARows * kK * 2;  // one A operand in shared memory
+constexpr int kMaxDayHours = 64;
+constexpr uint32_t kWaitPolls = 1u << 24;
+
+// Element offset of (row n, patch k) in the canonical K-major layout.
+__host__ __device__ __forceinline__ int canon_off(int n, int k) {
+    return (n >> 3) * (kSBO / 2) + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
+}
+
+// Sunlit / shaded tables of one hour (size a multiple of 16 bytes).
+struct DayTable {
+    double tsun[kK];        // sorted: patch sunlit  <=> tan(asvf) <  T_k
+    double vshade[kK];      // sorted: patch shaded  <=> tan(asvf) >= V_k
+    uint32_t suf[kK + 1][SOLWEIG_MASK_WORDS];  // patches at sorted sunlit positions >= i
+    uint32_t pre[kK + 1][SOLWEIG_MASK_WORDS];  // patches at sorted shaded positions <  j
+    uint32_t test[SOLWEIG_MASK_WORDS];         // longwave sun test of the hour
+    uint32_t pad[5];
+};
+static_assert(sizeof(DayTable) % 16 == 0, "DayTable must be a multiple of 16 bytes");
+
+// Band boundaries (patch index) of the sky layouts the batched form supports.
+template <int OPT>
+struct Bands;
+template <>
+struct Bands<2> {  // 153 patches: 31, 30, 28, 24, 19, 13, 7, 1
+    __host__ __device__ static constexpr int off(int b) {
+        return b <= 0 ? 0 : b == 1 ? 31 : b == 2 ? 61 : b == 3 ? 89 : b == 4 ? 113 : b == 5 ? 132
+               : b == 6 ? 145 : b == 7 ? 152 : 153;
+    }
+};
+template <>
+struct Bands<1> {  // 145 patches: 30, 30, 24, 24, 18, 12, 6, 1
+    __host__ __device__ static constexpr int off(int b) {
+        return b <= 0 ? 0 : b == 1 ? 30 : b == 2 ? 60 : b == 3 ? 84 : b == 4 ? 108 : b == 5 ? 126
+               : b == 6 ? 138 : b == 7 ? 144 : 145;
+    }
+};
+
+// sum over bands of w[b] * popcount(m restricted to band b).
+template <int OPT>
+__device__ __forceinline__ float band_weighted(const uint32_t (&m)[SOLWEIG_MASK_WORDS], const float* w) {
+    float s = 0.f;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const int lo = Bands<OPT>::off(b), hi = Bands<OPT>::off(b + 1);
+        int c = 0;
+#pragma unroll
+        for (int wd = 0; wd < SOLWEIG_MASK_WORDS; ++wd) {
+            const int a = lo > wd * 32 ? lo : wd * 32;
+            const int e = hi < wd * 32 + 32 ? hi : wd * 32 + 32;
+            if (a < e) {
+                const uint32_t mask = (e - a == 32) ? 0xffffffffu : (((1u << (e - a)) - 1u) << (a - wd * 32));
+                c += __popc(m[wd] & mask);
+            }
+        }
+        s = fmaf((float)c, w[b], s);
+    }
+    return s;
+}
+
+// Number of entries of the ascending array a[0..n) that are <= t.
+__device__ __forceinline__ int count_le(const double* a, int n, double t) {
+    int lo = 0;
+    while (n > 0) {
+        const int half = n >> 1;
+        if (a[lo + half] <= t) {
+            lo += half + 1;
+            n -= half + 1;
+        } else {
+            n = half;
+        }
+    }
+    return lo;
+}
+
+// Monotone integer keys of the doubles (NaN excluded).
+__device__ __forceinline__ unsigned long long dkey(double x) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dval(unsigned long long k) {
+    const unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)u);
+}
+
+// Smallest double t in [-inf, +inf] with pred(t) true, for pred monotone
+// (false, then true); +inf when pred is false for every finite t.
+template <typename Pred>
+__device__ double first_true(Pred pred) {
+    const double ninf = __longlong_as_double(0xfff0000000000000ll);
+    const double pinf = __longlong_as_double(0x7ff0000000000000ll);
+    if (pred(ninf)) return ninf;
+    if (!pred(pinf)) return pinf;
+    unsigned long long lo = dkey(ninf), hi = dkey(pinf);  // pred(lo) false, pred(hi) true
+    while (hi - lo > 1) {
+        const unsigned long long mid = lo + (hi - lo) / 2;
+        if (pred(dval(mid))) hi = mid;
+        else lo = mid;
+    }
+    return dval(hi);
+}
+
+// ---------------------------------------------------------------- kernels 1, 2
+
+__global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
+                                                                   const SolweigHour* __restrict__ hours,
+                                                                   float4* __restrict__ quads,
+                                                                   float* __restrict__ lup_first) {
+    const int z = blockIdx.z;
+    const SolweigHour& h = hours[z];
+    if (!h.daytime) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (r >= S.rows || c >= S.cols) return;
+    const long long n = (long long)S.rows * S.cols;
+    shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr);
+}
+
+struct DayGvfArgs {
+    int first, second, halo;
+};
+
+// gvf[z][0] = Lup GVF (ambient added), gvf[z][1] = albedo GVF, gvf[z][2] = shadow.
+// nosh = albedo-without-shadow GVF: the same for every hour (walk geometry and
+// albedo only), so every daytime launch writes the same values.
+template <int TY, int FIRST, int SECOND, int TABLE, bool WATER>
+__global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
+                                                         DayGvfArgs ga, GvfTable<TABLE> tab,
+                                                         const float4* __restrict__ quads,
+                                                         const float* __restrict__ lup_first_all,
+                                                         float* __restrict__ gvf, float* __restrict__ nosh) {
+    const int z = blockIdx.z;
+    const SolweigHour& h = hours[z];
+    if (!h.daytime) return;
+    const long long n = (long long)S.rows * S.cols;
+    const float4* quad = quads + z * n;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int H = ga.halo, second = ga.second, first = ga.first;
+    const int pitch = 32 + 2 * H;
+    float4* tile = reinterpret_cast<float4*>(smem_raw);
+    const int row0 = blockIdx.y * TY - H, col0 = blockIdx.x * 32 - H;
+    load_quad_tile(tile, pitch, TY + 2 * H, quad, S.rows, S.cols, row0, col0);
+    __syncthreads();
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const int r = blockIdx.y * TY + threadIdx.y;
+    if (r >= S.rows || c >= S.cols) return;
+    const long long p = (long long)r * S.cols + c;
+    const float4* own_cell = tile + (threadIdx.y + H) * pitch + threadIdx.x + H;
+    const float4 own = *own_cell;
+    const double ta = h.ta;
+    const float lwall = (float)(kSBC * 0.9 * pow4(h.tgwall + ta + 273.15) - kSBC * 0.9 * pow4(ta + 273.15));
+    const float albedo_b = 0.2f;
+    const uint32_t face = S.gvf_face[p];
+    const bool own_ground = (__float_as_int(own.w) & kQuadGround) != 0;
+    float lup, alb, nsh;
+    if (WATER) {
+        const float* lfp = lup_first_all + z * n;
+        GvfScalars gs{lwall, albedo_b, first, second};
+        auto sample = [&](int rr, int cc) -> float4 { return tile[(rr - row0) * pitch + (cc - col0)]; };
+        auto lfirst = [&](int rr, int cc) -> float { return __ldg(&lfp[(long long)rr * S.cols + cc]); };
+        const GvfSums g = gvf_walk(sample, lfirst, true, r, c, S.rows, S.cols, tab.offs, face, own, gs);
+        lup = g.lup[0];
+        alb = g.alb[0];
+        nsh = g.nosh[0];
+    } else {
+        lup = alb = nsh = 0.f;
+        const bool interior = row0 >= 0 && col0 >= 0 && row0 + TY + 2 * H <= S.rows && col0 + pitch <= S.cols;
+        const float inv_first = 1.f / first, inv_first1 = 1.f / (first + 1);
+        const float inv_second = 1.f / second, inv_second1 = 1.f / (second + 1);
+#pragma unroll 1
+        for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
+            const bool fj = (face >> j) & 1u;
+            const int base = j * (SECOND > 0 ? SECOND : second);
+            GvfDir d;
+            if (SECOND > 0) {
+                d = interior ? gvf_direction_fixed<true, FIRST, SECOND>(own_cell, tab.delta + base, tab.offs + base, r,
+                                                                        c, S.rows, S.cols, own_ground, lwall,
+                                                                        albedo_b, fj)
+                             : gvf_direction_fixed<false, FIRST, SECOND>(own_cell, tab.delta + base, tab.offs + base,
+                                                                         r, c, S.rows, S.cols, own_ground, lwall,
+                                                                         albedo_b, fj);
+            } else {
+                d = interior ? gvf_direction<true>(own_cell, tab.delta + base, tab.offs + base, r, c, S.rows, S.cols,
+                                                   own_ground, first, second, inv_first, inv_first1, inv_second,
+                                                   inv_second1, lwall, albedo_b, fj)
+                             : gvf_direction<false>(own_cell, tab.delta + base, tab.offs + base, r, c, S.rows, S.cols,
+                                                    own_ground, first, second, inv_first, inv_first1, inv_second,
+                                                    inv_second1, lwall, albedo_b, fj);
+            }
+            lup += d.lup;
+            alb += d.alb;
+            nsh += d.nosh;
+        }
+        const float ob = own_ground ? 1.f : 0.f;
+        nsh *= ob;
+        lup += 18.f * (own.y * (1.f - ob));
+        alb += 18.f * (own.z * (1.f - ob) * own.x);
+        nsh += 18.f * (own.z * (1.f - ob));
+    }
+    const double ambient = kSBC * (double)S.emis[p] * pow4(ta + 273.15);
+    gvf[(3 * z) * n + p] = (float)((double)(lup / 18.f) + ambient);
+    gvf[(3 * z + 1) * n + p] = alb / 18.f;
+    gvf[(3 * z + 2) * n + p] = own.x;
+    nosh[p] = nsh / 18.f;
+}
+
+// ------------------------------------------------------------- kernels 3, 4, 5
+
+// w[2h][k] = luminance, w[2h+1][k] = luminance * cos(alt) * omega (0 at night).
+__global__ void day_weights_kernel(const SolweigSkyLayout* __restrict__ L, const SolweigHour* __restrict__ hours,
+                                   int nhours, float* __restrict__ w) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 2 * nhours * kK) return;
+    const int row = idx / kK, k = idx - row * kK;
+    const SolweigHour& h = hours[row >> 1];
+    float v = 0.f;
+    if (h.daytime && k < L->patches) v = (row & 1) ? h.lum[k] * L->cos_alt[k] * L->omega[k] : h.lum[k];
+    w[idx] = v;
+}
+
+// BF16 hi/lo split of w [ncols][kK] into the canonical operand layout
+// b[0][nb rows] (hi) and b[1][nb rows] (lo); rows >= ncols are zero.
+__global__ void split_bf16_kernel(const float* __restrict__ w, int ncols, int nb, int patches,
+                                  __nv_bfloat16* __restrict__ b) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * kK) return;
+    const int n = idx / kK, k = idx - n * kK;
+    const float v = (n < ncols && k < patches) ? w[n * kK + k] : 0.f;
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+    const int o = canon_off(n, k);
+    b[o] = hi;
+    b[nb * kK + o] = lo;
+}
+
+// One block per hour, kK threads.
+__global__ void __launch_bounds__(kK) day_tables_kernel(const SolweigSkyLayout* __restrict__ L,
+                                                        const SolweigHour* __restrict__ hours,
+                                                        DayTable* __restrict__ tables) {
+    __shared__ double ts[kK], vs[kK];
+    __shared__ int perm_t[kK], perm_v[kK];
+    const SolweigHour& h = hours[blockIdx.x];
+    DayTable& T = tables[blockIdx.x];
+    const int P = L->patches;
+    const int k = threadIdx.x;
+    double tk = 0.0, vk = 0.0;
+    if (k < P) {
+        const double yi = h.yi[k], lo = L->sunlit_below[k], hi = L->shaded_above[k];
+        tk = first_true([&](double t) { return !((t + yi) < lo); });
+        vk = first_true([&](double t) { return (t + yi) > hi; });
+        ts[k] = tk;
+        vs[k] = vk;
+    }
+    __syncthreads();
+    if (k < P) {
+        int rt = 0, rv = 0;
+        for (int j = 0; j < P; ++j) {
+            rt += (ts[j] < tk || (ts[j] == tk && j < k)) ? 1 : 0;
+            rv += (vs[j] < vk || (vs[j] == vk && j < k)) ? 1 : 0;
+        }
+        T.tsun[rt] = tk;
+        T.vshade[rv] = vk;
+        perm_t[rt] = k;
+        perm_v[rv] = k;
+    }
+    __syncthreads();
+    for (int i = k; i <= P; i += blockDim.x) {
+        uint32_t suf[SOLWEIG_MASK_WORDS] = {0, 0, 0, 0, 0}, pre[SOLWEIG_MASK_WORDS] = {0, 0, 0, 0, 0};
+        for (int r = 0; r < P; ++r) {
+            if (r >= i) suf[perm_t[r] >> 5] |= 1u << (perm_t[r] & 31);
+            if (r < i) pre[perm_v[r] >> 5] |= 1u << (perm_v[r] & 31);
+        }
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            T.suf[i][w] = suf[w];
+            T.pre[i][w] = pre[w];
+        }
+    }
+    if (k < SOLWEIG_MASK_WORDS) {
+        uint32_t t = 0;
+        for (int b = 0; b < 32; ++b) {
+            const int kk = k * 32 + b;
+            if (kk < P && h.daytime && h.lw_sun_test[kk]) t |= 1u << b;
+        }
+        T.test[k] = t;
+    }
+}
+
+// ------------------------------------------------------------------ kernel 6
+
+struct GemmArgs {
+    const uint32_t* masks;  // S/V bit planes [10][px]
+    long long px;
+    int patches;
+    const __nv_bfloat16* b;  // [2][nb * kK] canonical hi, lo
+    int ncols, nb;
+    float* out;  // [2 * ncols][px]: sky columns, then vegetation columns
+    int* error;
+};
+
+size_t gemm_smem_bytes(int nb) { return (size_t)2 * kABytes + (size_t)2 * nb * kK * 2 + 16; }
+
+// Expand 8 mask bits to 8 BF16 values (1.0 or 0.0) packed in a uint4.
+__device__ __forceinline__ uint4 expand8(uint32_t byte) {
+    uint32_t v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t two = (byte >> (2 * i)) & 3u;
+        v[i] = ((two & 1u) | ((two & 2u) << 15)) * 0x3F80u;
+    }
+    return make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+// Persistent: one 128-pixel tile per iteration.  All 128 threads expand the
+// tile's masks into the two A operands; thread 0 issues the MMAs (sky and
+// vegetation, BF16 hi and lo weights accumulating into the same FP32
+// columns) and commits them to an mbarrier; each warp then reads its 32 rows
+// (pixels) of the accumulators from tensor memory and stores them.
+__global__ void __launch_bounds__(kARows, 1) patch_gemm_kernel(GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* a_sky = smem;
+    unsigned char* a_veg = smem + kABytes;
+    unsigned char* b_ops = smem + 2 * kABytes;  // hi then lo
+    const int bbytes = g.nb * kK * 2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(b_ops + 2 * bbytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint32_t ncols_tmem = 32;
+    while (ncols_tmem < (uint32_t)(2 * g.nb)) ncols_tmem <<= 1;
+
+    {  // weights: global -> shared, 16 bytes per copy
+        const uint4* src = reinterpret_cast<const uint4*>(g.b);
+        uint4* dst = reinterpret_cast<uint4*>(b_ops);
+        for (int i = tid; i < 2 * bbytes / 16; i += blockDim.x) dst[i] = src[i];
+    }
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(tmem_slot, ncols_tmem);
+        tc::tmem_relinquish();
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = tc::idesc_bf16_f32(kARows, g.nb);
+    const uint32_t a_sky_addr = tc::smem_addr(a_sky), a_veg_addr = tc::smem_addr(a_veg);
+    const uint32_t b_hi_addr = tc::smem_addr(b_ops), b_lo_addr = b_hi_addr + bbytes;
+    uint32_t valid[SOLWEIG_MASK_WORDS];
+#pragma unroll
+    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+        const int nbits = g.patches - 32 * w;
+        valid[w] = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
+    }
+    const long long ntiles = (g.px + kARows - 1) / kARows;
+    uint32_t phase = 0;
+    bool failed = false;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long p = t * kARows + tid;
+        const bool in = p < g.px;
+        // Expand this pixel's row of both A operands.
+        unsigned char* row_sky = a_sky + (tid >> 3) * kSBO + (tid & 7) * 16;
+        unsigned char* row_veg = a_veg + (tid >> 3) * kSBO + (tid & 7) * 16;
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            const uint32_t s = in ? g.masks[(long long)w * g.px + p] : 0u;
+            const uint32_t v = in ? g.masks[(long long)(SOLWEIG_MASK_WORDS + w) * g.px + p] : 0u;
+            const uint32_t sky = s & ~v & valid[w], veg = s & v & valid[w];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int chunk = w * 4 + j;
+                *reinterpret_cast<uint4*>(row_sky + chunk * 128) = expand8((sky >> (8 * j)) & 0xFFu);
+                *reinterpret_cast<uint4*>(row_veg + chunk * 128) = expand8((veg >> (8 * j)) & 0xFFu);
+            }
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll 1
+            for (int s = 0; s < kK / 16; ++s) {
+                const uint64_t bh = tc::smem_desc(b_hi_addr + s * 256, 128, kSBO);
+                const uint64_t bl = tc::smem_desc(b_lo_addr + s * 256, 128, kSBO);
+                const uint64_t as = tc::smem_desc(a_sky_addr + s * 256, 128, kSBO);
+                const uint64_t av = tc::smem_desc(a_veg_addr + s * 256, 128, kSBO);
+                tc::mma_bf16(tmem, as, bh, idesc, s > 0);
+                tc::mma_bf16(tmem, as, bl, idesc, true);
+                tc::mma_bf16(tmem + g.nb, av, bh, idesc, s > 0);
+                tc::mma_bf16(tmem + g.nb, av, bl, idesc, true);
+            }
+            tc::mma_commit(bar);
+        }
+        const bool ok = tc::mbar_wait(bar, phase, kWaitPolls);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        phase ^= 1u;
+        tc::fence_after_sync();
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < g.ncols; c0 += 8) {
+            float vs[8], vv[8];
+            tc::tmem_ld8(lane_base + c0, vs);
+            tc::tmem_ld8(lane_base + g.nb + c0, vv);
+            tc::tmem_wait_ld();
+            if (in) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (c0 + i < g.ncols) {
+                        g.out[(long long)(c0 + i) * g.px + p] = vs[i];
+                        g.out[(long long)(g.ncols + c0 + i) * g.px + p] = vv[i];
+                    }
+                }
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(g.error, 1);
+        // let the MMAs of the abandoned tile finish before freeing their columns
+        tc::mbar_wait(bar, phase, kWaitPolls);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, ncols_tmem);
+    }
+}
+
+// ------------------------------------------------------------------ kernel 7
+
+struct DayRadArgs {
+    const SolweigSkyLayout* layout;
+    const SolweigHour* hours;
+    int nhours;
+    const DayTable* tables;
+    const float* gvf;   // [H][3][px]
+    const float* nosh;  // [px]
+    const float* sums;  // [2 * ncols][px]
+    int ncols;
+    SolweigState state;
+    SolweigOutputs out;  // base pointers; hour h at + h * hour_stride
+    long long hour_stride;
+};
+
+
+struct HourSmem {
+    DayTable table;
+    float band_down[SOLWEIG_MAX_BANDS], band_side[SOLWEIG_MAX_BANDS];
+};
+
+__device__ __forceinline__ void stage_hour(HourSmem& hs, const DayRadArgs& a, int hr) {
+    const uint4* src = reinterpret_cast<const uint4*>(a.tables + hr);
+    uint4* dst = reinterpret_cast<uint4*>(&hs.table);
+    for (int i = threadIdx.x; i < (int)(sizeof(DayTable) / 16); i += blockDim.x) dst[i] = src[i];
+    if (threadIdx.x < SOLWEIG_MAX_BANDS) {
+        const SolweigSkyLayout& L = *a.layout;
+        const SolweigHour& h = a.hours[hr];
+        const int b = threadIdx.x;
+        const bool ok = b < L.nbands;
+        hs.band_down[b] = ok ? h.band_lsky[b] * L.band_omega[b] * L.band_sin[b] : 0.f;
+        hs.band_side[b] = ok ? h.band_lsky[b] * L.band_omega[b] * L.band_cos[b] : 0.f;
+    }
+}
+
+__device__ __forceinline__ float* hour_plane(float* base, int hr, long long stride) {
+    return base ? base + hr * stride : nullptr;
+}
+
+template <int OPT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(SolweigScene S, DayRadArgs a) {
+    __shared__ HourSmem hsm[2];
+    __shared__ float wcos[SOLWEIG_MAX_BANDS], wsin[SOLWEIG_MAX_BANDS];
+    const SolweigSkyLayout& L = *a.layout;
+    if (threadIdx.x < SOLWEIG_MAX_BANDS) {
+        const int b = threadIdx.x;
+        const int k0 = Bands<OPT>::off(b < 8 ? b : 0);
+        wcos[b] = b < L.nbands ? L.omega[k0] * L.cos_alt[k0] : 0.f;
+        wsin[b] = b < L.nbands ? L.omega[k0] * L.sin_alt[k0] : 0.f;
+    }
+    stage_hour(hsm[0], a, 0);
+    const long long n = (long long)S.rows * S.cols;
+    const long long p = (long long)blockIdx.x * THREADS + threadIdx.x;
+    const bool in = p < n;
+    const long long q = in ? p : 0;  // a valid pixel for the loads of idle threads
+
+    // --- per-pixel static data, loaded once for the day
+    uint32_t bld[SOLWEIG_MASK_WORDS];
+#pragma unroll
+    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+        const int nbits = S.patches - 32 * w;
+        const uint32_t valid = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
+        bld[w] = ~S.masks[(long long)w * n + q] & ~S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + q] & valid;
+    }
+    uint32_t cnt_lo = 0, cnt_hi = 0;  // sky patches per band, 8 bits each
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        cnt_lo |= (uint32_t)S.sky_band_counts[(long long)b * n + q] << (8 * b);
+        cnt_hi |= (uint32_t)(b + 4 < S.nbands ? S.sky_band_counts[(long long)(b + 4) * n + q] : 0) << (8 * b);
+    }
+    const uint8_t fl = S.flags[q];
+    const bool ground = fl & 1;
+    const bool water = S.has_water && (fl & 4);
+    const double emis = S.emis[q];
+    const float tgk = S.tgk[q], tstart = S.tstart[q], tmaxlst = S.tmaxlst[q];
+    const double svfbuveg = S.svfbuveg[q];
+    const double tan_alfa = tan(S.svfalfa[q]);
+    const double tan_asvf = S.tan_asvf[q];
+    const double vc = S.veg_sums[q], vs = S.veg_sums[n + q];
+    const double oc = S.veg_sums[2 * n + q], os = S.veg_sums[3 * n + q];
+    const double g_nosh = a.nosh[q];
+    constexpr double ewall = 0.9, albedo_b = 0.2;
+    constexpr double absK = 0.7, absL = 0.95, Fside = 0.22, Fup = 0.06, Fcyl = 0.28;
+    const double dsh_veg = 1.0 - (1.0 - 0.03);
+
+    float st_lup = a.state.tgmap1 ? a.state.tgmap1[q] : 0.f;
+    float st_tg = a.state.tgout1 ? a.state.tgout1[q] : 0.f;
+
+    for (int hr = 0; hr < a.nhours; ++hr) {
+        HourSmem& hs = hsm[hr & 1];
+        __syncthreads();  // hs staged; the other buffer is free
+        if (hr + 1 < a.nhours) stage_hour(hsm[(hr + 1) & 1], a, hr + 1);
+        const SolweigHour& h = a.hours[hr];
+        const bool day = h.daytime != 0;
+        const double ta = h.ta;
+        const double tk = ta + 273.15;
+
+        // building patches: sunlit / shaded split of the hour
+        const DayTable& T = hs.table;
+        const int P = S.patches;
+        const int isun = count_le(T.tsun, P, tan_asvf);
+        const int ishd = count_le(T.vshade, P, tan_asvf);
+        uint32_t m_sun[SOLWEIG_MASK_WORDS], m_shd[SOLWEIG_MASK_WORDS], m_lsun[SOLWEIG_MASK_WORDS],
+            m_lshd[SOLWEIG_MASK_WORDS];
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            const uint32_t test = T.test[w];
+            m_sun[w] = bld[w] & T.suf[isun][w];
+            m_shd[w] = bld[w] & T.pre[ishd][w];
+            m_lsun[w] = m_sun[w] & test;
+            m_lshd[w] = bld[w] & (~test | m_shd[w]);
+        }
+        const float lw_sun_c = band_weighted<OPT>(m_lsun, wcos), lw_sun_s = band_weighted<OPT>(m_lsun, wsin);
+        const float lw_shd_c = band_weighted<OPT>(m_lshd, wcos), lw_shd_s = band_weighted<OPT>(m_lshd, wsin);
+        double ld_sky = 0.0, ls_sky = 0.0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const double cnt = (double)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
+            ld_sky += (double)hs.band_down[b] * cnt;
+            ls_sky += (double)hs.band_side[b] * cnt;
+        }
+        const double lw_shade = (ewall * kSBC * pow4(tk)) / kPi;
+        const double lw_sun = day ? (ewall * kSBC * pow4(ta + h.tgwall + 273.15)) / kPi : 0.0;
+
+        double shadow = 0.0, tg = 0.0, tg_out = ta;
+        double kup_all = 0.0, lup_all;
+        double kdown = 0.0, kside = 0.0, kside_i = 0.0, kside_d = 0.0, d_rad = 0.0;
+        if (day) {
+            const long long g0 = (3LL * hr) * n + q;
+            const double g_lup = a.gvf[g0];
+            const double g_alb = a.gvf[g0 + n];
+            shadow = a.gvf[g0 + 2 * n];
+            const double fsh = wedge_fsh_tan(tan_alfa, h.tan_zen);
+            const double reflected = albedo_b * (1.0 - svfbuveg) * (h.rad_g * (1.0 - fsh) + h.rad_d * fsh);
+            const double base_up = h.rad_d * svfbuveg + reflected;
+            const double direct_up = h.rad_i * h.sin_alt;
+            kup_all = g_alb * direct_up + base_up * g_nosh;
+            const double prev = h.firstdaytime ? g_lup : (double)st_lup;
+            lup_all = g_lup * (1.0 - h.wave_weight) + prev * h.wave_weight;
+            st_lup = (float)(h.wave_update ? lup_all : prev);
+            // ground temperature (TsWaveDelay of Tg * shadow + Ta)
+            const double amp = (double)tgk * h.altmax + (double)tstart;
+            const double phase =
+                ((h.dectime_frac - h.snup / 24.0) / ((double)tmaxlst / 24.0 - h.snup / 24.0)) * kPi / 2.0;
+            tg = amp * sin(phase) * h.ci_tgg;
+            if (S.landcover == 1 && tg < 0.0) tg = 0.0;
+            if (water) tg = h.twater - ta;
+            {
+                const double cur = tg * shadow + ta;
+                const double prv = h.firstdaytime ? cur : (double)st_tg;
+                tg_out = cur * (1.0 - h.wave_weight) + prv * h.wave_weight;
+                st_tg = (float)(h.wave_update ? tg_out : prv);
+            }
+            const long long s0 = 2LL * hr;
+            const double lum_sky = a.sums[s0 * n + q], cw_sky = a.sums[(s0 + 1) * n + q];
+            const double lum_veg = a.sums[(a.ncols + s0) * n + q], cw_veg = a.sums[(a.ncols + s0 + 1) * n + q];
+            d_rad = h.rad_d * (lum_sky + dsh_veg * lum_veg);
+            kdown = h.rad_i * shadow * h.sin_alt + d_rad + reflected;
+            kside_i = shadow * h.rad_i * h.cos_alt;
+            kside_d = (h.rad_d / h.rad_tot) * (cw_sky + dsh_veg * cw_veg);
+            const double sw_shade = (albedo_b * h.rad_d * 0.5) / kPi;
+            const double sw_sun = (albedo_b * (h.rad_i * h.cos_alt) + h.rad_d * 0.5) / kPi;
+            kside = kside_i + kside_d + sw_sun * (double)band_weighted<OPT>(m_sun, wcos) +
+                    sw_shade * (double)band_weighted<OPT>(m_shd, wcos) + sw_shade * vc;
+        } else {
+            double lup = kSBC * emis * pow4(ta + 0.0 + 273.15);
+            if (S.landcover == 1 && (fl & 4)) lup = kSBC * 0.98 * pow4(h.twater + 273.15);
+            lup_all = lup;
+        }
+        const double refl = ((ld_sky + lup_all) * (1.0 - ewall) * 0.5) / kPi;
+        const double ldown = ld_sky + lw_shade * vs + lw_shade * (double)lw_shd_s + lw_sun * (double)lw_sun_s + refl * os;
+        const double lside = ls_sky + lw_shade * vc + lw_shade * (double)lw_shd_c + lw_sun * (double)lw_sun_c + refl * oc;
+        // E+S+W+N of Kup and Lup are 4x the all-direction values (see the file header).
+        const double sstr = absK * (kside * Fcyl + (kdown + kup_all) * Fup + 2.0 * kup_all * Fside) +
+                            absL * ((ldown + lup_all) * Fup + lside * Fcyl + 2.0 * lup_all * Fside);
+        const double tmrt = sqrt(sqrt(sstr / (absL * kSBC))) - 273.2;
+        if (in) {
+            const SolweigOutputs& o = a.out;
+            const long long hs_ = a.hour_stride;
+            if (o.tmrt) o.tmrt[hr * hs_ + p] = (float)tmrt;
+            if (o.utci)
+                o.utci[hr * hs_ + p] = ground ? utci_eval(h.utci, tmrt, ta, h.utci_valid) : __int_as_float(0x7fc00000);
+            if (o.kdown) o.kdown[hr * hs_ + p] = (float)kdown;
+            if (o.kup) o.kup[hr * hs_ + p] = (float)kup_all;
+            if (o.ldown) o.ldown[hr * hs_ + p] = (float)ldown;
+            if (o.lup) o.lup[hr * hs_ + p] = (float)lup_all;
+            if (o.lside) o.lside[hr * hs_ + p] = (float)lside;
+            if (o.kside_i) o.kside_i[hr * hs_ + p] = (float)kside_i;
+            if (o.kside_d) o.kside_d[hr * hs_ + p] = (float)kside_d;
+            if (o.kside) o.kside[hr * hs_ + p] = (float)kside;
+            if (o.d_rad) o.d_rad[hr * hs_ + p] = (float)d_rad;
+            if (o.shadow) o.shadow[hr * hs_ + p] = (float)shadow;
+            if (o.tg) o.tg[hr * hs_ + p] = (float)tg;
+            if (o.tg_out) o.tg_out[hr * hs_ + p] = (float)tg_out;
+        }
+    }
+    if (in) {
+        if (a.state.tgmap1) a.state.tgmap1[p] = st_lup;
+        if (a.state.tgout1) a.state.tgout1[p] = st_tg;
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+inline long long align256(long long x) { return (x + 255) & ~255LL; }
+
+struct DayWork {
+    long long quads, lup_first, gvf, nosh, sums, wf32, bw, tables, error, total;
+};
+
+DayWork day_work_layout(long long px, int nhours, bool water) {
+    DayWork w{};
+    const int ncols = 2 * nhours;
+    const int nb = (ncols + 15) / 16 * 16;
+    long long o = 0;
+    w.quads = o; o = align256(o + 16LL * px * nhours);
+    w.lup_first = o; o = align256(o + (water ? 4LL * px * nhours : 0));
+    w.gvf = o; o = align256(o + 12LL * px * nhours);
+    w.nosh = o; o = align256(o + 4LL * px);
+    w.sums = o; o = align256(o + 4LL * px * 2 * ncols);
+    w.wf32 = o; o = align256(o + 4LL * ncols * kK);
+    w.bw = o; o = align256(o + 2LL * 2 * nb * kK);
+    w.tables = o; o = align256(o + (long long)sizeof(DayTable) * nhours);
+    w.error = o; o = align256(o + 16);
+    w.total = o;
+    return w;
+}
+
+void set_smem_attr(const void* kernel, size_t bytes) {
+    // Not a stream operation; cheap after the first call.
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int TABLE>
+void fill_day_table(GvfTable<TABLE>& tab, const int32_t* dxdy, int second, int pitch) {
+    for (int i = 0; i < SOLWEIG_GVF_DIRECTIONS * second; ++i) {
+        tab.offs[i] = make_int2(dxdy[2 * i], dxdy[2 * i + 1]);
+        tab.delta[i] = dxdy[2 * i] * pitch + dxdy[2 * i + 1];
+    }
+}
+
+template <int TY, int FIRST, int SECOND, int TABLE>
+void launch_day_gvf_ty(const SolweigScene& S, const SolweigHour* hours, int nhours, const DayGvfArgs& ga,
+                       const GvfTable<TABLE>& tab, const float4* quads, const float* lup_first, float* gvf,
+                       float* nosh, cudaStream_t st) {
+    const size_t smem = sizeof(float4) * (size_t)(32 + 2 * ga.halo) * (TY + 2 * ga.halo);
+    dim3 grid(blocks_for(S.cols, 32), blocks_for(S.rows, TY), nhours);
+    if (S.has_water) {
+        auto k = day_gvf_kernel<TY, FIRST, SECOND, TABLE, true>;
+        set_smem_attr((const void*)k, smem);
+        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, ga, tab, quads, lup_first, gvf, nosh);
+    } else {
+        auto k = day_gvf_kernel<TY, FIRST, SECOND, TABLE, false>;
+        set_smem_attr((const void*)k, smem);
+        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, ga, tab, quads, lup_first, gvf, nosh);
+    }
+}
+
+template <int FIRST, int SECOND, int TABLE>
+void launch_day_gvf(int ty, const SolweigScene& S, const SolweigHour* hours, int nhours, const DayGvfArgs& ga,
+                    const GvfTable<TABLE>& tab, const float4* quads, const float* lup_first, float* gvf,
+                    float* nosh, cudaStream_t st) {
+    if (ty == 4) launch_day_gvf_ty<4, FIRST, SECOND, TABLE>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+    else if (ty == 16) launch_day_gvf_ty<16, FIRST, SECOND, TABLE>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+    else launch_day_gvf_ty<8, FIRST, SECOND, TABLE>(S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+}
+
+int launch_gemm(const uint32_t* masks, long long px, int patches, const __nv_bfloat16* b, int ncols, int nb,
+                float* out, int* error, cudaStream_t st, int ctas_per_sm = 0) {
+    const size_t smem = gemm_smem_bytes(nb);
+    SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "patch contraction: %d weight columns need %zu bytes of shared memory",
+                      ncols, smem);
+    set_smem_attr((const void*)patch_gemm_kernel, smem);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, patch_gemm_kernel, kARows, smem);
+    if (per_sm < 1) per_sm = 1;
+    if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+    const long long ntiles = (px + kARows - 1) / kARows;
+    long long grid = (long long)sms * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    if (grid < 1) grid = 1;
+    GemmArgs g{masks, px, patches, b, ncols, nb, out, error};
+    patch_gemm_kernel<<<(unsigned)grid, kARows, smem, st>>>(g);
+    SOLWEIG_CHECK_LAUNCH("patch_gemm_kernel");
+    return SOLWEIG_OK;
+}
+
+}  // namespace
+
+}  // namespace solweig

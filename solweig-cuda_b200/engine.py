@@ -495,6 +495,7 @@ class HourScalars:
     CI_TgG: float
     Tgwall: float
     lv: object
+    band_lsky: object = None  # float64 band sky emittances (the record holds float32)
 
 
 def _ster_sin(L):
@@ -588,9 +589,11 @@ def hour_plan(scene, latitude, altitude, azimuth, zen, jday, dectime, altmax, ta
     # per-patch weights
     band_e = _sky.band_emissivity(esky, L)
     base = SBC * ((ta + 273.15) ** 4)
+    band_lsky = np.zeros(L.band_counts.size)
     for b in range(L.band_counts.size):
         k = int(L.band_offsets[b])
-        h.band_lsky[b] = (band_e[k] * base) / np.pi
+        band_lsky[b] = (band_e[k] * base) / np.pi
+        h.band_lsky[b] = band_lsky[b]
     if day:
         lum = lv[:, 2]
         # sequential float64 sum in patch order, as the reference loop
@@ -615,7 +618,7 @@ def hour_plan(scene, latitude, altitude, azimuth, zen, jday, dectime, altmax, ta
         h.utci[i] = coef[i]
     h.utci_valid = int(not (np.float32(ta) <= -999 or np.float32(rh) <= -999 or np.float32(ws) <= -999))
     scal = HourScalars(ea=ea, esky=esky, I0=I0, CI=CI, radI=rad_i, radD=rad_d, CI_Tg=CI_Tg,
-                       CI_TgG=CI_TgG, Tgwall=tgwall, lv=lv)
+                       CI_TgG=CI_TgG, Tgwall=tgwall, lv=lv, band_lsky=band_lsky)
     return h, ray, scal, next_state
 
 
