@@ -44,7 +44,7 @@ def _args():
     p.add_argument("--form", choices=("plain", "batched", "chosen"), default="chosen")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=("day", "month", "tiles", "precision"), default="day",
+    p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient"), default="day",
                    help="day: the headline 2000^2 x 24 h line; month: 2000^2 x 720 h in one graph; "
                         "tiles: 64 uneven tiles in one graph; precision: 4000^2 patch-sum error report")
     p.add_argument("--no-tune", dest="tune", action="store_false",
@@ -358,6 +358,86 @@ def run_precision(a):
         "patch_gemm_tflops": gemm_flops / (stage["patch_gemm_kernel"] / 1000.0) / 1e12}), flush=True)
 
 
+def run_gradient(a):
+    """1000^2 px x 24 h: adjoint of the daily-mean UTCI (masks fixed) w.r.t. albedo
+    U[0.1,0.4], emissivity U[0.9,0.98], vegetation transmissivity U[0.02,0.2] and
+    Ta/RH/wind; timed, and checked against central differences along random
+    directions."""
+    import numpy as np
+    import torch
+    from solweig_cuda_b200 import engine, grad, synthetic
+    dev = torch.device("cuda", 0)
+    n = 1000 if a.size == 2000 else a.size
+    sc = synthetic.make_scene(n, seed=0)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, device=dev)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    rng = np.random.default_rng(0)
+    prm = {"albedo": rng.uniform(0.1, 0.4, scene.shape).astype(np.float32),
+           "emissivity": rng.uniform(0.9, 0.98, scene.shape).astype(np.float32),
+           "transmissivity": rng.uniform(0.02, 0.2, scene.shape).astype(np.float32)}
+    w = np.ones(scene.shape, np.float32) / scene.pixels
+    dg = grad.DayGradient(scene, 53.0, 0.0, 3.0, 0.0)
+    P = {k: torch.from_numpy(v).to(dev) for k, v in prm.items()}
+    Wt = torch.from_numpy(w).to(dev)
+
+    def fwd():
+        return dg.forward(P["albedo"], P["emissivity"], P["transmissivity"], met)
+
+    def bwd():
+        return dg.backward(P["albedo"], P["emissivity"], P["transmissivity"], met, Wt)
+
+    for _ in range(a.warmup):
+        fwd()
+        bwd()
+    t_f, t_b = [], []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        fwd()
+        t_f.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        out = bwd()
+        t_b.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    jac = dg.forcing_jacobian(met)
+    t_jac = time.perf_counter() - t0
+    fg = dg.forcing_grad(met, out[3], out[4], jac)
+    g = {"albedo": out[0].cpu().numpy().astype(np.float64), "emissivity": out[1].cpu().numpy().astype(np.float64),
+         "transmissivity": out[2].cpu().numpy().astype(np.float64), **fg}
+
+    def J(p, m):
+        d = dg.forward(p["albedo"], p["emissivity"], p["transmissivity"], m).cpu().numpy()
+        return float(np.nansum(d * w))
+
+    steps = {"albedo": 1e-2, "emissivity": 1e-2, "transmissivity": 1e-2, "ta": 1e-2, "rh": 1e-1, "ws": 1e-2}
+    rng = np.random.default_rng(1)
+    checks = {}
+    for name, h in steps.items():
+        v = rng.uniform(-1, 1, scene.shape if name in prm else 24)
+        pp = {k: x.copy() for k, x in prm.items()}
+        pm = {k: x.copy() for k, x in prm.items()}
+        mp, mm = met.copy(), met.copy()
+        if name in prm:
+            pp[name] = (prm[name] + h * v).astype(np.float32)
+            pm[name] = (prm[name] - h * v).astype(np.float32)
+        else:
+            col = grad.FORCING_COLUMNS[name]
+            mp[:, col] += h * v
+            mm[:, col] -= h * v
+        fd = (J(pp, mp) - J(pm, mm)) / (2 * h)
+        ad = float(np.sum(g[name] * v))
+        checks[name] = {"adjoint": ad, "central_difference": fd, "rel_error": abs(ad - fd) / max(abs(fd), 1e-30)}
+    print(json.dumps({
+        "metric": "daily-mean UTCI adjoint, 1000^2 px x 24 h (masks fixed)",
+        "value": float(np.mean(t_b)), "unit": "s per backward (forward recomputed inside)",
+        "higher_is_better": False, "steps": a.steps, "warmup": a.warmup,
+        "forward_s": float(np.mean(t_f)), "forcing_jacobian_s": t_jac,
+        "config": {"workload": f"{n}x{n} px at 1 m, DOY 172, 53N; albedo U[0.1,0.4], emissivity U[0.9,0.98], "
+                               "transmissivity U[0.02,0.2]; J = mean over pixels of daily-mean UTCI",
+                   "timing": "host wall clock around each synchronous call"},
+        "directional_checks": checks,
+        "gradient_norms": {k: float(np.linalg.norm(v)) for k, v in g.items()}}), flush=True)
+
+
 def main():
     a = _args()
     rank = int(os.environ.get("RANK", "0"))
@@ -369,7 +449,8 @@ def main():
         if rank == 0:
             import torch
             torch.cuda.set_device(0)
-            {"month": run_month, "tiles": run_tiles, "precision": run_precision}[a.workload](a)
+            {"month": run_month, "tiles": run_tiles, "precision": run_precision,
+             "gradient": run_gradient}[a.workload](a)
         return 0
     import numpy as np
     import torch
