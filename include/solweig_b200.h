@@ -265,12 +265,15 @@ int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layou
                         int first_steps, int second_steps, void* work, int64_t work_bytes,
                         void* stream);
 /* Launch shapes of the batched day (the autotuner's search space).
- * Defaults (config == NULL): {32, 8, 8, 256, 0}. */
+ * Defaults (config == NULL): {32, 8, 8, 256, 0, 1}. */
 typedef struct SolweigDayConfig {
     int32_t shadow_bx, shadow_by;  /* shadow block: <= 256 threads, a multiple of 32 */
     int32_t gvf_rows;              /* GVF tile rows per block: 4, 8 or 16 (32 columns) */
     int32_t rad_threads;           /* radiation block: 128 or 256 pixels */
     int32_t gemm_ctas_per_sm;      /* contraction CTAs per SM: 0 = as many as fit, 1, 2 */
+    int32_t gvf_hours;             /* 1: interior 32x32 tiles walk all daytime hours in one
+                                      block, 4 hours per pass (1 m walk, no water); 0: one
+                                      launch slice per hour everywhere */
 } SolweigDayConfig;
 int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSkyLayout* layout,
                            const SolweigHour* hours, int nhours, const SolweigState* state,

@@ -75,7 +75,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
                      int nhours, const SolweigState* state, const SolweigOutputs* base, int64_t hour_stride,
                      const int32_t* gvf_dxdy, int first_steps, int second_steps, void* work,
                      int64_t work_bytes, void* stream, cudaEvent_t* ev, const SolweigDayConfig* cfg_in) {
-    SolweigDayConfig cfg{32, 8, 8, 256, 0};
+    SolweigDayConfig cfg{32, 8, 8, 256, 0, 1};
     if (cfg_in) cfg = *cfg_in;
     SOLWEIG_CHECK_ARG(cfg.shadow_bx > 0 && cfg.shadow_by > 0 && cfg.shadow_bx * cfg.shadow_by <= 256 &&
                           (cfg.shadow_bx * cfg.shadow_by) % 32 == 0,
@@ -87,6 +87,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
                       "solweig_day_batched: rad_threads must be 128 or 256");
     SOLWEIG_CHECK_ARG(cfg.gemm_ctas_per_sm >= 0 && cfg.gemm_ctas_per_sm <= 2,
                       "solweig_day_batched: gemm_ctas_per_sm must be 0 (auto), 1 or 2");
+    SOLWEIG_CHECK_ARG(cfg.gvf_hours == 0 || cfg.gvf_hours == 1, "solweig_day_batched: gvf_hours must be 0 or 1");
     SOLWEIG_CHECK_ARG(scene && layout && hours && base && work, "solweig_day_batched: null argument");
     const SolweigScene& S = *scene;
     SOLWEIG_CHECK_ARG(S.rows > 0 && S.cols > 0, "solweig_day_batched: bad scene shape %dx%d", S.rows, S.cols);
@@ -138,7 +139,17 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     if (first_steps == 1 && second_steps == 22) {
         GvfTable<22> tab;
         fill_day_table(tab, gvf_dxdy, 22, pitch);
-        launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+        const bool hv = cfg.gvf_hours == 1 && !S.has_water;
+        DayGvfArgs gh = ga;
+        gh.hv_skip = hv ? 1 : 0;
+        launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, gh, tab, quads, lup_first, gvf, nosh, st);
+        if (hv) {
+            const size_t smem = hv_smem_bytes();
+            set_smem_attr((const void*)day_gvf_hv_kernel, smem);
+            dim3 grid(blocks_for(S.cols, kHvTile), blocks_for(S.rows, kHvTile));
+            day_gvf_hv_kernel<<<grid, dim3(kHvTile, kHvTile), smem, st>>>(S, hours, nhours, tab, quads, gvf, nosh);
+            SOLWEIG_CHECK_LAUNCH("day_gvf_hv_kernel");
+        }
     } else {
         GvfTable<SOLWEIG_GVF_MAX_STEPS> tab;
         fill_day_table(tab, gvf_dxdy, second_steps, pitch);

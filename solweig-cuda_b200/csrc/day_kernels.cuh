@@ -137,7 +137,17 @@ __global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
 
 struct DayGvfArgs {
     int first, second, halo;
+    int hv_skip;  // 1: blocks inside an interior tile of the hour-vectorized kernel return at once
 };
+
+// Tiles of the hour-vectorized GVF kernel: 32 x 32 pixels, halo 21 (the 1 m
+// walk, second = 22).  A tile is interior when its halo lies inside the raster.
+constexpr int kHvTile = 32, kHvHalo = 21, kHvPitch = kHvTile + 2 * kHvHalo;
+
+__host__ __device__ __forceinline__ bool hv_tile_interior(int rows, int cols, int tr, int tc) {
+    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
+    return row0 >= 0 && col0 >= 0 && row0 + kHvPitch <= rows && col0 + kHvPitch <= cols;
+}
 
 // gvf[z][0] = Lup GVF (ambient added), gvf[z][1] = albedo GVF, gvf[z][2] = shadow.
 // nosh = albedo-without-shadow GVF: the same for every hour (walk geometry and
@@ -151,6 +161,7 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
+    if (ga.hv_skip && hv_tile_interior(S.rows, S.cols, (int)(blockIdx.y * TY) / kHvTile, blockIdx.x)) return;
     const long long n = (long long)S.rows * S.cols;
     const float4* quad = quads + z * n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -221,6 +232,210 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
     gvf[(3 * z + 1) * n + p] = alb / 18.f;
     gvf[(3 * z + 2) * n + p] = own.x;
     nosh[p] = nsh / 18.f;
+}
+
+// Hour-vectorized GVF for interior 32 x 32 tiles (the 1 m walk: first = 1,
+// second = 22), all daytime hours of the day in one block.  The walk length
+// of every direction (first building step) and the albedo-without-shadow
+// plane depend only on the ground bits and the albedo, so they are computed
+// once; then per pass of kHvCh daytime hours the tile is staged as
+// (Lup, albedo*shadow) pairs plus the sunlit-wall bits of those hours, and
+// every walked sample is one pair of 16-byte shared loads serving all kHvCh
+// hours.  The sunlit-wall statistics need only the first step at which each
+// hour's bit appears: seen at step f < hit means n_sun = second - f (the
+// steps after a building hit keep counting, as in gvf_direction_fixed).
+// Same recurrences and the same float32 operation order as
+// gvf_direction_fixed except albedo*shadow, which is rounded once per sample
+// here instead of fused into the sum.
+constexpr int kHvN = kHvPitch * kHvPitch;
+constexpr int kHvCh = 4;
+constexpr int kHvThreads = kHvTile * kHvTile;
+
+size_t hv_smem_bytes() { return (size_t)kHvN * (2 * sizeof(float4) + 2 * sizeof(uint32_t)) + 64 * sizeof(int); }
+
+__global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
+                                                                  int nhours, GvfTable<22> tab,
+                                                                  const float4* __restrict__ quads,
+                                                                  float* __restrict__ gvf, float* __restrict__ nosh) {
+    constexpr int FIRST = 1, SECOND = 22;
+    const int tr = blockIdx.y, tc = blockIdx.x;
+    if (!hv_tile_interior(S.rows, S.cols, tr, tc)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* LA = reinterpret_cast<float4*>(smem_raw);  // Lup, albsh of pass hours 0, 1
+    float4* LB = LA + kHvN;                            // pass hours 2, 3
+    uint32_t* bits = reinterpret_cast<uint32_t*>(LB + kHvN);  // bit0 ground, bits 1..4 sunlit wall
+    float* albs = reinterpret_cast<float*>(bits + kHvN);      // albedo
+    int* dayh = reinterpret_cast<int*>(albs + kHvN);          // daytime hour indices
+    __shared__ int nday;
+    const int tid = threadIdx.y * kHvTile + threadIdx.x;
+    const long long n = (long long)S.rows * S.cols;
+    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
+    if (tid == 0) {
+        int k = 0;
+        for (int h = 0; h < nhours && k < 64; ++h)
+            if (hours[h].daytime) dayh[k++] = h;
+        nday = k;
+    }
+    __syncthreads();
+    const int nd = nday;
+    if (nd == 0) return;
+    {
+        const float4* q0 = quads + (long long)dayh[0] * n;
+        for (int i = tid; i < kHvN; i += kHvThreads) {
+            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
+            const float4 q = q0[(long long)rr * S.cols + cc];
+            bits[i] = (uint32_t)__float_as_int(q.w) & kQuadGround;
+            albs[i] = q.z;
+        }
+    }
+    __syncthreads();
+    const int r = tr * kHvTile + threadIdx.y, c = tc * kHvTile + threadIdx.x;
+    const long long p = (long long)r * S.cols + c;
+    const int own = (threadIdx.y + kHvHalo) * kHvPitch + threadIdx.x + kHvHalo;
+    const bool own_ground = (bits[own] & 1u) != 0;
+    const float ob = own_ground ? 1.f : 0.f;
+    const uint32_t face = S.gvf_face[p];
+    constexpr float albedo_b = 0.2f;
+    constexpr float inv_first = 1.f / FIRST, inv_first1 = 1.f / (FIRST + 1);
+    constexpr float inv_second = 1.f / SECOND, inv_second1 = 1.f / (SECOND + 1);
+    // walk lengths (6 directions x 5 bits per word) and the static plane
+    uint32_t hits[3] = {0u, 0u, 0u};
+    float nsh = 0.f;
+    for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
+        int hit = 0;
+        float s_alb = 0.f, n_alb = 0.f;
+        if (own_ground) {
+            hit = SECOND;
+            for (int m = 0; m < SECOND; ++m) {
+                const int off = own + tab.delta[j * SECOND + m];
+                if (!(bits[off] & 1u)) {
+                    hit = m;
+                    break;
+                }
+                s_alb += albs[off];
+                if (m + 1 == FIRST) n_alb = s_alb;
+            }
+        }
+        hits[j / 6] |= (uint32_t)hit << (5 * (j % 6));
+        const int n_wall = SECOND - hit;
+        const int n_wall_first = FIRST > hit ? FIRST - hit : 0;
+        const float nosh1 = n_wall_first > 0 ? ((float)n_wall_first * albedo_b + n_alb) * inv_first1 : n_alb * inv_first;
+        const float nosh2 = n_wall > 0 ? ((float)n_wall * albedo_b + s_alb) * inv_second : s_alb * inv_second;
+        nsh += (nosh1 * 0.5f + nosh2 * 0.4f) * (1.f / 0.9f);
+    }
+    nsh *= ob;
+    nsh += 18.f * (albs[own] * (1.f - ob));
+    nosh[p] = nsh / 18.f;
+    const double ambient_e = kSBC * (double)S.emis[p];
+
+    for (int g0 = 0; g0 < nd; g0 += kHvCh) {
+        const int nc = nd - g0 < kHvCh ? nd - g0 : kHvCh;
+        __syncthreads();  // the previous pass no longer reads the tile
+        for (int i = tid; i < kHvN; i += kHvThreads) {
+            const long long pix = (long long)(row0 + i / kHvPitch) * S.cols + (col0 + i % kHvPitch);
+            float v[2 * kHvCh];
+            uint32_t b = bits[i] & 1u;
+#pragma unroll
+            for (int k = 0; k < kHvCh; ++k) {
+                if (k < nc) {
+                    const float4 q = quads[(long long)dayh[g0 + k] * n + pix];
+                    v[2 * k] = q.y;
+                    v[2 * k + 1] = q.z * q.x;
+                    b |= (((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u) << (1 + k);
+                } else {
+                    v[2 * k] = v[2 * k + 1] = 0.f;
+                }
+            }
+            LA[i] = make_float4(v[0], v[1], v[2], v[3]);
+            LB[i] = make_float4(v[4], v[5], v[6], v[7]);
+            bits[i] = b;
+        }
+        __syncthreads();
+        float lw[kHvCh];
+#pragma unroll
+        for (int k = 0; k < kHvCh; ++k) {
+            if (k < nc) {
+                const SolweigHour& hh = hours[dayh[g0 + k]];
+                lw[k] = (float)(kSBC * 0.9 * pow4(hh.tgwall + hh.ta + 273.15) - kSBC * 0.9 * pow4(hh.ta + 273.15));
+            } else {
+                lw[k] = 0.f;
+            }
+        }
+        float lup_t[kHvCh], alb_t[kHvCh];
+#pragma unroll
+        for (int k = 0; k < kHvCh; ++k) lup_t[k] = alb_t[k] = 0.f;
+        if (own_ground) {
+#pragma unroll 1
+            for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
+                const int hit = (int)((hits[j / 6] >> (5 * (j % 6))) & 31u);
+                float sl[kHvCh], sa[kHvCh], l0[kHvCh], a0[kHvCh];
+#pragma unroll
+                for (int k = 0; k < kHvCh; ++k) sl[k] = sa[k] = l0[k] = a0[k] = 0.f;
+                uint32_t seen = 0u, first_pk = 0xFFFFFu;  // 5 bits per hour, 31 = never
+#pragma unroll
+                for (int m = 0; m < SECOND; ++m) {
+                    if (m < hit) {
+                        const int off = own + tab.delta[j * SECOND + m];
+                        const float4 A = LA[off], B = LB[off];
+                        const uint32_t b = (bits[off] >> 1) & 15u;
+                        sl[0] += A.x; sa[0] += A.y; sl[1] += A.z; sa[1] += A.w;
+                        sl[2] += B.x; sa[2] += B.y; sl[3] += B.z; sa[3] += B.w;
+                        const uint32_t nb = b & ~seen;
+                        if (nb) {
+#pragma unroll
+                            for (int k = 0; k < kHvCh; ++k)
+                                if ((nb >> k) & 1u) first_pk = (first_pk & ~(31u << (5 * k))) | ((uint32_t)m << (5 * k));
+                            seen |= b;
+                        }
+                        if (m + 1 == FIRST) {
+#pragma unroll
+                            for (int k = 0; k < kHvCh; ++k) {
+                                l0[k] = sl[k];
+                                a0[k] = sa[k];
+                            }
+                        }
+                    }
+                }
+                const bool fj = (face >> j) & 1u;
+#pragma unroll
+                for (int k = 0; k < kHvCh; ++k) {
+                    const int f = (int)((first_pk >> (5 * k)) & 31u);
+                    const int n_sun = f < hit ? SECOND - f : 0;
+                    const int n_sun_first = (f < FIRST && f < hit) ? FIRST - f : 0;
+                    const bool sun_near = n_sun_first > 0, sun_far = n_sun > 0;
+                    const float s_wall = (float)n_sun;
+                    float s_lwall = s_wall * lw[k], s_albwall = s_wall * albedo_b;
+                    if (n_sun == SECOND && fj) {
+                        s_lwall = 0.f;
+                        s_albwall = 0.f;
+                    }
+                    const float nn = (float)n_sun_first;
+                    const float lup1 = sun_near ? (nn * lw[k] + l0[k]) * inv_first1 : l0[k] * inv_first;
+                    const float lup2 = sun_far ? (s_lwall + sl[k]) * inv_second1 : sl[k] * inv_second;
+                    const float alb1 = sun_near ? (nn * albedo_b + a0[k]) * inv_first1 : a0[k] * inv_first;
+                    const float alb2 = sun_far ? (s_albwall + sa[k]) * inv_second1 : sa[k] * inv_second;
+                    lup_t[k] += (lup1 * 0.5f + lup2 * 0.4f) * (1.f / 0.9f);
+                    alb_t[k] += (alb1 * 0.5f + alb2 * 0.4f) * (1.f / 0.9f);
+                }
+            }
+        }
+        const float4 oA = LA[own], oB = LB[own];
+        const float own_lup[4] = {oA.x, oA.z, oB.x, oB.z};
+        const float own_albsh[4] = {oA.y, oA.w, oB.y, oB.w};
+#pragma unroll
+        for (int k = 0; k < kHvCh; ++k) {
+            if (k < nc) {
+                const int h = dayh[g0 + k];
+                const SolweigHour& hh = hours[h];
+                const float lt = lup_t[k] + 18.f * (own_lup[k] * (1.f - ob));
+                const float at = alb_t[k] + 18.f * (own_albsh[k] * (1.f - ob));
+                const double ambient = ambient_e * pow4(hh.ta + 273.15);
+                gvf[(3LL * h) * n + p] = (float)((double)(lt / 18.f) + ambient);
+                gvf[(3LL * h + 1) * n + p] = at / 18.f;
+                gvf[(3LL * h + 2) * n + p] = quads[(long long)h * n + p].x;
+            }
+        }
+    }
 }
 
 // ------------------------------------------------------------- kernels 3, 4, 5

@@ -3,13 +3,15 @@
 The search space is :class:`_lib.SolweigDayConfig`:
 
 * shadow block (columns x rows): 32x8, 64x4, 16x16, 32x4, 128x2
-* GVF tile rows per block: 4, 8, 16 (32 columns, halo of ``second`` - 1)
+* GVF: tile rows per block of the per-hour kernel: 4, 8, 16 (32 columns,
+  halo of ``second`` - 1), with or without the hour-vectorized kernel on
+  interior 32 x 32 tiles
 * radiation block: 128 or 256 pixels
 * patch-contraction CTAs per SM: 1 or 2
 
 ``solweig_day_batched_timed`` times every stage with CUDA events on the
 launching stream, and each stage's time depends only on its own parameter,
-so the search is one pass per parameter with the others held (5 + 3 + 2 + 2
+so the search is one pass per parameter with the others held (5 + 6 + 2 + 2
 timed days, each repeated and the minimum taken).  Results are cached per
 (device, tile-size bucket, hours, patches) in a JSON file
 (``$SOLWEIG_TUNE_CACHE`` or ``~/.cache/solweig_cuda_b200/autotune.json``),
@@ -26,11 +28,12 @@ import torch
 
 from . import _lib
 
-__all__ = ["SHADOW_BLOCKS", "GVF_ROWS", "RAD_THREADS", "GEMM_CTAS", "cache_path", "tune_key",
+__all__ = ["SHADOW_BLOCKS", "GVF_ROWS", "GVF_HOURS", "RAD_THREADS", "GEMM_CTAS", "cache_path", "tune_key",
            "tune", "lookup", "apply"]
 
 SHADOW_BLOCKS = ((32, 8), (64, 4), (16, 16), (32, 4), (128, 2))
 GVF_ROWS = (4, 8, 16)
+GVF_HOURS = (0, 1)
 RAD_THREADS = (128, 256)
 GEMM_CTAS = (1, 2)
 
@@ -52,7 +55,7 @@ def _bucket(n):
 def tune_key(runner):
     sc = runner.scene
     name = torch.cuda.get_device_name(sc.device)
-    return f"{name}|{_bucket(sc.rows)}x{_bucket(sc.cols)}|h{runner.hours}|p{sc.struct.patches}"
+    return f"v2|{name}|{_bucket(sc.rows)}x{_bucket(sc.cols)}|h{runner.hours}|p{sc.struct.patches}"
 
 
 def _load():
@@ -123,7 +126,7 @@ def tune(runner, met, repeats=2, use_cache=True):
         c[0], c[1] = v
 
     def set_gvf(c, v):
-        c[2] = v
+        c[2], c[5] = v
 
     def set_rad(c, v):
         c[3] = v
@@ -132,7 +135,7 @@ def tune(runner, met, repeats=2, use_cache=True):
         c[4] = v
 
     pick("day_shadow_kernel", SHADOW_BLOCKS, set_shadow)
-    pick("day_gvf_kernel", GVF_ROWS, set_gvf)
+    pick("day_gvf_kernel", [(r, h) for h in GVF_HOURS for r in GVF_ROWS], set_gvf)
     pick("day_radiation_kernel", RAD_THREADS, set_rad)
     pick("patch_gemm_kernel", GEMM_CTAS, set_gemm)
     config = _lib.SolweigDayConfig(*cfg)

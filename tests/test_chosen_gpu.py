@@ -150,6 +150,7 @@ def test_tile_batch_and_autotuner(cuda, tmp_path, monkeypatch):
     cfg, stages = tune.tune(day, mets[2], repeats=1)
     assert (cfg.shadow_bx, cfg.shadow_by) in tune.SHADOW_BLOCKS
     assert cfg.gvf_rows in tune.GVF_ROWS and cfg.rad_threads in tune.RAD_THREADS
+    assert cfg.gvf_hours in tune.GVF_HOURS
     assert set(stages) >= {"day_shadow_kernel", "day_gvf_kernel", "day_radiation_kernel"}
     assert tune.lookup(day).astuple() == cfg.astuple()
     tb = batched.TileBatch(scenes, lats, [0.0] * 3, configs=[cfg] * 3)
@@ -159,3 +160,36 @@ def test_tile_batch_and_autotuner(cuda, tmp_path, monkeypatch):
         ref = batched.ChosenDay(s, lat, 0.0, 3.0, 0.0).run_day(met)
         torch.cuda.synchronize()
         assert torch.equal(o["tmrt"], ref["tmrt"])
+
+
+def test_hour_vectorized_gvf_matches_per_hour_kernel(cuda):
+    """Interior tiles through the hour-vectorized GVF kernel against the
+    per-hour kernel everywhere: GVF planes of every daytime hour and the day's
+    Tmrt.  The scene is large enough for interior 32 x 32 tiles."""
+    import torch
+    from solweig_cuda_b200 import _lib, batched, engine, synthetic
+    s = synthetic.make_scene(150, 134, seed=17)
+    scene = engine.Scene(s.dsm, s.trees, s.dem, 1.0, landcover=s.landcover)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, seed=2)
+    res = {}
+    for hv in (0, 1):
+        day = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+        cfg = _lib.SolweigDayConfig.default()
+        cfg.gvf_hours = hv
+        day.set_config(cfg)
+        out = {k: v.clone() for k, v in day.run_day(met).items()}
+        torch.cuda.synchronize()
+        o = day.work_offsets()
+        n = scene.pixels
+        gvf = day.work[o["gvf"]:o["gvf"] + 12 * 24 * n].view(torch.float32).view(24, 3, n).clone()
+        nosh = day.work[o["nosh"]:o["nosh"] + 4 * n].view(torch.float32).clone()
+        res[hv] = (out, gvf, nosh, [h.daytime for h, _, _ in day.plan(met)])
+    (o0, g0, n0, dayflags), (o1, g1, n1, _) = res[0], res[1]
+    torch.testing.assert_close(n1, n0, rtol=1e-6, atol=1e-6)
+    for h, d in enumerate(dayflags):
+        if d:
+            # Lup (W/m2): float32 sums in another order; albedo: albedo*shadow rounded per sample
+            torch.testing.assert_close(g1[h, 0], g0[h, 0], rtol=1e-5, atol=1e-3)
+            torch.testing.assert_close(g1[h, 1], g0[h, 1], rtol=1e-5, atol=1e-6)
+            assert torch.equal(g1[h, 2], g0[h, 2])
+    assert torch.max(torch.abs(o1["tmrt"] - o0["tmrt"])).item() <= 1e-3
