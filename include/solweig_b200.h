@@ -85,6 +85,10 @@ typedef struct SolweigScene {
     int32_t landcover;        /* 1 = land-cover maps in use (enables Tg clamp / water) */
     int32_t has_water;        /* any flags bit2 set */
     double hmax;              /* max over the raster of dsm, vegdem, vegdem2 */
+    /* optional: float4 (dsm, vegdem, vegdem2, 0) per pixel, set only when every
+       value of the three rasters is exactly representable in float32 (the
+       hourly shadow sweep then loads one 16-byte sample per step); NULL otherwise */
+    const void* geo32;
 } SolweigScene;
 
 /* Per-patch constants of the sky-vault layout (host arrays, copied per call). */

@@ -34,7 +34,7 @@ class SolweigScene(ctypes.Structure):
         ("tmaxlst", _vp), ("svfbuveg", _vp), ("svfalfa", _vp), ("tan_asvf", _vp), ("masks", _vp),
         ("veg_sums", _vp), ("sky_band_counts", _vp), ("gvf_face", _vp), ("svf_dir", _vp),
         ("patches", ctypes.c_int32), ("nbands", ctypes.c_int32), ("landcover", ctypes.c_int32),
-        ("has_water", ctypes.c_int32), ("hmax", ctypes.c_double),
+        ("has_water", ctypes.c_int32), ("hmax", ctypes.c_double), ("geo32", _vp),
     ]
 
 

@@ -30,9 +30,12 @@ __device__ __forceinline__ void shadow_quad_pixel(const SolweigScene& S, const S
     const double a = S.dsm[p];
     const double wall = S.walls[p];
     const uint8_t fl = S.flags[p];
+    const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
     const ShadowResult s =
-        shadow_walk(S.dsm, S.vegdem, S.vegdem2, S.rows, S.cols, r, c, a, S.vegdem[p], (fl & 2) != 0,
-                    wall, reinterpret_cast<const int2*>(h.ray_dxdy), h.ray_dz, h.steps, S.hmax, true);
+        S.geo32 ? shadow_walk_geo(GeoF32x4{reinterpret_cast<const float4*>(S.geo32)}, S.rows, S.cols, r, c, a,
+                                  S.vegdem[p], (fl & 2) != 0, wall, ray, h.ray_dz, h.steps, S.hmax, true)
+                : shadow_walk(S.dsm, S.vegdem, S.vegdem2, S.rows, S.cols, r, c, a, S.vegdem[p], (fl & 2) != 0,
+                              wall, ray, h.ray_dz, h.steps, S.hmax, true);
     // Wall sunlit height (only needed for the sunlit-wall bit of the GVF).
     const double wallbol = wall > 0.0 ? 1.0 : 0.0;
     const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);

@@ -32,11 +32,38 @@ struct ShadowResult {
     bool shadowed, veg, ever;
 };
 
+// Height samples of the sweep: the three float64 rasters ...
+struct GeoF64 {
+    const double* __restrict__ dsm;
+    const double* __restrict__ top;
+    const double* __restrict__ bot;
+    __device__ __forceinline__ void load(long long q, bool vegetation, double& a, double& t, double& b) const {
+        a = __ldg(&dsm[q]);
+        if (vegetation) {
+            t = __ldg(&top[q]);
+            b = __ldg(&bot[q]);
+        }
+    }
+};
+
+// ... or, when every value of all three is exactly representable in float32,
+// one interleaved (dsm, canopy, trunk, 0) float4 per pixel: a single 16-byte
+// load per step, widened to float64 exactly, so every compare is unchanged.
+struct GeoF32x4 {
+    const float4* __restrict__ geo;
+    __device__ __forceinline__ void load(long long q, bool, double& a, double& t, double& b) const {
+        const float4 v = __ldg(&geo[q]);
+        a = v.x;
+        t = v.y;
+        b = v.z;
+    }
+};
+
 // Walk the ray for pixel (r, c).  `is_wall` enables the wall-specific
 // continuation rules; `hmax` = max over the raster of dsm, vegdem and vegdem2.
-__device__ __forceinline__ ShadowResult shadow_walk(
-    const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
-    int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,
+template <typename Geo>
+__device__ __forceinline__ ShadowResult shadow_walk_geo(
+    const Geo& geo, int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,
     const int2* __restrict__ ray, const double* __restrict__ dz, int steps, double hmax,
     bool vegetation) {
     ShadowResult s;
@@ -59,11 +86,12 @@ __device__ __forceinline__ ShadowResult shadow_walk(
             break;
         }
         const long long q = (long long)rr * cols + cc;
-        const double aq = __ldg(&dsm[q]) - dzk;
+        double hq, tq = 0.0, bq = 0.0;
+        geo.load(q, vegetation, hq, tq, bq);
+        const double aq = hq - dzk;
         s.f = fmax(s.f, aq);
         s.shadowed = s.f > a;
         if (vegetation) {
-            const double tq = __ldg(&top[q]), bq = __ldg(&bot[q]);
             s.topmax = fmax(s.topmax, tq - dzk);
             if (s.shadowed) {
                 s.veg = false;
@@ -91,6 +119,15 @@ __device__ __forceinline__ ShadowResult shadow_walk(
         }
     }
     return s;
+}
+
+__device__ __forceinline__ ShadowResult shadow_walk(
+    const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
+    int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,
+    const int2* __restrict__ ray, const double* __restrict__ dz, int steps, double hmax,
+    bool vegetation) {
+    return shadow_walk_geo(GeoF64{dsm, top, bot}, rows, cols, r, c, a, top_p, bush, wall, ray, dz, steps, hmax,
+                           vegetation);
 }
 
 // Self-shadowed wall faces (facesh) for the sun window (low, high, middle).

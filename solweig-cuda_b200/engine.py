@@ -463,7 +463,21 @@ class Scene:
         s.landcover = self.landcover
         s.has_water = self.has_water
         s.hmax = self.hmax
+        self.geo32 = self._packed_geometry()
+        s.geo32 = self.geo32.data_ptr() if self.geo32 is not None else None
         return s
+
+    def _packed_geometry(self):
+        """(dsm, vegdem, vegdem2, 0) as float4 per pixel when all three rasters
+        are exactly representable in float32 (the sweep then loads one sample
+        per step); None otherwise."""
+        stack = torch.stack((self.dsm, self.vegdem, self.vegdem2), dim=-1)
+        packed = stack.to(torch.float32)
+        if not bool(torch.equal(packed.to(torch.float64), stack)):
+            return None
+        geo = torch.zeros(self.shape + (4,), dtype=torch.float32, device=self.dsm.device)
+        geo[..., :3] = packed
+        return geo
 
     # The 15 SVF planes in the reference's svf_calculator order, float32-rounded.
     SVF_ORDER = ("svf", "svfE", "svfS", "svfW", "svfN", "svfveg", "svfEveg", "svfSveg", "svfWveg",

@@ -193,3 +193,32 @@ def test_hour_vectorized_gvf_matches_per_hour_kernel(cuda):
             torch.testing.assert_close(g1[h, 1], g0[h, 1], rtol=1e-5, atol=1e-6)
             assert torch.equal(g1[h, 2], g0[h, 2])
     assert torch.max(torch.abs(o1["tmrt"] - o0["tmrt"])).item() <= 1e-3
+
+
+def test_packed_float32_geometry_is_bit_identical(scene64):
+    """The sweep's packed float4 geometry (used when the three height rasters
+    are exact in float32) gives the same shadow quads, bit for bit, as the
+    float64 rasters."""
+    import torch
+    from solweig_cuda_b200 import batched, synthetic
+    sc, scene = scene64
+    assert scene.geo32 is not None  # the generator's heights are float32 values
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    quads = {}
+    saved = scene.struct.geo32
+    try:
+        for packed in (True, False):
+            scene.struct.geo32 = saved if packed else None
+            day = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, use_graph=False)
+            day.run_day(met)
+            torch.cuda.synchronize()
+            o = day.work_offsets()
+            quads[packed] = day.work[o["quads"]:o["quads"] + 16 * 24 * scene.pixels].clone()
+    finally:
+        scene.struct.geo32 = saved
+    flags = [h.daytime for h, _, _ in day.plan(met)]
+    q1 = quads[True].view(torch.int32).view(24, -1)
+    q0 = quads[False].view(torch.int32).view(24, -1)
+    for h, d in enumerate(flags):
+        if d:
+            assert torch.equal(q1[h], q0[h]), h
