@@ -197,6 +197,16 @@ int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
                 const uint8_t* sectors /* [patches] bit d: E,S,W,N */,
                 double transmissivity, uint32_t* masks, double* planes,
                 float* veg_sums, uint8_t* sky_band_counts, void* stream);
+/* solweig_svf with the optional packed float4 (dsm, vegdem, vegdem2, 0)
+ * geometry of SolweigScene.geo32 (exact float32 values; NULL = the float64
+ * rasters): one 16-byte load per ray step, identical masks. */
+int solweig_svf_ex(const double* dsm, const double* vegdem, const double* vegdem2,
+                   const void* geo32, const uint8_t* flags, int rows, int cols, int patches,
+                   int capacity, const int32_t* ray_dxdy, const double* ray_dz,
+                   const int32_t* lengths, double hmax, const SolweigSkyLayout* layout,
+                   const double* band_weights, const uint8_t* sectors, double transmissivity,
+                   uint32_t* masks, double* planes, float* veg_sums, uint8_t* sky_band_counts,
+                   void* stream);
 /* Annulus sums of packed masks (the reduce half of solweig_svf). */
 int solweig_svf_reduce(const uint32_t* masks, const double* vegdem2, int64_t pixels,
                        const SolweigSkyLayout* layout, const double* band_weights,

@@ -118,7 +118,7 @@ EXPORTED_SYMBOLS = (
     "solweig_day_batched", "solweig_day_batched_work_bytes", "solweig_day_batched_error",
     "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex",
     "solweig_day_batched_layout", "solweig_day_grad_work_bytes", "solweig_day_grad_forward",
-    "solweig_day_grad_backward",
+    "solweig_day_grad_backward", "solweig_svf_ex",
 )
 
 _lock = threading.Lock()
@@ -139,6 +139,8 @@ def _declare(lib):
         "solweig_shadow": (i32, [P, P, P, i32, dbl, dbl, i32, i32, P, P]),
         "solweig_svf": (i32, [P, P, P, P, i32, i32, i32, i32, P, P, P, dbl, P, P, P, dbl, P, P, P, P,
                               P]),
+        "solweig_svf_ex": (i32, [P, P, P, P, P, i32, i32, i32, i32, P, P, P, dbl, P, P, P, dbl, P, P, P,
+                                 P, P]),
         "solweig_svf_unpack": (i32, [P, i64, i32, P, P, P, P]),
         "solweig_diffsh": (i32, [P, P, P, i64, fl, P]),
         "solweig_gvf": (i32, [P, P, P, P, dbl, dbl, dbl, dbl, dbl, P, i32, i32, P, P, P]),

@@ -22,8 +22,9 @@ def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixe
 
     form: "chosen" (batched day, tensor-core patch sums), "batched" (per-hour
     kernels in one launch sequence) or "plain" (per-hour loop)."""
-    arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in (dsm, trees, dem)]
-    lc = None if landcover is None else np.ascontiguousarray(landcover, dtype=np.float64)
+    # rasters are uploaded in their own dtype and widened on the device
+    arrays = [np.ascontiguousarray(a) for a in (dsm, trees, dem)]
+    lc = None if landcover is None else np.ascontiguousarray(landcover)
     h2d = sum(a.nbytes for a in arrays) + (lc.nbytes if lc is not None else 0)
     scene = engine.Scene(arrays[0], arrays[1], arrays[2], pixel_size, landcover=lc, device=device)
     met = np.asarray(met, dtype=np.float64)

@@ -23,10 +23,11 @@ struct SvfRayParams {
 };
 
 // grid.x: chunks of 32 consecutive pixels; grid.y: patch word (32 patches).
+// geo32: the packed float4 geometry (exact float32 values) or null.
 __global__ void __launch_bounds__(32 * kSvfWarps) svf_visibility_kernel(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
-    const uint8_t* __restrict__ flags, SvfRayParams prm, const int2* __restrict__ ray,
-    const double* __restrict__ dz, const int32_t* __restrict__ lengths,
+    const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
+    const int2* __restrict__ ray, const double* __restrict__ dz, const int32_t* __restrict__ lengths,
     uint32_t* __restrict__ masks) {
     __shared__ uint8_t state[kSvfPatchGroup][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -43,8 +44,11 @@ __global__ void __launch_bounds__(32 * kSvfWarps) svf_visibility_kernel(
         uint8_t st = 0;
         if (valid && patch < prm.patches) {
             const long long base = (long long)patch * prm.capacity;
-            ShadowResult s = shadow_walk(dsm, top, bot, prm.rows, prm.cols, r, c, a, top_p, bush,
-                                         0.0, ray + base, dz + base, lengths[patch], prm.hmax, true);
+            const ShadowResult s =
+                geo32 ? shadow_walk_geo(GeoF32x4{geo32}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
+                                        dz + base, lengths[patch], prm.hmax, true)
+                      : shadow_walk(dsm, top, bot, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
+                                    dz + base, lengths[patch], prm.hmax, true);
             st = (s.shadowed ? 0 : 1) | (s.ever ? 2 : 0);
         }
         state[j][lane] = st;
@@ -243,13 +247,13 @@ extern "C" int solweig_svf_pack(const float* shmat, const float* vegmat, const f
     return SOLWEIG_OK;
 }
 
-extern "C" int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
-                           const uint8_t* flags, int rows, int cols, int patches, int capacity,
-                           const int32_t* ray_dxdy, const double* ray_dz, const int32_t* lengths,
-                           double hmax, const SolweigSkyLayout* layout,
-                           const double* band_weights, const uint8_t* sectors,
-                           double transmissivity, uint32_t* masks, double* planes,
-                           float* veg_sums, uint8_t* sky_band_counts, void* stream) {
+extern "C" int solweig_svf_ex(const double* dsm, const double* vegdem, const double* vegdem2,
+                              const void* geo32, const uint8_t* flags, int rows, int cols, int patches,
+                              int capacity, const int32_t* ray_dxdy, const double* ray_dz,
+                              const int32_t* lengths, double hmax, const SolweigSkyLayout* layout,
+                              const double* band_weights, const uint8_t* sectors, double transmissivity,
+                              uint32_t* masks, double* planes, float* veg_sums, uint8_t* sky_band_counts,
+                              void* stream) {
     SOLWEIG_CHECK_ARG(dsm && vegdem && vegdem2 && flags && ray_dxdy && ray_dz && lengths && layout &&
                           band_weights && sectors && masks && planes && veg_sums && sky_band_counts,
                       "solweig_svf: null pointer");
@@ -270,11 +274,23 @@ extern "C" int solweig_svf(const double* dsm, const double* vegdem, const double
     const int words = (patches + 31) / 32;
     dim3 grid(blocks_for(pixels, 32), words);
     svf_visibility_kernel<<<grid, 32 * kSvfWarps, 0, st>>>(
-        dsm, vegdem, vegdem2, flags, rp, reinterpret_cast<const int2*>(ray_dxdy), ray_dz, lengths,
-        masks);
+        dsm, vegdem, vegdem2, reinterpret_cast<const float4*>(geo32), flags, rp,
+        reinterpret_cast<const int2*>(ray_dxdy), ray_dz, lengths, masks);
     SOLWEIG_CHECK_LAUNCH("svf_visibility_kernel");
     return solweig_svf_reduce(masks, vegdem2, pixels, layout, band_weights, sectors, transmissivity,
                               planes, veg_sums, sky_band_counts, stream);
+}
+
+extern "C" int solweig_svf(const double* dsm, const double* vegdem, const double* vegdem2,
+                           const uint8_t* flags, int rows, int cols, int patches, int capacity,
+                           const int32_t* ray_dxdy, const double* ray_dz, const int32_t* lengths,
+                           double hmax, const SolweigSkyLayout* layout,
+                           const double* band_weights, const uint8_t* sectors,
+                           double transmissivity, uint32_t* masks, double* planes,
+                           float* veg_sums, uint8_t* sky_band_counts, void* stream) {
+    return solweig_svf_ex(dsm, vegdem, vegdem2, nullptr, flags, rows, cols, patches, capacity, ray_dxdy, ray_dz,
+                          lengths, hmax, layout, band_weights, sectors, transmissivity, masks, planes, veg_sums,
+                          sky_band_counts, stream);
 }
 
 extern "C" int solweig_svf_unpack(const uint32_t* masks, int64_t pixels, int patches, float* shmat,

@@ -122,6 +122,19 @@ def _upload(arr, dtype, device):
     return torch.from_numpy(np.ascontiguousarray(arr, dtype=dtype)).to(device, non_blocking=False)
 
 
+def _raster_to_device(x, device):
+    """A 2-D raster (numpy in any real dtype, torch tensor, or anything with
+    __cuda_array_interface__) as a contiguous float64 device tensor; host
+    arrays are copied in their own dtype and widened on the device."""
+    if isinstance(x, torch.Tensor):
+        t = x.to(device=device)
+    elif hasattr(x, "__cuda_array_interface__"):
+        t = torch.as_tensor(x, device=device)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(x)).to(device)
+    return t.to(torch.float64).contiguous()
+
+
 def _as_device(x, dtype, device, shape):
     """Any array-like (numpy, torch, __cuda_array_interface__, scalar) as a
     contiguous device tensor of ``shape`` (scalars are broadcast)."""
@@ -209,6 +222,35 @@ def wall_aspect(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
     return aspect, walls
 
 
+def wall_aspect_device(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
+    """Wall aspect in degrees as a float64 device tensor (``src/walls.py:83-129``):
+    the template kernel on the device, the gradient fall-back only at the few
+    wall pixels the templates leave unresolved (from ``dsm_host`` when given)."""
+    rows, cols = dsm_dev.shape
+    key = float(pixel_size)
+    if key not in _TEMPLATE_CACHE:
+        _TEMPLATE_CACHE[key] = _aspect_templates(pixel_size)
+    radius, size, packed = _TEMPLATE_CACHE[key]
+    mask = walls_dev > 0
+    aspect = torch.zeros_like(dsm_dev)
+    if not bool(mask.any()):
+        return aspect
+    if rows > 2 * radius + 2 and cols > 2 * radius + 2:
+        dev = dsm_dev.device
+        t = [(_upload(o, np.int32, dev), _upload(s, np.int32, dev)) for o, s in packed]
+        _lib.check(_lib.lib().solweig_wall_aspect(
+            device_ptr(dsm_dev), device_ptr(walls_dev), device_ptr(aspect), rows, cols, radius,
+            device_ptr(t[0][0]), device_ptr(t[0][1]), device_ptr(t[1][0]), device_ptr(t[1][1]),
+            device_ptr(t[2][0]), device_ptr(t[2][1]), stream_handle(stream)), "solweig_wall_aspect")
+    unresolved = torch.nonzero((mask & (aspect == 0)).flatten()).flatten()
+    if unresolved.numel():
+        host = dsm_host if dsm_host is not None else dsm_dev.cpu().numpy()
+        fix = _gradient_aspect(host, pixel_size, unresolved.cpu().numpy())
+        flat = aspect.view(-1)
+        flat[unresolved] = flat[unresolved] + torch.from_numpy(fix).to(aspect.device)
+    return aspect
+
+
 def _gradient_aspect(dsm, pixel_size, flat_idx):
     """``-arctan2(fx, fy)`` in degrees at selected pixels, numpy.gradient semantics."""
     rows, cols = dsm.shape
@@ -228,8 +270,8 @@ def _gradient_aspect(dsm, pixel_size, flat_idx):
         out[hi] = (get(idx[hi], hi) - get(idx[hi] - 1, hi)) / step
         return out
 
-    fy = grad(rows, r, lambda ri, sel: dsm[ri, c[sel]])
-    fx = grad(cols, c, lambda ci, sel: dsm[r[sel], ci])
+    fy = grad(rows, r, lambda ri, sel: np.asarray(dsm[ri, c[sel]], dtype=np.float64))
+    fx = grad(cols, c, lambda ci, sel: np.asarray(dsm[r[sel], ci], dtype=np.float64))
     g = -np.arctan2(fx, fy)
     g[g < 0] += 2 * np.pi
     return 1 * (g / (math.pi / 180.0))
@@ -242,47 +284,47 @@ class Scene:
                  patch_option=2, device="cuda", walls=None, aspect=None, stream=None,
                  keep_planes=False):
         _require_cuda()
-        dsm = np.asarray(dsm, dtype=np.float64)
-        trees = np.asarray(trees, dtype=np.float64)
-        dem = np.asarray(dem, dtype=np.float64)
-        if dsm.ndim != 2 or dsm.shape != trees.shape or dsm.shape != dem.shape:
-            raise ValueError("dsm, trees and dem must be 2-D arrays of the same shape")
-        if landcover is not None and np.shape(landcover) != dsm.shape:
-            raise ValueError("landcover must have the raster's shape")
         self.device = torch.device(device)
-        self.shape = dsm.shape
-        self.rows, self.cols = dsm.shape
-        self.pixels = dsm.size
+        dev = self.device
+        # Rasters go to the device in their own dtype and are widened there.
+        dsm_in = _raster_to_device(dsm, dev)
+        trees_in = _raster_to_device(trees, dev)
+        dem_in = _raster_to_device(dem, dev)
+        if dsm_in.dim() != 2 or dsm_in.shape != trees_in.shape or dsm_in.shape != dem_in.shape:
+            raise ValueError("dsm, trees and dem must be 2-D arrays of the same shape")
+        if landcover is not None and tuple(np.shape(landcover)) != tuple(dsm_in.shape):
+            raise ValueError("landcover must have the raster's shape")
+        self.shape = tuple(dsm_in.shape)
+        self.rows, self.cols = self.shape
+        self.pixels = self.rows * self.cols
         self.pixel_size = float(pixel_size)
         self.scale = 1 / self.pixel_size
         self.layout = SkyLayout(patch_option)
         self.patch_option = int(patch_option)
         L = _lib.lib()
         st = stream_handle(stream)
-        dev = self.device
         n = self.pixels
-        dsm_in = _upload(dsm, np.float64, dev)
         # Walls from the unraised DSM, rounded through float32 (src/series.py:213-236).
         if walls is None:
             walls_dev = wall_heights_device(dsm_in, wall_threshold, stream)
-            aspect, walls = wall_aspect(dsm, dsm_in, walls_dev, pixel_size, stream)
-        walls = np.asarray(walls, dtype=np.float64).astype(np.float32).astype(np.float64)
-        aspect = np.asarray(aspect, dtype=np.float64).astype(np.float32).astype(np.float64)
-        self.walls_host = walls
-        self.aspect_host = aspect
-        self.walls = _upload(walls, np.float64, dev)
-        self.aspect = _upload(aspect * np.pi / 180., np.float64, dev)
-        # Raise / clip semantics of src/series.py:252-291, computed on the host copy.
-        raise_dsm = max(0.0, -float(dsm.min()))
-        raise_dem = max(0.0, -float(dem.min()))
-        a = dsm + raise_dsm if raise_dsm else dsm
-        t1 = np.where(trees < 0., 0., trees)
-        self.amaxvalue = float(max(a.max() - a.min(), t1.max()))
-        self.dsm_max = float(a.max())
-        self.hmax = float(a.max() + max(t1.max(), 0.0))
-        trees_in = _upload(trees, np.float64, dev)
-        dem_in = _upload(dem, np.float64, dev)
-        lc_in = _upload(landcover, np.float64, dev) if landcover is not None else None
+            aspect_dev = wall_aspect_device(dsm if isinstance(dsm, np.ndarray) else None, dsm_in, walls_dev,
+                                            pixel_size, stream)
+        else:
+            walls_dev = _raster_to_device(walls, dev)
+            aspect_dev = _raster_to_device(aspect, dev)
+        self.walls = walls_dev.to(torch.float32).to(torch.float64)
+        self._aspect_deg = aspect_dev.to(torch.float32).to(torch.float64)
+        self.aspect = ((self._aspect_deg * math.pi) / 180.).contiguous()
+        del walls_dev, aspect_dev
+        # Raise / clip semantics of src/series.py:252-291.
+        raise_dsm = max(0.0, -float(dsm_in.min()))
+        raise_dem = max(0.0, -float(dem_in.min()))
+        a_min, a_max = float(dsm_in.min()) + raise_dsm, float(dsm_in.max()) + raise_dsm
+        t1_max = float(trees_in.clamp_min(0.).max())
+        self.amaxvalue = float(max(a_max - a_min, t1_max))
+        self.dsm_max = a_max
+        self.hmax = float(a_max + max(t1_max, 0.0))
+        lc_in = _raster_to_device(landcover, dev) if landcover is not None else None
         self.landcover = 1 if landcover is not None else 0
         f64 = dict(dtype=torch.float64, device=dev)
         f32 = dict(dtype=torch.float32, device=dev)
@@ -327,8 +369,9 @@ class Scene:
         self.veg_sums = torch.empty((4, self.rows, self.cols), **f32)
         self.sky_band_counts = torch.empty((nb, self.rows, self.cols), dtype=torch.uint8, device=dev)
         lay = self.layout
-        _lib.check(L.solweig_svf(
-            device_ptr(self.dsm), device_ptr(self.vegdem), device_ptr(self.vegdem2),
+        self.geo32 = self._packed_geometry()
+        _lib.check(L.solweig_svf_ex(
+            device_ptr(self.dsm), device_ptr(self.vegdem), device_ptr(self.vegdem2), device_ptr(self.geo32),
             device_ptr(self.flags), self.rows, self.cols, lay.struct.patches, cap,
             device_ptr(t_dxdy), device_ptr(t_dz), device_ptr(t_len), self.hmax,
             ctypes.byref(lay.struct), lay.band_weights.ctypes.data_as(ctypes.c_void_p),
@@ -388,8 +431,7 @@ class Scene:
         self.walls = f64(inputs["walls"])
         dirwalls = f64(inputs["dirwalls"])
         self.aspect = (dirwalls * np.pi / 180.).contiguous()
-        self.walls_host = self.walls.cpu().numpy()
-        self.aspect_host = dirwalls.cpu().numpy()
+        self._aspect_deg = dirwalls
         bush = f64(inputs["bush"])
         buildings = f64(inputs["buildings"])
         lc = f64(inputs.get("lc_grid", 0.0))
@@ -463,7 +505,9 @@ class Scene:
         s.landcover = self.landcover
         s.has_water = self.has_water
         s.hmax = self.hmax
-        self.geo32 = self._packed_geometry()
+        if getattr(self, "geo32", None) is None and not getattr(self, "_geo_checked", False):
+            self.geo32 = self._packed_geometry()
+        self._geo_checked = True
         s.geo32 = self.geo32.data_ptr() if self.geo32 is not None else None
         return s
 
@@ -478,6 +522,16 @@ class Scene:
         geo = torch.zeros(self.shape + (4,), dtype=torch.float32, device=self.dsm.device)
         geo[..., :3] = packed
         return geo
+
+    @property
+    def walls_host(self):
+        """Wall heights, float64 host array (float32-rounded values)."""
+        return self.walls.cpu().numpy()
+
+    @property
+    def aspect_host(self):
+        """Wall aspect in degrees, float64 host array (float32-rounded values)."""
+        return self._aspect_deg.cpu().numpy()
 
     # The 15 SVF planes in the reference's svf_calculator order, float32-rounded.
     SVF_ORDER = ("svf", "svfE", "svfS", "svfW", "svfN", "svfveg", "svfEveg", "svfSveg", "svfWveg",
