@@ -7,6 +7,8 @@ UTCI copied back into pinned host memory.
 """
 from __future__ import annotations
 
+import threading
+
 import numpy as np
 import torch
 
@@ -15,13 +17,31 @@ from .batched import BatchedDay, ChosenDay
 
 __all__ = ["simulate_day"]
 
+# Page-locked host buffers for the results, reused across calls: page-locking
+# hundreds of megabytes on every call costs several times the day itself.
+_PINNED = {}
+_PINNED_LOCK = threading.Lock()
+
+
+def _pinned(name, shape):
+    key = (name, tuple(shape))
+    with _PINNED_LOCK:
+        buf = _PINNED.get(key)
+        if buf is None:
+            buf = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+            _PINNED[key] = buf
+    return buf
+
 
 def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixel_size=1.0,
-                 site_altitude=3.0, utc=0.0, device="cuda", form="chosen"):
+                 site_altitude=3.0, utc=0.0, device="cuda", form="chosen", reuse_output=True):
     """Returns {"tmrt": [H, rows, cols] float32, "utci": ..., "h2d_bytes", "d2h_bytes"}.
 
     form: "chosen" (batched day, tensor-core patch sums), "batched" (per-hour
-    kernels in one launch sequence) or "plain" (per-hour loop)."""
+    kernels in one launch sequence) or "plain" (per-hour loop).
+    reuse_output: the returned arrays live in page-locked buffers that the
+    next call with the same shape overwrites (copy them to keep them); False
+    page-locks fresh buffers for every call."""
     # rasters are uploaded in their own dtype and widened on the device
     arrays = [np.ascontiguousarray(a) for a in (dsm, trees, dem)]
     lc = None if landcover is None else np.ascontiguousarray(landcover)
@@ -40,7 +60,8 @@ def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixe
     out = {}
     d2h = 0
     for k in ("tmrt", "utci"):
-        host = torch.empty(res[k].shape, dtype=torch.float32, pin_memory=True)
+        host = (_pinned(k, res[k].shape) if reuse_output
+                else torch.empty(res[k].shape, dtype=torch.float32, pin_memory=True))
         host.copy_(res[k], non_blocking=True)
         out[k] = host
         d2h += host.numel() * 4

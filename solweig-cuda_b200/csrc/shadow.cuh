@@ -14,10 +14,12 @@
 // The per-pixel loop below evaluates these recurrences in the same float64
 // operations, so every mask is bit-identical to the reference, and stops early
 // when the remaining steps provably change nothing:
-//   * hmax - dz_{k-1} <= dsm_p   -> no later sample can rise above the pixel
-//     (and, for wall pixels, hmax - dz_k <= topmax so the canopy top is final);
-//     only taken when dsm_p >= 0 (and topmax >= 0), so the zero-valued samples
-//     beyond the raster edge could not change anything either;
+//   * hmax - dz_{k-1} < dsm_p (exactly) -> no later sample can rise above the
+//     pixel (and, for wall pixels, hmax - dz_k <= topmax so the canopy top is
+//     final); only taken when dsm_p >= 0 (and topmax >= 0), so the zero-valued
+//     samples beyond the raster edge could not change anything either;
+//   * a sample without canopy (top, trunk <= 0) skips the canopy compares
+//     (with dsm_p >= 0 and topmax >= 0 they cannot change anything);
 //   * shadowed and not a wall pixel -> every output is final;
 //   * shadowed wall pixel with f - dsm_p >= wall -> wallsun is already 0.
 // Once a sample leaves the raster it never re-enters (the offsets grow
@@ -73,6 +75,11 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
     s.veg = bush;
     s.ever = false;
     const bool is_wall = wall > 0.0;
+    // dz_prev >= clear  =>  hmax - dz_prev < a in exact arithmetic (the
+    // threshold is one ulp above the rounded difference), so no later sample
+    // of any of the three rasters can rise above the pixel.
+    const double clear = a >= 0.0 ? nextafter(hmax - a, __longlong_as_double(0x7ff0000000000000ll))
+                                  : __longlong_as_double(0x7ff0000000000000ll);
     double dz_prev = 0.0;
     int k = 0;
     for (; k < steps; ++k) {
@@ -81,7 +88,7 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
         const int rr = r + o.x, cc = c + o.y;
         if (!in_raster(rr, cc, rows, cols)) break;
         // Early exits that cannot change any output.
-        if (a >= 0.0 && hmax - dz_prev <= a && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
+        if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
             k = steps;  // nothing further can change; no outside fix-up needed
             break;
         }
@@ -92,14 +99,21 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
         s.f = fmax(s.f, aq);
         s.shadowed = s.f > a;
         if (vegetation) {
-            s.topmax = fmax(s.topmax, tq - dzk);
-            if (s.shadowed) {
-                s.veg = false;
+            if (tq <= 0.0 && bq <= 0.0 && a >= 0.0 && s.topmax >= 0.0) {
+                // No canopy at this sample: its shifted tops are <= 0 <= a and
+                // cannot raise topmax, so only the carried flags move.
+                if (s.shadowed) s.veg = false;
+                else s.ever = s.ever || s.veg;
             } else {
-                const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
-                              (int)(bq - dz_prev > a);
-                s.veg = s.veg || (n > 0 && n < 4);
-                s.ever = s.ever || s.veg;
+                s.topmax = fmax(s.topmax, tq - dzk);
+                if (s.shadowed) {
+                    s.veg = false;
+                } else {
+                    const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
+                                  (int)(bq - dz_prev > a);
+                    s.veg = s.veg || (n > 0 && n < 4);
+                    s.ever = s.ever || s.veg;
+                }
             }
         }
         if (s.shadowed && (!is_wall || s.f - a >= wall)) {

@@ -24,7 +24,7 @@ struct SvfRayParams {
 
 // grid.x: chunks of 32 consecutive pixels; grid.y: patch word (32 patches).
 // geo32: the packed float4 geometry (exact float32 values) or null.
-__global__ void __launch_bounds__(32 * kSvfWarps) svf_visibility_kernel(
+__global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
     const int2* __restrict__ ray, const double* __restrict__ dz, const int32_t* __restrict__ lengths,
