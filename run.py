@@ -3,6 +3,7 @@
     python run.py --case case.json [--output DIR] [--dtype float32|float64]
                   [--output-core ROW COL ROWS COLS] [--output-chunk-steps N]
                   [--sync-output] [--output-queue-size N] [--no-write] [--progress]
+                  [--check]
 
 Case keys follow the reference's ``examples/case.json`` (paths relative to the
 case file).  Rasters are ``.npy`` arrays (GeoTIFF where rasterio/GDAL is
@@ -81,8 +82,14 @@ def main(argv=None):
     parser.add_argument("--output-queue-size", type=int)
     parser.add_argument("--no-write", action="store_true")
     parser.add_argument("--progress", action=argparse.BooleanOptionalAction, default=True)
+    parser.add_argument("--check", action="store_true",
+                        help="validate case.json and the forcing first (the reference's input_check rules)")
     args = parser.parse_args(argv)
     case_path = args.case.resolve()
+    if args.check:
+        from solweig_cuda_b200 import input_check
+        checked, _ = input_check.check_case(case_path)
+        input_check.check_weather(checked["met_file"])
     case, settings = load_case(case_path)
     if settings["case_type"] == "open_data":
         missing = [k for k in ("building_dsm_path", "tree_path", "dem_path", "met_file")
