@@ -129,14 +129,15 @@ class ChosenDay(BatchedDay):
         self.graph = None
 
     def _sequence(self):
+        # Each day starts from the reset state (src/series.py:425-436): the
+        # batched kernel starts from zero state when no state planes are given,
+        # and nothing needs the day's final state.
         self.buffers.upload(0, self.hours, self.buffers.kmax)
-        for t in self.state.values():
-            t.zero_()
         sc = self.scene
         base = outputs_struct(self.out, 0)
         _lib.check(_lib.lib().solweig_day_batched_ex(
             ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
-            ctypes.byref(self._state_struct()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
+            ctypes.byref(_lib.SolweigState()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
             sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes,
             ctypes.byref(self.config), stream_handle()), "solweig_day_batched_ex")
 
@@ -175,14 +176,12 @@ class ChosenDay(BatchedDay):
         recorded on the launching stream between the stages."""
         self.plan(met)
         self.buffers.upload(0, self.hours, self.buffers.kmax)
-        for t in self.state.values():
-            t.zero_()
         sc = self.scene
         base = outputs_struct(self.out, 0)
         ms = (ctypes.c_float * len(self.STAGES))()
         _lib.check(_lib.lib().solweig_day_batched_timed(
             ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
-            ctypes.byref(self._state_struct()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
+            ctypes.byref(_lib.SolweigState()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
             sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes,
             ctypes.byref(self.config), stream_handle(), ms), "solweig_day_batched_timed")
         self.buffers.mark()
@@ -259,13 +258,9 @@ class MultiDay:
         sc = self.scene
         L = _lib.lib()
         self.buffers.upload(0, self.days * self.hours, self.buffers.kmax)
-        st = _lib.SolweigState()
-        for k in _lib.STATE_FIELDS:
-            setattr(st, k, self.state[k].data_ptr())
+        st = _lib.SolweigState()  # zero state at the start of every day
         hsize = self.buffers.hsize
         for d in range(self.days):
-            for t in self.state.values():
-                t.zero_()
             base = outputs_struct(self.out, d * self.hours)
             hours_ptr = ctypes.c_void_p(self.buffers.h_dev.data_ptr() + d * self.hours * hsize)
             _lib.check(L.solweig_day_batched_ex(
@@ -342,11 +337,7 @@ class TileBatch:
         for s, b, lay, state, out, cfg in zip(self.scenes, self.buffers, self.layouts, self.state, self.out,
                                               self.configs):
             b.upload(0, self.hours, b.kmax)
-            st = _lib.SolweigState()
-            st.tgmap1 = state["tgmap1"].data_ptr()
-            st.tgout1 = state["tgout1"].data_ptr()
-            for t in state.values():
-                t.zero_()
+            st = _lib.SolweigState()  # zero state at the start of the day
             base = outputs_struct(out, 0)
             _lib.check(L.solweig_day_batched_ex(
                 ctypes.byref(s.struct), device_ptr(lay), b.ptr(), self.hours, ctypes.byref(st),

@@ -682,10 +682,16 @@ struct DayRadArgs {
 };
 
 
-struct HourSmem {
+// 16-byte aligned (and so a multiple of 16 bytes): stage_hour copies the table
+// with 16-byte stores into both elements of the double buffer.
+struct __align__(16) HourSmem {
     DayTable table;
     float band_down[SOLWEIG_MAX_BANDS], band_side[SOLWEIG_MAX_BANDS];
+    // hour scalars of the flux arithmetic, rounded once from the float64 plan
+    float lw_shade, lw_sun, sw_shade, sw_sun, rad_d, rad_g, direct_up, rad_i_sin, rad_i_cos, rad_ratio;
+    float wave_w, tan_zen, night_lup, night_lup_water;
 };
+static_assert(sizeof(HourSmem) % 16 == 0, "HourSmem must keep 16-byte alignment in an array");
 
 __device__ __forceinline__ void stage_hour(HourSmem& hs, const DayRadArgs& a, int hr) {
     const uint4* src = reinterpret_cast<const uint4*>(a.tables + hr);
@@ -699,12 +705,54 @@ __device__ __forceinline__ void stage_hour(HourSmem& hs, const DayRadArgs& a, in
         hs.band_down[b] = ok ? h.band_lsky[b] * L.band_omega[b] * L.band_sin[b] : 0.f;
         hs.band_side[b] = ok ? h.band_lsky[b] * L.band_omega[b] * L.band_cos[b] : 0.f;
     }
+    if (threadIdx.x == 32) {
+        const SolweigHour& h = a.hours[hr];
+        const double tk = h.ta + 273.15;
+        hs.lw_shade = (float)((0.9 * kSBC * pow4(tk)) / kPi);
+        hs.lw_sun = h.daytime ? (float)((0.9 * kSBC * pow4(h.ta + h.tgwall + 273.15)) / kPi) : 0.f;
+        hs.sw_shade = (float)((0.2 * h.rad_d * 0.5) / kPi);
+        hs.sw_sun = (float)((0.2 * (h.rad_i * h.cos_alt) + h.rad_d * 0.5) / kPi);
+        hs.rad_d = (float)h.rad_d;
+        hs.rad_g = (float)h.rad_g;
+        hs.direct_up = (float)(h.rad_i * h.sin_alt);
+        hs.rad_i_sin = (float)(h.rad_i * h.sin_alt);
+        hs.rad_i_cos = (float)(h.rad_i * h.cos_alt);
+        hs.rad_ratio = (float)(h.rad_d / h.rad_tot);
+        hs.wave_w = (float)h.wave_weight;
+        hs.tan_zen = (float)h.tan_zen;
+        hs.night_lup = (float)(kSBC * pow4(tk));
+        hs.night_lup_water = (float)(kSBC * 0.98 * pow4(h.twater + 273.15));
+    }
 }
 
 __device__ __forceinline__ float* hour_plane(float* base, int hr, long long stride) {
     return base ? base + hr * stride : nullptr;
 }
 
+// Fraction of shaded wall (cylindric_wedge, NaN -> 0.5) in float32.
+__device__ __forceinline__ float wedge_fsh_f(float ta, float tan_zen) {
+    const float xa = 1.f - 2.f / (ta * tan_zen);
+    const float ha = 2.f / (ta * tan_zen);
+    const float ba = 1.f / ta;
+    const float hkil = 2.f * ba * ha;
+    float ukil = 0.f;
+    if (xa < 0.f) {
+        const float qa = tan_zen / 2.f;
+        const float za = sqrtf(ba * ba - qa * qa / 4.f);
+        const float phi = atanf(za / qa);
+        const float cphi = cosf(phi);
+        const float area = (sinf(phi) - phi * cphi) / (1.f - cphi);
+        ukil = 2.f * ba * xa * area;
+    }
+    const float pi2 = 2.f * (float)kPi;
+    const float fsh = (pi2 * ba - (hkil + ukil)) / (pi2 * ba);
+    return isnan(fsh) ? 0.5f : fsh;
+}
+
+// Flux arithmetic of the hour loop in float32 (the hour's scalars are
+// staged once per block, rounded from the float64 host plan); the building
+// split keeps its exact float64 thresholds.  Against the per-hour form
+// (float64 fluxes) Tmrt differs by < 1e-3 K (tested).
 template <int OPT, int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(SolweigScene S, DayRadArgs a) {
     __shared__ HourSmem hsm[2];
@@ -721,6 +769,8 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(S
     const long long p = (long long)blockIdx.x * THREADS + threadIdx.x;
     const bool in = p < n;
     const long long q = in ? p : 0;  // a valid pixel for the loads of idle threads
+    const SolweigOutputs& o = a.out;
+    const bool need_tg = o.tg || o.tg_out || a.state.tgout1;
 
     // --- per-pixel static data, loaded once for the day
     uint32_t bld[SOLWEIG_MASK_WORDS];
@@ -739,17 +789,17 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(S
     const uint8_t fl = S.flags[q];
     const bool ground = fl & 1;
     const bool water = S.has_water && (fl & 4);
-    const double emis = S.emis[q];
-    const float tgk = S.tgk[q], tstart = S.tstart[q], tmaxlst = S.tmaxlst[q];
-    const double svfbuveg = S.svfbuveg[q];
-    const double tan_alfa = tan(S.svfalfa[q]);
+    const float emis = S.emis[q];
+    const float svfbuveg = S.svfbuveg[q];
+    const float tan_alfa = (float)tan(S.svfalfa[q]);
     const double tan_asvf = S.tan_asvf[q];
-    const double vc = S.veg_sums[q], vs = S.veg_sums[n + q];
-    const double oc = S.veg_sums[2 * n + q], os = S.veg_sums[3 * n + q];
-    const double g_nosh = a.nosh[q];
-    constexpr double ewall = 0.9, albedo_b = 0.2;
-    constexpr double absK = 0.7, absL = 0.95, Fside = 0.22, Fup = 0.06, Fcyl = 0.28;
-    const double dsh_veg = 1.0 - (1.0 - 0.03);
+    const float vc = S.veg_sums[q], vs = S.veg_sums[n + q];
+    const float oc = S.veg_sums[2 * n + q], os = S.veg_sums[3 * n + q];
+    const float g_nosh = a.nosh[q];
+    constexpr float ewall = 0.9f, albedo_b = 0.2f;
+    constexpr float absK = 0.7f, absL = 0.95f, Fside = 0.22f, Fup = 0.06f, Fcyl = 0.28f;
+    constexpr float dsh_veg = 0.03f;
+    constexpr float sbc = (float)kSBC, inv_pi = (float)(1.0 / kPi);
 
     float st_lup = a.state.tgmap1 ? a.state.tgmap1[q] : 0.f;
     float st_tg = a.state.tgout1 ? a.state.tgout1[q] : 0.f;
@@ -760,8 +810,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(S
         if (hr + 1 < a.nhours) stage_hour(hsm[(hr + 1) & 1], a, hr + 1);
         const SolweigHour& h = a.hours[hr];
         const bool day = h.daytime != 0;
-        const double ta = h.ta;
-        const double tk = ta + 273.15;
+        const float ta = (float)h.ta;
 
         // building patches: sunlit / shaded split of the hour
         const DayTable& T = hs.table;
@@ -780,86 +829,83 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(S
         }
         const float lw_sun_c = band_weighted<OPT>(m_lsun, wcos), lw_sun_s = band_weighted<OPT>(m_lsun, wsin);
         const float lw_shd_c = band_weighted<OPT>(m_lshd, wcos), lw_shd_s = band_weighted<OPT>(m_lshd, wsin);
-        double ld_sky = 0.0, ls_sky = 0.0;
+        float ld_sky = 0.f, ls_sky = 0.f;
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
-            const double cnt = (double)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
-            ld_sky += (double)hs.band_down[b] * cnt;
-            ls_sky += (double)hs.band_side[b] * cnt;
+            const float cnt = (float)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
+            ld_sky = fmaf(hs.band_down[b], cnt, ld_sky);
+            ls_sky = fmaf(hs.band_side[b], cnt, ls_sky);
         }
-        const double lw_shade = (ewall * kSBC * pow4(tk)) / kPi;
-        const double lw_sun = day ? (ewall * kSBC * pow4(ta + h.tgwall + 273.15)) / kPi : 0.0;
+        const float lw_shade = hs.lw_shade, lw_sun = hs.lw_sun;
 
-        double shadow = 0.0, tg = 0.0, tg_out = ta;
-        double kup_all = 0.0, lup_all;
-        double kdown = 0.0, kside = 0.0, kside_i = 0.0, kside_d = 0.0, d_rad = 0.0;
+        float shadow = 0.f, tg = 0.f, tg_out = ta;
+        float kup_all = 0.f, lup_all;
+        float kdown = 0.f, kside = 0.f, kside_i = 0.f, kside_d = 0.f, d_rad = 0.f;
         if (day) {
             const long long g0 = (3LL * hr) * n + q;
-            const double g_lup = a.gvf[g0];
-            const double g_alb = a.gvf[g0 + n];
+            const float g_lup = a.gvf[g0];
+            const float g_alb = a.gvf[g0 + n];
             shadow = a.gvf[g0 + 2 * n];
-            const double fsh = wedge_fsh_tan(tan_alfa, h.tan_zen);
-            const double reflected = albedo_b * (1.0 - svfbuveg) * (h.rad_g * (1.0 - fsh) + h.rad_d * fsh);
-            const double base_up = h.rad_d * svfbuveg + reflected;
-            const double direct_up = h.rad_i * h.sin_alt;
-            kup_all = g_alb * direct_up + base_up * g_nosh;
-            const double prev = h.firstdaytime ? g_lup : (double)st_lup;
-            lup_all = g_lup * (1.0 - h.wave_weight) + prev * h.wave_weight;
-            st_lup = (float)(h.wave_update ? lup_all : prev);
-            // ground temperature (TsWaveDelay of Tg * shadow + Ta)
-            const double amp = (double)tgk * h.altmax + (double)tstart;
-            const double phase =
-                ((h.dectime_frac - h.snup / 24.0) / ((double)tmaxlst / 24.0 - h.snup / 24.0)) * kPi / 2.0;
-            tg = amp * sin(phase) * h.ci_tgg;
-            if (S.landcover == 1 && tg < 0.0) tg = 0.0;
-            if (water) tg = h.twater - ta;
-            {
-                const double cur = tg * shadow + ta;
-                const double prv = h.firstdaytime ? cur : (double)st_tg;
-                tg_out = cur * (1.0 - h.wave_weight) + prv * h.wave_weight;
-                st_tg = (float)(h.wave_update ? tg_out : prv);
+            const float fsh = wedge_fsh_f(tan_alfa, hs.tan_zen);
+            const float reflected = albedo_b * (1.f - svfbuveg) * (hs.rad_g * (1.f - fsh) + hs.rad_d * fsh);
+            const float base_up = hs.rad_d * svfbuveg + reflected;
+            kup_all = g_alb * hs.direct_up + base_up * g_nosh;
+            const float prev = h.firstdaytime ? g_lup : st_lup;
+            lup_all = g_lup * (1.f - hs.wave_w) + prev * hs.wave_w;
+            st_lup = h.wave_update ? lup_all : prev;
+            if (need_tg) {
+                // ground temperature (TsWaveDelay of Tg * shadow + Ta); not part of Tmrt
+                const double amp = (double)S.tgk[q] * h.altmax + (double)S.tstart[q];
+                const double phase = ((h.dectime_frac - h.snup / 24.0) /
+                                      ((double)S.tmaxlst[q] / 24.0 - h.snup / 24.0)) * kPi / 2.0;
+                double tgd = amp * sin(phase) * h.ci_tgg;
+                if (S.landcover == 1 && tgd < 0.0) tgd = 0.0;
+                if (water) tgd = h.twater - h.ta;
+                tg = (float)tgd;
+                const float cur = tg * shadow + ta;
+                const float prv = h.firstdaytime ? cur : st_tg;
+                tg_out = cur * (1.f - hs.wave_w) + prv * hs.wave_w;
+                st_tg = h.wave_update ? tg_out : prv;
             }
             const long long s0 = 2LL * hr;
-            const double lum_sky = a.sums[s0 * n + q], cw_sky = a.sums[(s0 + 1) * n + q];
-            const double lum_veg = a.sums[(a.ncols + s0) * n + q], cw_veg = a.sums[(a.ncols + s0 + 1) * n + q];
-            d_rad = h.rad_d * (lum_sky + dsh_veg * lum_veg);
-            kdown = h.rad_i * shadow * h.sin_alt + d_rad + reflected;
-            kside_i = shadow * h.rad_i * h.cos_alt;
-            kside_d = (h.rad_d / h.rad_tot) * (cw_sky + dsh_veg * cw_veg);
-            const double sw_shade = (albedo_b * h.rad_d * 0.5) / kPi;
-            const double sw_sun = (albedo_b * (h.rad_i * h.cos_alt) + h.rad_d * 0.5) / kPi;
-            kside = kside_i + kside_d + sw_sun * (double)band_weighted<OPT>(m_sun, wcos) +
-                    sw_shade * (double)band_weighted<OPT>(m_shd, wcos) + sw_shade * vc;
+            const float lum_sky = a.sums[s0 * n + q], cw_sky = a.sums[(s0 + 1) * n + q];
+            const float lum_veg = a.sums[(a.ncols + s0) * n + q], cw_veg = a.sums[(a.ncols + s0 + 1) * n + q];
+            d_rad = hs.rad_d * (lum_sky + dsh_veg * lum_veg);
+            kdown = hs.rad_i_sin * shadow + d_rad + reflected;
+            kside_i = shadow * hs.rad_i_cos;
+            kside_d = hs.rad_ratio * (cw_sky + dsh_veg * cw_veg);
+            kside = kside_i + kside_d + hs.sw_sun * band_weighted<OPT>(m_sun, wcos) +
+                    hs.sw_shade * band_weighted<OPT>(m_shd, wcos) + hs.sw_shade * vc;
         } else {
-            double lup = kSBC * emis * pow4(ta + 0.0 + 273.15);
-            if (S.landcover == 1 && (fl & 4)) lup = kSBC * 0.98 * pow4(h.twater + 273.15);
+            float lup = emis * hs.night_lup;
+            if (S.landcover == 1 && (fl & 4)) lup = hs.night_lup_water;
             lup_all = lup;
         }
-        const double refl = ((ld_sky + lup_all) * (1.0 - ewall) * 0.5) / kPi;
-        const double ldown = ld_sky + lw_shade * vs + lw_shade * (double)lw_shd_s + lw_sun * (double)lw_sun_s + refl * os;
-        const double lside = ls_sky + lw_shade * vc + lw_shade * (double)lw_shd_c + lw_sun * (double)lw_sun_c + refl * oc;
+        const float refl = (ld_sky + lup_all) * ((1.f - ewall) * 0.5f * inv_pi);
+        const float ldown = ld_sky + lw_shade * vs + lw_shade * lw_shd_s + lw_sun * lw_sun_s + refl * os;
+        const float lside = ls_sky + lw_shade * vc + lw_shade * lw_shd_c + lw_sun * lw_sun_c + refl * oc;
         // E+S+W+N of Kup and Lup are 4x the all-direction values (see the file header).
-        const double sstr = absK * (kside * Fcyl + (kdown + kup_all) * Fup + 2.0 * kup_all * Fside) +
-                            absL * ((ldown + lup_all) * Fup + lside * Fcyl + 2.0 * lup_all * Fside);
-        const double tmrt = sqrt(sqrt(sstr / (absL * kSBC))) - 273.2;
+        const float sstr = absK * (kside * Fcyl + (kdown + kup_all) * Fup + 2.f * kup_all * Fside) +
+                           absL * ((ldown + lup_all) * Fup + lside * Fcyl + 2.f * lup_all * Fside);
+        const float tmrt = sqrtf(sqrtf(sstr * (1.f / (absL * sbc)))) - 273.2f;
         if (in) {
-            const SolweigOutputs& o = a.out;
             const long long hs_ = a.hour_stride;
-            if (o.tmrt) o.tmrt[hr * hs_ + p] = (float)tmrt;
+            if (o.tmrt) o.tmrt[hr * hs_ + p] = tmrt;
             if (o.utci)
-                o.utci[hr * hs_ + p] = ground ? utci_eval(h.utci, tmrt, ta, h.utci_valid) : __int_as_float(0x7fc00000);
-            if (o.kdown) o.kdown[hr * hs_ + p] = (float)kdown;
-            if (o.kup) o.kup[hr * hs_ + p] = (float)kup_all;
-            if (o.ldown) o.ldown[hr * hs_ + p] = (float)ldown;
-            if (o.lup) o.lup[hr * hs_ + p] = (float)lup_all;
-            if (o.lside) o.lside[hr * hs_ + p] = (float)lside;
-            if (o.kside_i) o.kside_i[hr * hs_ + p] = (float)kside_i;
-            if (o.kside_d) o.kside_d[hr * hs_ + p] = (float)kside_d;
-            if (o.kside) o.kside[hr * hs_ + p] = (float)kside;
-            if (o.d_rad) o.d_rad[hr * hs_ + p] = (float)d_rad;
-            if (o.shadow) o.shadow[hr * hs_ + p] = (float)shadow;
-            if (o.tg) o.tg[hr * hs_ + p] = (float)tg;
-            if (o.tg_out) o.tg_out[hr * hs_ + p] = (float)tg_out;
+                o.utci[hr * hs_ + p] = ground ? utci_eval(h.utci, (double)tmrt, h.ta, h.utci_valid)
+                                              : __int_as_float(0x7fc00000);
+            if (o.kdown) o.kdown[hr * hs_ + p] = kdown;
+            if (o.kup) o.kup[hr * hs_ + p] = kup_all;
+            if (o.ldown) o.ldown[hr * hs_ + p] = ldown;
+            if (o.lup) o.lup[hr * hs_ + p] = lup_all;
+            if (o.lside) o.lside[hr * hs_ + p] = lside;
+            if (o.kside_i) o.kside_i[hr * hs_ + p] = kside_i;
+            if (o.kside_d) o.kside_d[hr * hs_ + p] = kside_d;
+            if (o.kside) o.kside[hr * hs_ + p] = kside;
+            if (o.d_rad) o.d_rad[hr * hs_ + p] = d_rad;
+            if (o.shadow) o.shadow[hr * hs_ + p] = shadow;
+            if (o.tg) o.tg[hr * hs_ + p] = tg;
+            if (o.tg_out) o.tg_out[hr * hs_ + p] = tg_out;
         }
     }
     if (in) {
