@@ -506,7 +506,7 @@ def main():
 
     sun_alt = __import__("solweig_cuda_b200.sun", fromlist=["metdata"]).metdata(met, 53.0, 0.0, 3.0, 0.0).altitude
     # our kernels per timed day: 7 for the batched form, shadow/GVF/radiation per hour otherwise
-    launches_per_day = 7 if a.form == "chosen" else 3 * len(met)
+    launches_per_day = chosen.launches_per_day if a.form == "chosen" else 3 * len(met)
     plain_times = timed(plain, max(1, min(a.steps, 3)), 1)
     with ClockSampler(local) as clocks:
         chosen_times = timed(chosen, a.steps, a.warmup)

@@ -40,7 +40,11 @@ class BatchedDay:
                     for k in self.out_names}
         self.use_graph = use_graph
         self.graph = None
-        self.launches_per_day = 2 * hours
+
+    @property
+    def launches_per_day(self):
+        """Shadow, GVF and radiation kernel of every hour."""
+        return 3 * self.hours
 
     def _state_struct(self):
         s = _lib.SolweigState()
@@ -93,6 +97,13 @@ class BatchedDay:
         return {k: self.out[k] for k in names}
 
 
+def day_launches(scene, config):
+    """Kernel launches of one batched day for this scene and launch shapes."""
+    hv = config.gvf_hours == 1 and not scene.struct.has_water and scene.first_steps == 1 \
+        and scene.second_steps == 22
+    return 8 if hv else 7
+
+
 class ChosenDay(BatchedDay):
     """The batched form: every hour of a day in seven launches
     (``solweig_day_batched``: per-launch shadow and GVF over all hours, the
@@ -118,8 +129,13 @@ class ChosenDay(BatchedDay):
         if self.work_bytes <= 0:
             raise ValueError("bad batched-day shape")
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=scene.device)
-        self.launches_per_day = 7
         self.config = _lib.SolweigDayConfig.default()
+
+    @property
+    def launches_per_day(self):
+        """Kernels of one day: shadow, GVF (+ the hour-vectorized interior
+        kernel), weights, split, tables, contraction, radiation."""
+        return day_launches(self.scene, self.config)
 
     def set_config(self, config):
         """Launch shapes (``SolweigDayConfig`` or a 5-tuple); drops a captured graph."""
@@ -240,7 +256,7 @@ class MultiDay:
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=dev)
         self.config = config if config is not None else _lib.SolweigDayConfig.default()
         self.graph = None
-        self.launches = 7 * days
+        self.launches = day_launches(scene, self.config) * days
 
     def plan(self, met):
         met = np.asarray(met, dtype=np.float64)
@@ -317,7 +333,7 @@ class TileBatch:
                     for s in self.scenes]
         self.configs = list(configs) if configs is not None else [_lib.SolweigDayConfig.default()] * n
         self.graph = None
-        self.launches = 7 * n
+        self.launches = sum(day_launches(s_, c) for s_, c in zip(self.scenes, self.configs))
 
     @property
     def pixels(self):
