@@ -34,7 +34,34 @@ struct DayTable {
     uint32_t pre[kK + 1][SOLWEIG_MASK_WORDS];  // patches at sorted shaded positions <  j
     uint32_t test[SOLWEIG_MASK_WORDS];         // longwave sun test of the hour
     uint32_t pad[5];
+    // first sorted position whose threshold is >= bucket boundary i (see
+    // tan_bucket): the counts of thresholds <= t start there for t in bucket i
+    uint8_t sun_start[256];
+    uint8_t shd_start[256];
 };
+
+// 256 buckets of tan(asvf): boundary i = tan(i * pi / 512) for i >= 1,
+// -inf for i = 0 (the same float64 expression wherever it is evaluated).
+__device__ __forceinline__ double tan_bucket_bound(int i) {
+    return i == 0 ? __longlong_as_double(0xfff0000000000000ll) : tan((double)i * (kPi / 512.0));
+}
+
+// Largest i with tan_bucket_bound(i) <= t.
+__device__ __forceinline__ int tan_bucket(double t) {
+    int i = (int)(atan(t) * (512.0 / kPi));
+    i = i < 0 ? 0 : (i > 255 ? 255 : i);
+    while (i < 255 && tan_bucket_bound(i + 1) <= t) ++i;
+    while (i > 0 && tan_bucket_bound(i) > t) --i;
+    return i;
+}
+
+// Number of entries of the ascending a[0..n) that are <= t, starting from
+// `from` = the number of entries below the bucket boundary of t.
+__device__ __forceinline__ int count_le_from(const double* a, int n, int from, double t) {
+    int i = from;
+    while (i < n && a[i] <= t) ++i;
+    return i;
+}
 static_assert(sizeof(DayTable) % 16 == 0, "DayTable must be a multiple of 16 bytes");
 
 // Band boundaries (patch index) of the sky layouts the batched form supports.
@@ -517,6 +544,17 @@ __global__ void __launch_bounds__(kK) day_tables_kernel(const SolweigSkyLayout* 
         }
         T.test[k] = t;
     }
+    __syncthreads();  // sorted arrays complete
+    for (int i = k; i < 256; i += blockDim.x) {
+        const double bound = tan_bucket_bound(i);
+        int ns = 0, nv = 0;
+        for (int j = 0; j < P; ++j) {
+            ns += T.tsun[j] < bound ? 1 : 0;
+            nv += T.vshade[j] < bound ? 1 : 0;
+        }
+        T.sun_start[i] = (uint8_t)ns;
+        T.shd_start[i] = (uint8_t)nv;
+    }
 }
 
 // ------------------------------------------------------------------ kernel 6
@@ -793,6 +831,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(S
     const float svfbuveg = S.svfbuveg[q];
     const float tan_alfa = (float)tan(S.svfalfa[q]);
     const double tan_asvf = S.tan_asvf[q];
+    const int tbucket = tan_bucket(tan_asvf);
     const float vc = S.veg_sums[q], vs = S.veg_sums[n + q];
     const float oc = S.veg_sums[2 * n + q], os = S.veg_sums[3 * n + q];
     const float g_nosh = a.nosh[q];
@@ -815,8 +854,8 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) day_radiation_kernel(S
         // building patches: sunlit / shaded split of the hour
         const DayTable& T = hs.table;
         const int P = S.patches;
-        const int isun = count_le(T.tsun, P, tan_asvf);
-        const int ishd = count_le(T.vshade, P, tan_asvf);
+        const int isun = count_le_from(T.tsun, P, T.sun_start[tbucket], tan_asvf);
+        const int ishd = count_le_from(T.vshade, P, T.shd_start[tbucket], tan_asvf);
         uint32_t m_sun[SOLWEIG_MASK_WORDS], m_shd[SOLWEIG_MASK_WORDS], m_lsun[SOLWEIG_MASK_WORDS],
             m_lshd[SOLWEIG_MASK_WORDS];
 #pragma unroll
