@@ -279,7 +279,7 @@ int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layou
                         int first_steps, int second_steps, void* work, int64_t work_bytes,
                         void* stream);
 /* Launch shapes of the batched day (the autotuner's search space).
- * Defaults (config == NULL): {32, 8, 8, 256, 0, 1}. */
+ * Defaults (config == NULL): {32, 8, 8, 256, 0, 1, 0}. */
 typedef struct SolweigDayConfig {
     int32_t shadow_bx, shadow_by;  /* shadow block: <= 256 threads, a multiple of 32 */
     int32_t gvf_rows;              /* GVF tile rows per block: 4, 8 or 16 (32 columns) */
@@ -288,6 +288,9 @@ typedef struct SolweigDayConfig {
     int32_t gvf_hours;             /* 1: interior 32x32 tiles walk all daytime hours in one
                                       block, 4 hours per pass (1 m walk, no water); 0: one
                                       launch slice per hour everywhere */
+    int32_t no_ceiling;            /* 0: the sweep stops on the per-hour ray ceilings
+                                      (same results, fewer steps); 1: every ray walks
+                                      to its global clearance */
 } SolweigDayConfig;
 int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSkyLayout* layout,
                            const SolweigHour* hours, int nhours, const SolweigState* state,

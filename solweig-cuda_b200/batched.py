@@ -101,7 +101,7 @@ def day_launches(scene, config):
     """Kernel launches of one batched day for this scene and launch shapes."""
     hv = config.gvf_hours == 1 and not scene.struct.has_water and scene.first_steps == 1 \
         and scene.second_steps == 22
-    return 8 if hv else 7
+    return 7 + int(hv) + int(not config.no_ceiling)
 
 
 class ChosenDay(BatchedDay):
@@ -133,12 +133,12 @@ class ChosenDay(BatchedDay):
 
     @property
     def launches_per_day(self):
-        """Kernels of one day: shadow, GVF (+ the hour-vectorized interior
-        kernel), weights, split, tables, contraction, radiation."""
+        """Kernels of one day: ray ceilings, shadow, GVF (+ the hour-vectorized
+        interior kernel), weights, split, tables, contraction, radiation."""
         return day_launches(self.scene, self.config)
 
     def set_config(self, config):
-        """Launch shapes (``SolweigDayConfig`` or a 5-tuple); drops a captured graph."""
+        """Launch shapes (``SolweigDayConfig`` or a tuple of its fields); drops a captured graph."""
         if not isinstance(config, _lib.SolweigDayConfig):
             config = _lib.SolweigDayConfig(*config)
         self.config = config
@@ -161,8 +161,10 @@ class ChosenDay(BatchedDay):
     def stage_bytes(pixels, hours, day_hours):
         """Algorithmic HBM bytes of each stage of one day.
 
-        shadow: per daytime pixel-hour 40 B float64 geometry + 1 B flags + 20 B
-        float32 fields read, 16 B quad written (77 B); GVF: 16 B quad + 4 B face
+        shadow (with the ray ceilings): per daytime pixel-hour 16 B packed
+        geometry read and a 4 B ceiling written and read back, 40 B float64
+        geometry + 1 B flags + 20 B float32 fields read, 16 B quad written
+        (101 B); GVF: 16 B quad + 4 B face
         bits + 4 B emissivity read, 3 planes + the albedo-without-shadow plane
         written (40 B); tables: per-hour tables (negligible); contraction: 40 B
         of mask words per pixel read, 2 x 2 sums per pixel-hour written
@@ -170,7 +172,7 @@ class ChosenDay(BatchedDay):
         day, 28 B per daytime pixel-hour (3 GVF planes, 4 sums) and 8 B per
         pixel-hour written (Tmrt, UTCI)."""
         return {
-            "day_shadow_kernel": pixels * day_hours * 77,
+            "day_shadow_kernel": pixels * day_hours * 101,
             "day_gvf_kernel": pixels * day_hours * 40,
             "day_tables_kernel": hours * 9552,
             "patch_gemm_kernel": pixels * (40 + 16 * hours),

@@ -1,0 +1,222 @@
+// Ray ceilings: per daytime hour, an upper bound at every pixel q of the
+// heights that the rest of a sun ray passing through q can still present,
+// discounted by the ray's rise.  The shadow sweep uses it to stop walking a
+// ray as soon as no later sample can change any of its outputs.
+//
+// The sweep of pixel p visits q_j = p + o_j (j = 0 .. K-1, o_j the ray table)
+// and at step j compares the heights h in {dsm, canopy top, trunk} at q_j
+// against the pixel through h - dz_j and h - dz_{j-1}.  Let H = max(dsm,
+// vegdem, vegdem2).  If a value C(q_k) satisfies, for every pixel p whose ray
+// visits q_k at step k and every later step j >= k,
+//        H(q_j) - dz_{j-1}  <=  C(q_k) - dz_{k-1}                        (*)
+// then C(q_k) - dz_{k-1} < dsm_p means no later sample reaches above the
+// pixel (its shadow height, vegetation flags and, when also <= topmax, the
+// canopy top seen by a wall are final).
+//
+// Construction (all bounds exact, no trigonometry):
+//  * frame: the major axis is the one whose offset equals +-j at every step
+//    (checked over the whole table); X runs along it in the ray direction and
+//    Y along the other axis, oriented so the last offset is >= 0.  Then
+//    X(q_j) = X(q_k) + (j - k) and Y(q_j) = Y(p) + m_j with m_j the minor
+//    offset.
+//  * shear: with v = M / D, M = m_{K-1}, D = K - 1, R(X) = floor(X M / D) in
+//    integers and the sheared line N = Y - R(X).  Along one ray
+//    N(q_j) - N(q_k) = (e_j - e_k) - (R(X_j) - R(X_k) - (j-k) v) with
+//    e_i = m_i - i v, so |N(q_j) - N(q_k)| < spread(e) + 1, i.e. <= W with
+//    W = floor(spread) + 1 (spread measured exactly as D * e_i in integers;
+//    about 1 for the rounded digital rays, so W = 2).
+//  * discount: delta = the smallest increment dz_i - dz_{i-1} of the table
+//    (exact in float64 by Sterbenz), rounded down to float32, so
+//    dz_{j-1} - dz_{k-1} >= (j - k) delta for j >= k >= 1.
+//  * along each sheared line, G(X) = max(Hd(X), G(X+1) - delta) with
+//    Hd(X, N) = max over |d| <= W of H(X, N + d + R(X)) and the subtraction
+//    rounded up, so G(X, N) >= H(X', N') - (X' - X) delta for X' >= X and
+//    |N' - N| <= W: C(q) = G(X(q), N(q)) satisfies (*) for k >= 1.
+//
+// Thread layout: a block owns 32 consecutive sheared lines (one per lane) and
+// splits the major axis into 32 segments (one per warp).  Phase 1 scans each
+// segment backwards from -inf; phase 2 carries the later segments' maxima in
+// and rescans, writing the plane.  Lanes read consecutive Y at one X, so the
+// reads are coalesced when Y is the column axis.
+#pragma once
+#include "common.cuh"
+
+namespace solweig {
+
+constexpr int kCeilLanes = 32;     // sheared lines per block
+constexpr int kCeilWarps = 32;     // major-axis segments per block
+constexpr int kCeilMaxBand = 3;    // largest dilation W handled
+constexpr int kCeilMinSteps = 5;   // the sweep consults the plane from step 4 on
+
+// Upper bound (float32) of max(dsm, vegdem, vegdem2) at pixel p.
+template <bool G32>
+__device__ __forceinline__ float ceiling_height(const SolweigScene& S, long long p) {
+    if (G32) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(S.geo32) + p);
+        return fmaxf(v.x, fmaxf(v.y, v.z));
+    }
+    const double m = fmax(__ldg(&S.dsm[p]), fmax(__ldg(&S.vegdem[p]), __ldg(&S.vegdem2[p])));
+    return __double2float_ru(m);
+}
+
+struct CeilingFrame {
+    int ok;            // 0: the table fits no frame; the plane is +inf
+    int rows_major;    // major axis = rows (else columns)
+    int s_major, s_minor;
+    int nx, nb;        // extents along X (major) and Y (minor)
+    int m, d;          // slope v = m / d of the shear
+    int band;          // dilation W
+    int lines;         // sheared lines: nb + R(nx - 1)
+    float delta;       // per-step discount
+};
+
+// Frame of one hour's ray, derived by the whole block from the table.
+__device__ inline CeilingFrame ceiling_frame(const SolweigScene& S, const int2* __restrict__ ray,
+                                      const double* __restrict__ dz, int K) {
+    __shared__ long long s_emin, s_emax;
+    __shared__ unsigned s_dmin;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    const int2 last = ray[K - 1];
+    const int sr = last.x < 0 ? -1 : 1, sc = last.y < 0 ? -1 : 1;
+    int rows_ok = 1, cols_ok = 1;
+    for (int i = tid; i < K; i += nt) {
+        const int2 o = __ldg(&ray[i]);
+        rows_ok &= (o.x == sr * i);
+        cols_ok &= (o.y == sc * i);
+    }
+    rows_ok = __syncthreads_and(rows_ok);
+    cols_ok = __syncthreads_and(cols_ok);
+    CeilingFrame f{};
+    f.rows_major = rows_ok;
+    f.ok = rows_ok || cols_ok;
+    if (!f.ok) return f;
+    f.s_major = rows_ok ? sr : sc;
+    f.s_minor = rows_ok ? sc : sr;
+    f.nx = rows_ok ? S.rows : S.cols;
+    f.nb = rows_ok ? S.cols : S.rows;
+    f.d = K - 1;
+    f.m = f.s_minor * (rows_ok ? last.y : last.x);  // >= 0
+    if (tid == 0) {
+        s_emin = LLONG_MAX;
+        s_emax = LLONG_MIN;
+        s_dmin = 0x7f800000u;  // +inf
+    }
+    __syncthreads();
+    long long emin = LLONG_MAX, emax = LLONG_MIN;
+    float dmin = __int_as_float(0x7f800000);
+    int inc_ok = 1;
+    for (int i = tid; i < K; i += nt) {
+        const int2 o = __ldg(&ray[i]);
+        const long long mi = (long long)f.s_minor * (rows_ok ? o.y : o.x);
+        const long long e = mi * f.d - (long long)i * f.m;  // D * e_i
+        emin = min(emin, e);
+        emax = max(emax, e);
+        if (i >= 1) {
+            const double inc = __ldg(&dz[i]) - __ldg(&dz[i - 1]);  // exact (Sterbenz)
+            inc_ok &= (inc >= 0.0);                                 // false for NaN too
+            if (inc >= 0.0) dmin = fminf(dmin, __double2float_rd(inc));
+        }
+    }
+    atomicMin(&s_emin, emin);
+    atomicMax(&s_emax, emax);
+    atomicMin(&s_dmin, __float_as_uint(dmin));  // non-negative floats order as integers
+    inc_ok = __syncthreads_and(inc_ok);
+    const long long spread = s_emax - s_emin;  // D * spread(e)
+    f.band = (int)(spread / f.d) + 1;
+    f.delta = __uint_as_float(s_dmin);
+    if (!inc_ok || f.m > f.d || f.band > kCeilMaxBand) {
+        f.ok = 0;
+        return f;
+    }
+    f.lines = f.nb + (int)((long long)(f.nx - 1) * f.m / f.d);
+    return f;
+}
+
+__device__ __forceinline__ long long ceiling_pixel(const CeilingFrame& f, int cols, int x, int y) {
+    const int a = f.s_major > 0 ? x : f.nx - 1 - x;
+    const int b = f.s_minor > 0 ? y : f.nb - 1 - y;
+    return f.rows_major ? (long long)a * cols + b : (long long)b * cols + a;
+}
+
+// Dilated height of this lane's sheared line at X (all lanes of the warp call it).
+template <bool G32, int W>
+__device__ __forceinline__ float ceiling_dilated(const SolweigScene& S, const CeilingFrame& f, int line0, int x) {
+    const int lane = threadIdx.x;
+    const int rx = (int)((long long)x * f.m / f.d);
+    // run element e <-> Y = line0 - W + e + R(X); lane l holds e = l and, for
+    // l < 2W, e = 32 + l
+    const float ninf = __int_as_float(0xff800000);
+    const int y0 = line0 - W + rx + lane;
+    const float c = (y0 >= 0 && y0 < f.nb) ? ceiling_height<G32>(S, ceiling_pixel(f, S.cols, x, y0)) : ninf;
+    float e = ninf;
+    if (lane < 2 * W) {
+        const int y1 = y0 + 32;
+        if (y1 >= 0 && y1 < f.nb) e = ceiling_height<G32>(S, ceiling_pixel(f, S.cols, x, y1));
+    }
+    float hd = c;
+#pragma unroll
+    for (int t = 1; t <= 2 * W; ++t) {
+        const float dn = __shfl_down_sync(0xffffffffu, c, t);
+        const float wr = __shfl_sync(0xffffffffu, e, (lane + t) & 31);
+        hd = fmaxf(hd, lane + t < 32 ? dn : wr);
+    }
+    return hd;
+}
+
+// Both phases for one block of 32 sheared lines (see the file comment).
+template <bool G32, int W>
+__device__ __forceinline__ void ceiling_scan(const SolweigScene& S, const CeilingFrame& f, int line0,
+                                             float (*s_seg)[kCeilLanes], float* __restrict__ out) {
+    const int seg = (f.nx + kCeilWarps - 1) / kCeilWarps;
+    const int w = threadIdx.y;
+    const int x0 = min(f.nx, w * seg), x1 = min(f.nx, x0 + seg);
+    const float ninf = __int_as_float(0xff800000);
+    // phase 1: segment maxima from -inf
+    float g = ninf;
+    for (int x = x1 - 1; x >= x0; --x) g = fmaxf(ceiling_dilated<G32, W>(S, f, line0, x), __fsub_ru(g, f.delta));
+    s_seg[w][threadIdx.x] = g;
+    __syncthreads();
+    // phase 2: carry of the later segments, then the rescan that writes
+    float carry = ninf;
+    for (int s = kCeilWarps - 1; s > w; --s) {
+        const int s0 = min(f.nx, s * seg), s1 = min(f.nx, s0 + seg);
+        carry = fmaxf(s_seg[s][threadIdx.x], __fsub_ru(carry, __fmul_rd((float)(s1 - s0), f.delta)));
+    }
+    g = carry;
+    const int line = line0 + threadIdx.x;
+    for (int x = x1 - 1; x >= x0; --x) {
+        g = fmaxf(ceiling_dilated<G32, W>(S, f, line0, x), __fsub_ru(g, f.delta));
+        const int y = line + (int)((long long)x * f.m / f.d);
+        if (y >= 0 && y < f.nb) out[ceiling_pixel(f, S.cols, x, y)] = g;
+    }
+}
+
+// grid (ceil((rows + cols) / 32), 1, hours), block (32, 32): the ceiling plane
+// of every daytime hour whose ray has at least kCeilMinSteps steps.
+template <bool G32>
+__global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
+    SolweigScene S, const SolweigHour* __restrict__ hours, float* __restrict__ ceiling) {
+    __shared__ float s_seg[kCeilWarps][kCeilLanes];
+    const SolweigHour& h = hours[blockIdx.z];
+    if (!h.daytime || h.steps < kCeilMinSteps) return;
+    const long long n = (long long)S.rows * S.cols;
+    float* out = ceiling + (long long)blockIdx.z * n;
+    const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
+    const CeilingFrame f = ceiling_frame(S, ray, h.ray_dz, h.steps);
+    const int tid = threadIdx.y * kCeilLanes + threadIdx.x;
+    if (!f.ok) {
+        for (long long p = (long long)blockIdx.x * blockDim.x * blockDim.y + tid; p < n;
+             p += (long long)gridDim.x * blockDim.x * blockDim.y)
+            out[p] = __int_as_float(0x7f800000);
+        return;
+    }
+    const int line_first = blockIdx.x * kCeilLanes;
+    if (line_first >= f.lines) return;
+    // lane l owns sheared line N = line_first + l - R(nx - 1)
+    const int line0 = line_first - (f.lines - f.nb);
+    if (f.band == 1) ceiling_scan<G32, 1>(S, f, line0, s_seg, out);
+    else if (f.band == 2) ceiling_scan<G32, 2>(S, f, line0, s_seg, out);
+    else ceiling_scan<G32, 3>(S, f, line0, s_seg, out);
+}
+
+}  // namespace solweig

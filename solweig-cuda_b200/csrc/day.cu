@@ -2,6 +2,8 @@
 // (instead of three per hour), with the luminance-weighted patch sums of all
 // hours as one BF16 tensor-core contraction.
 //
+//  0 day_ray_ceiling_kernel grid.z = hour: upper bounds of the heights ahead
+//                           along the sun ray (early exit of the sweep)
 //  1 day_shadow_kernel      grid.z = hour: shadow sweep + GVF field quads
 //  2 day_gvf_kernel         grid.z = hour: all-direction GVF (Lup, albedo) +
 //                           the pixel's shadow; the hour-independent
@@ -75,7 +77,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
                      int nhours, const SolweigState* state, const SolweigOutputs* base, int64_t hour_stride,
                      const int32_t* gvf_dxdy, int first_steps, int second_steps, void* work,
                      int64_t work_bytes, void* stream, cudaEvent_t* ev, const SolweigDayConfig* cfg_in) {
-    SolweigDayConfig cfg{32, 8, 8, 256, 0, 1};
+    SolweigDayConfig cfg{32, 8, 8, 256, 0, 1, 0};
     if (cfg_in) cfg = *cfg_in;
     SOLWEIG_CHECK_ARG(cfg.shadow_bx > 0 && cfg.shadow_by > 0 && cfg.shadow_bx * cfg.shadow_by <= 256 &&
                           (cfg.shadow_bx * cfg.shadow_by) % 32 == 0,
@@ -88,6 +90,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     SOLWEIG_CHECK_ARG(cfg.gemm_ctas_per_sm >= 0 && cfg.gemm_ctas_per_sm <= 2,
                       "solweig_day_batched: gemm_ctas_per_sm must be 0 (auto), 1 or 2");
     SOLWEIG_CHECK_ARG(cfg.gvf_hours == 0 || cfg.gvf_hours == 1, "solweig_day_batched: gvf_hours must be 0 or 1");
+    SOLWEIG_CHECK_ARG(cfg.no_ceiling == 0 || cfg.no_ceiling == 1, "solweig_day_batched: no_ceiling must be 0 or 1");
     SOLWEIG_CHECK_ARG(scene && layout && hours && base && work, "solweig_day_batched: null argument");
     const SolweigScene& S = *scene;
     SOLWEIG_CHECK_ARG(S.rows > 0 && S.cols > 0, "solweig_day_batched: bad scene shape %dx%d", S.rows, S.cols);
@@ -130,9 +133,18 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     cudaMemsetAsync(err, 0, sizeof(int), st);
     cudaMemsetAsync(nosh, 0, 4 * px, st);
     if (ev) cudaEventRecord(ev[0], st);
+    // The ceiling planes (4 B per pixel-hour) live in the GVF region (12 B per
+    // pixel-hour): the sweep reads them before the GVF kernels write it.
+    float* ceiling = cfg.no_ceiling ? nullptr : gvf;
+    if (ceiling) {
+        dim3 grid(blocks_for((long long)S.rows + S.cols, kCeilLanes), 1, nhours);
+        if (S.geo32) day_ray_ceiling_kernel<true><<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours, ceiling);
+        else day_ray_ceiling_kernel<false><<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours, ceiling);
+        SOLWEIG_CHECK_LAUNCH("day_ray_ceiling_kernel");
+    }
     {
         dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nhours);
-        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(S, hours, quads, lup_first);
+        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(S, hours, quads, lup_first, ceiling);
         SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
     }
     if (ev) cudaEventRecord(ev[1], st);

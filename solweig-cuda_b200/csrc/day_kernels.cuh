@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_bf16.h>
 
+#include "ceiling.cuh"
 #include "gvf_fields.cuh"
 #include "hour.cuh"
 #include "radiation.cuh"
@@ -151,7 +152,8 @@ __device__ double first_true(Pred pred) {
 __global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
                                                                    const SolweigHour* __restrict__ hours,
                                                                    float4* __restrict__ quads,
-                                                                   float* __restrict__ lup_first) {
+                                                                   float* __restrict__ lup_first,
+                                                                   const float* __restrict__ ceiling) {
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
@@ -159,7 +161,8 @@ __global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
     const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (r >= S.rows || c >= S.cols) return;
     const long long n = (long long)S.rows * S.cols;
-    shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr);
+    shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
+                      ceiling ? ceiling + z * n : nullptr);
 }
 
 struct DayGvfArgs {

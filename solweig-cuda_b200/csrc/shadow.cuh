@@ -21,7 +21,11 @@
 //   * a sample without canopy (top, trunk <= 0) skips the canopy compares
 //     (with dsm_p >= 0 and topmax >= 0 they cannot change anything);
 //   * shadowed and not a wall pixel -> every output is final;
-//   * shadowed wall pixel with f - dsm_p >= wall -> wallsun is already 0.
+//   * shadowed wall pixel with f - dsm_p >= wall -> wallsun is already 0;
+//   * with a ray-ceiling plane (ceiling.cuh), every 4th step from step 4 on:
+//     ceiling(q_k) - dz_{k-1} (rounded up) < dsm_p bounds every later
+//     sample's h - dz_{j-1} below the pixel (dsm_p >= 0; for wall pixels
+//     also <= topmax >= 0), so nothing further can change.
 // Once a sample leaves the raster it never re-enters (the offsets grow
 // monotonically), so the first outside step is applied and the loop ends.
 #pragma once
@@ -67,7 +71,7 @@ template <typename Geo>
 __device__ __forceinline__ ShadowResult shadow_walk_geo(
     const Geo& geo, int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,
     const int2* __restrict__ ray, const double* __restrict__ dz, int steps, double hmax,
-    bool vegetation) {
+    bool vegetation, const float* __restrict__ ceiling = nullptr) {
     ShadowResult s;
     s.f = a;
     s.topmax = top_p;
@@ -87,12 +91,19 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
         const double dzk = __ldg(&dz[k]);
         const int rr = r + o.x, cc = c + o.y;
         if (!in_raster(rr, cc, rows, cols)) break;
+        const long long q = (long long)rr * cols + cc;
         // Early exits that cannot change any output.
         if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
             k = steps;  // nothing further can change; no outside fix-up needed
             break;
         }
-        const long long q = (long long)rr * cols + cc;
+        if (ceiling != nullptr && k >= 4 && (k & 3) == 0) {
+            const double e = __dsub_ru((double)__ldg(&ceiling[q]), dz_prev);
+            if (a >= 0.0 && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) {
+                k = steps;
+                break;
+            }
+        }
         double hq, tq = 0.0, bq = 0.0;
         geo.load(q, vegetation, hq, tq, bq);
         const double aq = hq - dzk;

@@ -55,7 +55,7 @@ def _bucket(n):
 def tune_key(runner):
     sc = runner.scene
     name = torch.cuda.get_device_name(sc.device)
-    return f"v2|{name}|{_bucket(sc.rows)}x{_bucket(sc.cols)}|h{runner.hours}|p{sc.struct.patches}"
+    return f"v3|{name}|{_bucket(sc.rows)}x{_bucket(sc.cols)}|h{runner.hours}|p{sc.struct.patches}"
 
 
 def _load():

@@ -222,3 +222,44 @@ def test_packed_float32_geometry_is_bit_identical(scene64):
     for h, d in enumerate(flags):
         if d:
             assert torch.equal(q1[h], q0[h]), h
+
+
+@pytest.mark.parametrize("doy,lat,shift", [(172, 53.0, 0.0), (355, 60.0, 0.0), (80, 10.0, -3.0)])
+def test_ray_ceiling_exit_is_bit_identical(cuda, doy, lat, shift):
+    """The sweep's early exit on the per-hour ray ceilings changes no bit of the
+    shadow quads (shadow, Lup, albedo, ground/sunlit-wall bits) nor of the
+    day's outputs, for packed and float64 geometry, low winter sun (long
+    rays) and a terrain partly below zero (where the exit is never taken)."""
+    import torch
+    from solweig_cuda_b200 import _lib, batched, engine, synthetic
+    s = synthetic.make_scene(150, 134, seed=17)
+    dsm = (s.dsm + np.float32(shift)).astype(np.float32)
+    scene = engine.Scene(dsm, s.trees, s.dem + np.float32(shift), 1.0, landcover=s.landcover)
+    met = synthetic.make_met(doy=doy, latitude=lat, longitude=0.0, seed=5)
+    saved = scene.struct.geo32
+    res = {}
+    try:
+        for packed in (True, False):
+            scene.struct.geo32 = saved if packed else None
+            for no_ceiling in (0, 1):
+                day = batched.ChosenDay(scene, lat, 0.0, 3.0, 0.0, outputs=("tmrt", "utci", "shadow"),
+                                        use_graph=False)
+                cfg = _lib.SolweigDayConfig.default()
+                cfg.no_ceiling = no_ceiling
+                day.set_config(cfg)
+                out = {k: v.clone() for k, v in day.run_day(met).items()}
+                torch.cuda.synchronize()
+                assert day.error_flag() == 0
+                o = day.work_offsets()
+                q = day.work[o["quads"]:o["quads"] + 16 * 24 * scene.pixels].clone()
+                res[packed, no_ceiling] = (out, q.view(torch.int32).view(24, -1))
+    finally:
+        scene.struct.geo32 = saved
+    flags = [h.daytime for h, _, _ in day.plan(met)]
+    for packed in (True, False):
+        (o1, q1), (o0, q0) = res[packed, 0], res[packed, 1]
+        for h, d in enumerate(flags):
+            if d:
+                assert torch.equal(q1[h], q0[h]), (packed, h)
+        for k in o0:  # bit patterns: UTCI is NaN on building pixels
+            assert torch.equal(o1[k].view(torch.int32), o0[k].view(torch.int32)), (packed, k)
