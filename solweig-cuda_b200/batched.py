@@ -101,7 +101,7 @@ def day_launches(scene, config):
     """Kernel launches of one batched day for this scene and launch shapes."""
     hv = config.gvf_hours == 1 and not scene.struct.has_water and scene.first_steps == 1 \
         and scene.second_steps == 22
-    return 7 + int(hv) + int(not config.no_ceiling)
+    return 8 + int(hv) + 2 * int(not config.no_ceiling)
 
 
 class ChosenDay(BatchedDay):
@@ -133,8 +133,9 @@ class ChosenDay(BatchedDay):
 
     @property
     def launches_per_day(self):
-        """Kernels of one day: ray ceilings, shadow, GVF (+ the hour-vectorized
-        interior kernel), weights, split, tables, contraction, radiation."""
+        """Kernels of one day: height dilation and ray ceilings, ray exits,
+        shadow, GVF (+ the hour-vectorized interior kernel), weights, split,
+        tables, contraction, radiation."""
         return day_launches(self.scene, self.config)
 
     def set_config(self, config):

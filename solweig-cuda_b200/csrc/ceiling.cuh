@@ -33,11 +33,18 @@
 //    rounded up, so G(X, N) >= H(X', N') - (X' - X) delta for X' >= X and
 //    |N' - N| <= W: C(q) = G(X(q), N(q)) satisfies (*) for k >= 1.
 //
-// Thread layout: a block owns 32 consecutive sheared lines (one per lane) and
+// The dilation runs along the raster's minor axis only, so it is done once
+// per day (ceiling_dilate_kernel): H dilated by +-1 and +-2 along the columns
+// (row-major planes, for rays whose major axis is the rows) and along the rows
+// (stored transposed, for rays whose major axis is the columns).  Either way
+// the scan reads plane[a * nb + b] with a the oriented major index and b the
+// oriented minor index, so a warp's 32 lanes (consecutive Y) read 32
+// consecutive floats.
+//
+// Scan layout: a block owns 32 consecutive sheared lines (one per lane) and
 // splits the major axis into 32 segments (one per warp).  Phase 1 scans each
 // segment backwards from -inf; phase 2 carries the later segments' maxima in
-// and rescans, writing the plane.  Lanes read consecutive Y at one X, so the
-// reads are coalesced when Y is the column axis.
+// and rescans, writing the plane.
 #pragma once
 #include "common.cuh"
 
@@ -124,11 +131,12 @@ __device__ inline CeilingFrame ceiling_frame(const SolweigScene& S, const int2* 
     const long long spread = s_emax - s_emin;  // D * spread(e)
     f.band = (int)(spread / f.d) + 1;
     f.delta = __uint_as_float(s_dmin);
-    if (!inc_ok || f.m > f.d || f.band > kCeilMaxBand) {
+    // (nx - 1) * m must fit the 32-bit shear cursor
+    if (!inc_ok || f.m > f.d || f.band > kCeilMaxBand || (long long)(f.nx - 1) * f.m > INT_MAX) {
         f.ok = 0;
         return f;
     }
-    f.lines = f.nb + (int)((long long)(f.nx - 1) * f.m / f.d);
+    f.lines = f.nb + (f.nx - 1) * f.m / f.d;
     return f;
 }
 
@@ -138,43 +146,80 @@ __device__ __forceinline__ long long ceiling_pixel(const CeilingFrame& f, int co
     return f.rows_major ? (long long)a * cols + b : (long long)b * cols + a;
 }
 
-// Dilated height of this lane's sheared line at X (all lanes of the warp call it).
-template <bool G32, int W>
-__device__ __forceinline__ float ceiling_dilated(const SolweigScene& S, const CeilingFrame& f, int line0, int x) {
-    const int lane = threadIdx.x;
-    const int rx = (int)((long long)x * f.m / f.d);
-    // run element e <-> Y = line0 - W + e + R(X); lane l holds e = l and, for
-    // l < 2W, e = 32 + l
-    const float ninf = __int_as_float(0xff800000);
-    const int y0 = line0 - W + rx + lane;
-    const float c = (y0 >= 0 && y0 < f.nb) ? ceiling_height<G32>(S, ceiling_pixel(f, S.cols, x, y0)) : ninf;
-    float e = ninf;
-    if (lane < 2 * W) {
-        const int y1 = y0 + 32;
-        if (y1 >= 0 && y1 < f.nb) e = ceiling_height<G32>(S, ceiling_pixel(f, S.cols, x, y1));
+// R(X) = floor(X m / d) while X steps down by one: quotient and remainder
+// carried in 32-bit integers (X m <= rows * cols), no division per step.
+struct ShearCursor {
+    int rx, rem;
+    __device__ __forceinline__ ShearCursor(int x, int m, int d) {
+        const int num = x * m;
+        rx = num / d;
+        rem = num - rx * d;
     }
-    float hd = c;
+    __device__ __forceinline__ void step_down(int m, int d) {  // m <= d
+        rem -= m;
+        if (rem < 0) {
+            rem += d;
+            --rx;
+        }
+    }
+};
+
+constexpr int kCeilBatch = 8;  // samples fetched ahead of the dependent max chain
+
+// H dilated by +-W along the minor axis around Y = y at major index a:
+// plane[a * nb + b].  A line whose centre lies up to W outside the raster
+// still sees its in-raster neighbours: the edge pixel's window covers them.
+__device__ __forceinline__ float ceiling_sample(const float* __restrict__ plane, const CeilingFrame& f, int a, int y) {
+    if (y < -f.band || y >= f.nb + f.band) return __int_as_float(0xff800000);
+    const int yc = min(max(y, 0), f.nb - 1);
+    const int b = f.s_minor > 0 ? yc : f.nb - 1 - yc;
+    return __ldg(&plane[(long long)a * f.nb + b]);
+}
+
+// One backward scan of [x0, x1) from g over the lane's sheared line; with OUT,
+// writes every pixel of the line.  A batch of loads is issued before the
+// dependent chain consumes it.
+template <bool OUT>
+__device__ __forceinline__ float ceiling_run(const float* __restrict__ plane, const CeilingFrame& f, int cols,
+                                             int line, int x0, int x1, float g, float* __restrict__ out) {
+    ShearCursor cur(max(x1 - 1, 0), f.m, f.d);
+    int x = x1 - 1;
+    for (; x - (kCeilBatch - 1) >= x0; x -= kCeilBatch) {
+        float v[kCeilBatch];
+        int y[kCeilBatch];
 #pragma unroll
-    for (int t = 1; t <= 2 * W; ++t) {
-        const float dn = __shfl_down_sync(0xffffffffu, c, t);
-        const float wr = __shfl_sync(0xffffffffu, e, (lane + t) & 31);
-        hd = fmaxf(hd, lane + t < 32 ? dn : wr);
+        for (int u = 0; u < kCeilBatch; ++u) {
+            y[u] = line + cur.rx;
+            const int a = f.s_major > 0 ? x - u : f.nx - 1 - (x - u);
+            v[u] = ceiling_sample(plane, f, a, y[u]);
+            cur.step_down(f.m, f.d);
+        }
+#pragma unroll
+        for (int u = 0; u < kCeilBatch; ++u) {
+            g = fmaxf(v[u], __fsub_ru(g, f.delta));
+            if (OUT && y[u] >= 0 && y[u] < f.nb) out[ceiling_pixel(f, cols, x - u, y[u])] = g;
+        }
     }
-    return hd;
+    for (; x >= x0; --x) {
+        const int yy = line + cur.rx;
+        const int a = f.s_major > 0 ? x : f.nx - 1 - x;
+        g = fmaxf(ceiling_sample(plane, f, a, yy), __fsub_ru(g, f.delta));
+        if (OUT && yy >= 0 && yy < f.nb) out[ceiling_pixel(f, cols, x, yy)] = g;
+        cur.step_down(f.m, f.d);
+    }
+    return g;
 }
 
 // Both phases for one block of 32 sheared lines (see the file comment).
-template <bool G32, int W>
-__device__ __forceinline__ void ceiling_scan(const SolweigScene& S, const CeilingFrame& f, int line0,
-                                             float (*s_seg)[kCeilLanes], float* __restrict__ out) {
+__device__ __forceinline__ void ceiling_scan(const float* __restrict__ plane, const CeilingFrame& f, int cols,
+                                             int line0, float (*s_seg)[kCeilLanes], float* __restrict__ out) {
     const int seg = (f.nx + kCeilWarps - 1) / kCeilWarps;
     const int w = threadIdx.y;
     const int x0 = min(f.nx, w * seg), x1 = min(f.nx, x0 + seg);
+    const int line = line0 + threadIdx.x;
     const float ninf = __int_as_float(0xff800000);
     // phase 1: segment maxima from -inf
-    float g = ninf;
-    for (int x = x1 - 1; x >= x0; --x) g = fmaxf(ceiling_dilated<G32, W>(S, f, line0, x), __fsub_ru(g, f.delta));
-    s_seg[w][threadIdx.x] = g;
+    s_seg[w][threadIdx.x] = ceiling_run<false>(plane, f, cols, line, x0, x1, ninf, nullptr);
     __syncthreads();
     // phase 2: carry of the later segments, then the rescan that writes
     float carry = ninf;
@@ -182,20 +227,58 @@ __device__ __forceinline__ void ceiling_scan(const SolweigScene& S, const Ceilin
         const int s0 = min(f.nx, s * seg), s1 = min(f.nx, s0 + seg);
         carry = fmaxf(s_seg[s][threadIdx.x], __fsub_ru(carry, __fmul_rd((float)(s1 - s0), f.delta)));
     }
-    g = carry;
-    const int line = line0 + threadIdx.x;
-    for (int x = x1 - 1; x >= x0; --x) {
-        g = fmaxf(ceiling_dilated<G32, W>(S, f, line0, x), __fsub_ru(g, f.delta));
-        const int y = line + (int)((long long)x * f.m / f.d);
-        if (y >= 0 && y < f.nb) out[ceiling_pixel(f, S.cols, x, y)] = g;
+    ceiling_run<true>(plane, f, cols, line, x0, x1, carry, out);
+}
+
+// The four dilated planes of H (see the file comment), each rows x cols floats:
+//   dil[0], dil[1]: +-1, +-2 along the columns, row-major [r][c];
+//   dil[2], dil[3]: +-1, +-2 along the rows, transposed [c][r].
+// block (32, 8) over a 32 x 32 tile, H staged with a 2-pixel halo.
+constexpr int kDilTile = 32, kDilHalo = 2, kDilPitch = kDilTile + 2 * kDilHalo + 1;
+
+template <bool G32>
+__global__ void __launch_bounds__(256) ceiling_dilate_kernel(SolweigScene S, float* __restrict__ dil) {
+    __shared__ float tile[kDilTile + 2 * kDilHalo][kDilPitch];
+    const int r0 = blockIdx.y * kDilTile, c0 = blockIdx.x * kDilTile;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const float ninf = __int_as_float(0xff800000);
+    constexpr int side = kDilTile + 2 * kDilHalo;
+    for (int i = tid; i < side * side; i += 256) {
+        const int tr = i / side, tc = i - tr * side;
+        const int r = r0 - kDilHalo + tr, c = c0 - kDilHalo + tc;
+        tile[tr][tc] = (r >= 0 && r < S.rows && c >= 0 && c < S.cols)
+                           ? ceiling_height<G32>(S, (long long)r * S.cols + c) : ninf;
+    }
+    __syncthreads();
+    const long long n = (long long)S.rows * S.cols;
+    // along the columns: thread x = column (row-major writes coalesced)
+    for (int k = threadIdx.y; k < kDilTile; k += 8) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r >= S.rows || c >= S.cols) continue;
+        const float* t = &tile[k + kDilHalo][threadIdx.x + kDilHalo];
+        const float d1 = fmaxf(t[0], fmaxf(t[-1], t[1]));
+        const float d2 = fmaxf(d1, fmaxf(t[-2], t[2]));
+        dil[(long long)r * S.cols + c] = d1;
+        dil[n + (long long)r * S.cols + c] = d2;
+    }
+    // along the rows: thread x = row (transposed writes coalesced)
+    for (int k = threadIdx.y; k < kDilTile; k += 8) {
+        const int r = r0 + threadIdx.x, c = c0 + k;
+        if (r >= S.rows || c >= S.cols) continue;
+        const int tr = threadIdx.x + kDilHalo, tc = k + kDilHalo;
+        const float d1 = fmaxf(tile[tr][tc], fmaxf(tile[tr - 1][tc], tile[tr + 1][tc]));
+        const float d2 = fmaxf(d1, fmaxf(tile[tr - 2][tc], tile[tr + 2][tc]));
+        dil[2 * n + (long long)c * S.rows + r] = d1;
+        dil[3 * n + (long long)c * S.rows + r] = d2;
     }
 }
 
 // grid (ceil((rows + cols) / 32), 1, hours), block (32, 32): the ceiling plane
-// of every daytime hour whose ray has at least kCeilMinSteps steps.
-template <bool G32>
-__global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
-    SolweigScene S, const SolweigHour* __restrict__ hours, float* __restrict__ ceiling) {
+// of every daytime hour whose ray has at least kCeilMinSteps steps, from the
+// dilated planes of ceiling_dilate_kernel.
+static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
+    SolweigScene S, const SolweigHour* __restrict__ hours, const float* __restrict__ dil,
+    float* __restrict__ ceiling) {
     __shared__ float s_seg[kCeilWarps][kCeilLanes];
     const SolweigHour& h = hours[blockIdx.z];
     if (!h.daytime || h.steps < kCeilMinSteps) return;
@@ -204,7 +287,7 @@ __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kerne
     const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
     const CeilingFrame f = ceiling_frame(S, ray, h.ray_dz, h.steps);
     const int tid = threadIdx.y * kCeilLanes + threadIdx.x;
-    if (!f.ok) {
+    if (!f.ok || f.band > 2) {
         for (long long p = (long long)blockIdx.x * blockDim.x * blockDim.y + tid; p < n;
              p += (long long)gridDim.x * blockDim.x * blockDim.y)
             out[p] = __int_as_float(0x7f800000);
@@ -214,9 +297,8 @@ __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kerne
     if (line_first >= f.lines) return;
     // lane l owns sheared line N = line_first + l - R(nx - 1)
     const int line0 = line_first - (f.lines - f.nb);
-    if (f.band == 1) ceiling_scan<G32, 1>(S, f, line0, s_seg, out);
-    else if (f.band == 2) ceiling_scan<G32, 2>(S, f, line0, s_seg, out);
-    else ceiling_scan<G32, 3>(S, f, line0, s_seg, out);
+    const float* plane = dil + (long long)((f.rows_major ? 0 : 2) + (f.band - 1)) * n;
+    ceiling_scan(plane, f, S.cols, line0, s_seg, out);
 }
 
 }  // namespace solweig

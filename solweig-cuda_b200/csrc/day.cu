@@ -2,8 +2,9 @@
 // (instead of three per hour), with the luminance-weighted patch sums of all
 // hours as one BF16 tensor-core contraction.
 //
-//  0 day_ray_ceiling_kernel grid.z = hour: upper bounds of the heights ahead
-//                           along the sun ray (early exit of the sweep)
+//  0 ceiling_dilate_kernel, day_ray_ceiling_kernel (grid.z = hour): upper
+//                           bounds of the heights ahead along the sun ray
+//                           (early exit of the sweep)
 //  1 day_shadow_kernel      grid.z = hour: shadow sweep + GVF field quads
 //  2 day_gvf_kernel         grid.z = hour: all-direction GVF (Lup, albedo) +
 //                           the pixel's shadow; the hour-independent
@@ -134,17 +135,29 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     cudaMemsetAsync(nosh, 0, 4 * px, st);
     if (ev) cudaEventRecord(ev[0], st);
     // The ceiling planes (4 B per pixel-hour) live in the GVF region (12 B per
-    // pixel-hour): the sweep reads them before the GVF kernels write it.
+    // pixel-hour) and the four dilated height planes (16 B per pixel) in the
+    // patch-sum region (at least 16 B per pixel): both are consumed by the
+    // sweep before the GVF kernels and the contraction write those regions.
     float* ceiling = cfg.no_ceiling ? nullptr : gvf;
     if (ceiling) {
+        float* dil = sums;
+        dim3 dgrid(blocks_for(S.cols, kDilTile), blocks_for(S.rows, kDilTile));
+        if (S.geo32) ceiling_dilate_kernel<true><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
+        else ceiling_dilate_kernel<false><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
+        SOLWEIG_CHECK_LAUNCH("ceiling_dilate_kernel");
         dim3 grid(blocks_for((long long)S.rows + S.cols, kCeilLanes), 1, nhours);
-        if (S.geo32) day_ray_ceiling_kernel<true><<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours, ceiling);
-        else day_ray_ceiling_kernel<false><<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours, ceiling);
+        day_ray_ceiling_kernel<<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours, dil, ceiling);
         SOLWEIG_CHECK_LAUNCH("day_ray_ceiling_kernel");
     }
+    // first-outside steps of every row and column per hour (4 B each), in the
+    // GVF region after the ceiling planes (8 B per pixel-hour left there)
+    int* exits = reinterpret_cast<int*>(wb + w.gvf + 4LL * px * nhours);
+    day_ray_exits_kernel<<<nhours, 1024, 0, st>>>(S, hours, exits);
+    SOLWEIG_CHECK_LAUNCH("day_ray_exits_kernel");
     {
         dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nhours);
-        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(S, hours, quads, lup_first, ceiling);
+        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(S, hours, quads, lup_first, ceiling,
+                                                                              exits);
         SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
     }
     if (ev) cudaEventRecord(ev[1], st);
@@ -153,7 +166,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
         fill_day_table(tab, gvf_dxdy, 22, pitch);
         const bool hv = cfg.gvf_hours == 1 && !S.has_water;
         DayGvfArgs gh = ga;
-        gh.hv_skip = hv ? 1 : 0;
+        gh.border = hv ? 1 : 0;
         launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, gh, tab, quads, lup_first, gvf, nosh, st);
         if (hv) {
             const size_t smem = hv_smem_bytes();

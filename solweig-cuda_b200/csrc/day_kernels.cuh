@@ -153,7 +153,8 @@ __global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
                                                                    const SolweigHour* __restrict__ hours,
                                                                    float4* __restrict__ quads,
                                                                    float* __restrict__ lup_first,
-                                                                   const float* __restrict__ ceiling) {
+                                                                   const float* __restrict__ ceiling,
+                                                                   const int* __restrict__ exits) {
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
@@ -162,13 +163,66 @@ __global__ void __launch_bounds__(256) day_shadow_kernel(SolweigScene S,
     if (r >= S.rows || c >= S.cols) return;
     const long long n = (long long)S.rows * S.cols;
     shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
-                      ceiling ? ceiling + z * n : nullptr);
+                      ceiling ? ceiling + z * n : nullptr,
+                      exits ? exits + (long long)z * (S.rows + S.cols) : nullptr);
+}
+
+// Per daytime hour, the first-outside step of every row and column of the
+// raster (first_outside), for the bounds-check-free sweep.
+__global__ void __launch_bounds__(1024) day_ray_exits_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
+                                                             int* __restrict__ exits) {
+    const SolweigHour& h = hours[blockIdx.x];
+    if (!h.daytime) return;
+    const int K = h.steps;
+    const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
+    int xi = 1, xd = 1, yi = 1, yd = 1;
+    for (int k = 1 + threadIdx.x; k < K; k += blockDim.x) {
+        const int2 o = __ldg(&ray[k]), q = __ldg(&ray[k - 1]);
+        xi &= o.x >= q.x;
+        xd &= o.x <= q.x;
+        yi &= o.y >= q.y;
+        yd &= o.y <= q.y;
+    }
+    const int axi = __syncthreads_and(xi), axd = __syncthreads_and(xd);
+    const int ayi = __syncthreads_and(yi), ayd = __syncthreads_and(yd);
+    const bool mx = axi || axd, my = ayi || ayd;
+    int* e = exits + (long long)blockIdx.x * (S.rows + S.cols);
+    for (int i = threadIdx.x; i < S.rows + S.cols; i += blockDim.x)
+        e[i] = i < S.rows ? first_outside(ray, K, true, i, S.rows, mx)
+                          : first_outside(ray, K, false, i - S.rows, S.cols, my);
 }
 
 struct DayGvfArgs {
     int first, second, halo;
-    int hv_skip;  // 1: blocks inside an interior tile of the hour-vectorized kernel return at once
+    // border: 1 = the grid is one-dimensional over the blocks outside the
+    // rectangle [bx0, bx1] x [by0, by1] of blocks that the hour-vectorized
+    // kernel covers (gx x gy blocks in all)
+    int border;
+    int gx, gy, bx0, bx1, by0, by1;
 };
+
+// Block (bx, by) of border block i: the rows above the interior rectangle,
+// the left and right flanks beside it, then the rows below it.
+__device__ __forceinline__ void border_block(const DayGvfArgs& g, int i, int& bx, int& by) {
+    const int top = g.by0 * g.gx;
+    if (i < top) {
+        by = i / g.gx;
+        bx = i - by * g.gx;
+        return;
+    }
+    i -= top;
+    const int left = g.bx0, per_row = g.bx0 + (g.gx - 1 - g.bx1);
+    const int mid = (g.by1 - g.by0 + 1) * per_row;
+    if (i < mid) {
+        const int k = i % per_row;
+        by = g.by0 + i / per_row;
+        bx = k < left ? k : g.bx1 + 1 + (k - left);
+        return;
+    }
+    i -= mid;
+    by = g.by1 + 1 + i / g.gx;
+    bx = i % g.gx;
+}
 
 // Tiles of the hour-vectorized GVF kernel: 32 x 32 pixels, halo 21 (the 1 m
 // walk, second = 22).  A tile is interior when its halo lies inside the raster.
@@ -191,18 +245,19 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
-    if (ga.hv_skip && hv_tile_interior(S.rows, S.cols, (int)(blockIdx.y * TY) / kHvTile, blockIdx.x)) return;
+    int bx = blockIdx.x, by = blockIdx.y;
+    if (ga.border) border_block(ga, blockIdx.x, bx, by);
     const long long n = (long long)S.rows * S.cols;
     const float4* quad = quads + z * n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int H = ga.halo, second = ga.second, first = ga.first;
     const int pitch = 32 + 2 * H;
     float4* tile = reinterpret_cast<float4*>(smem_raw);
-    const int row0 = blockIdx.y * TY - H, col0 = blockIdx.x * 32 - H;
+    const int row0 = by * TY - H, col0 = bx * 32 - H;
     load_quad_tile(tile, pitch, TY + 2 * H, quad, S.rows, S.cols, row0, col0);
     __syncthreads();
-    const int c = blockIdx.x * 32 + threadIdx.x;
-    const int r = blockIdx.y * TY + threadIdx.y;
+    const int c = bx * 32 + threadIdx.x;
+    const int r = by * TY + threadIdx.y;
     if (r >= S.rows || c >= S.cols) return;
     const long long p = (long long)r * S.cols + c;
     const float4* own_cell = tile + (threadIdx.y + H) * pitch + threadIdx.x + H;
@@ -1001,14 +1056,40 @@ void launch_day_gvf_ty(const SolweigScene& S, const SolweigHour* hours, int nhou
                        float* nosh, cudaStream_t st) {
     const size_t smem = sizeof(float4) * (size_t)(32 + 2 * ga.halo) * (TY + 2 * ga.halo);
     dim3 grid(blocks_for(S.cols, 32), blocks_for(S.rows, TY), nhours);
+    DayGvfArgs g = ga;
+    if (g.border) {
+        // interior 32 x 32 tiles form a rectangle; its blocks are left out
+        g.gx = (int)grid.x;
+        g.gy = (int)grid.y;
+        int tr0 = 1 << 30, tr1 = -1, tc0 = 1 << 30, tc1 = -1;
+        for (int tr = 0; tr * kHvTile < S.rows; ++tr)
+            for (int tc = 0; tc * kHvTile < S.cols; ++tc)
+                if (hv_tile_interior(S.rows, S.cols, tr, tc)) {
+                    tr0 = std::min(tr0, tr);
+                    tr1 = std::max(tr1, tr);
+                    tc0 = std::min(tc0, tc);
+                    tc1 = std::max(tc1, tc);
+                }
+        long long count = (long long)g.gx * g.gy;
+        if (tr1 >= 0) {
+            g.bx0 = tc0;
+            g.bx1 = tc1;
+            g.by0 = tr0 * kHvTile / TY;
+            g.by1 = (tr1 + 1) * kHvTile / TY - 1;
+            count -= (long long)(g.bx1 - g.bx0 + 1) * (g.by1 - g.by0 + 1);
+        } else {
+            g.border = 0;  // no interior tile: the plain two-dimensional grid
+        }
+        if (g.border) grid = dim3((unsigned)count, 1, nhours);
+    }
     if (S.has_water) {
         auto k = day_gvf_kernel<TY, FIRST, SECOND, TABLE, true>;
         set_smem_attr((const void*)k, smem);
-        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, ga, tab, quads, lup_first, gvf, nosh);
+        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, g, tab, quads, lup_first, gvf, nosh);
     } else {
         auto k = day_gvf_kernel<TY, FIRST, SECOND, TABLE, false>;
         set_smem_attr((const void*)k, smem);
-        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, ga, tab, quads, lup_first, gvf, nosh);
+        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, g, tab, quads, lup_first, gvf, nosh);
     }
 }
 

@@ -24,19 +24,29 @@ __device__ __forceinline__ double lup_excess(double emis, double tg, double shad
 // Shadow sweep of pixel (r, c) for hour h and the per-pixel GVF inputs: the
 // float4 quad (shadow, Lup, albedo, ground|sunwall bits) and, for scenes with
 // water, the Lup of the first GVF search direction.
+// `exits` (optional): the hour's first-outside step of every row and column
+// (first_outside); with the packed geometry the walk then needs no bounds checks.
 __device__ __forceinline__ void shadow_quad_pixel(const SolweigScene& S, const SolweigHour& h, int r, int c,
                                                   float4* __restrict__ quad, float* __restrict__ lup_first,
-                                                  const float* __restrict__ ceiling = nullptr) {
+                                                  const float* __restrict__ ceiling = nullptr,
+                                                  const int* __restrict__ exits = nullptr) {
     const long long p = (long long)r * S.cols + c;
     const double a = S.dsm[p];
     const double wall = S.walls[p];
     const uint8_t fl = S.flags[p];
     const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
-    const ShadowResult s =
-        S.geo32 ? shadow_walk_geo(GeoF32x4{reinterpret_cast<const float4*>(S.geo32)}, S.rows, S.cols, r, c, a,
-                                  S.vegdem[p], (fl & 2) != 0, wall, ray, h.ray_dz, h.steps, S.hmax, true, ceiling)
-                : shadow_walk_geo(GeoF64{S.dsm, S.vegdem, S.vegdem2}, S.rows, S.cols, r, c, a, S.vegdem[p],
-                                  (fl & 2) != 0, wall, ray, h.ray_dz, h.steps, S.hmax, true, ceiling);
+    ShadowResult s;
+    if (S.geo32 && exits) {
+        const int kend = min(h.steps, min(__ldg(&exits[r]), __ldg(&exits[S.rows + c])));
+        s = shadow_walk_packed(reinterpret_cast<const float4*>(S.geo32), S.cols, p, a, S.vegdem[p], (fl & 2) != 0,
+                               wall, ray, h.ray_dz, h.steps, kend, S.hmax, ceiling);
+    } else if (S.geo32) {
+        s = shadow_walk_geo(GeoF32x4{reinterpret_cast<const float4*>(S.geo32)}, S.rows, S.cols, r, c, a,
+                            S.vegdem[p], (fl & 2) != 0, wall, ray, h.ray_dz, h.steps, S.hmax, true, ceiling);
+    } else {
+        s = shadow_walk_geo(GeoF64{S.dsm, S.vegdem, S.vegdem2}, S.rows, S.cols, r, c, a, S.vegdem[p],
+                            (fl & 2) != 0, wall, ray, h.ray_dz, h.steps, S.hmax, true, ceiling);
+    }
     // Wall sunlit height (only needed for the sunlit-wall bit of the GVF).
     const double wallbol = wall > 0.0 ? 1.0 : 0.0;
     const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);

@@ -146,6 +146,104 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
     return s;
 }
 
+// The same walk over the packed float4 geometry, for a ray known to stay in
+// the raster for `kend` steps (the first step outside, or `steps`): no
+// per-step bounds checks, linear sample offsets, and only the DSM height is
+// widened to float64 at a sample without canopy (tq, bq <= 0 compare the
+// same in float32).  Results are identical to shadow_walk_geo.
+__device__ __forceinline__ ShadowResult shadow_walk_packed(
+    const float4* __restrict__ geo, int cols, long long p, double a, double top_p, bool bush, double wall,
+    const int2* __restrict__ ray, const double* __restrict__ dz, int steps, int kend, double hmax,
+    const float* __restrict__ ceiling) {
+    ShadowResult s;
+    s.f = a;
+    s.topmax = top_p;
+    s.shadowed = false;
+    s.veg = bush;
+    s.ever = false;
+    const bool is_wall = wall > 0.0;
+    const bool nonneg = a >= 0.0;
+    const double clear = nonneg ? nextafter(hmax - a, __longlong_as_double(0x7ff0000000000000ll))
+                                : __longlong_as_double(0x7ff0000000000000ll);
+    double dz_prev = 0.0;
+    bool final = false;
+    int k = 0;
+    for (; k < kend; ++k) {
+        const int2 o = __ldg(&ray[k]);
+        const double dzk = __ldg(&dz[k]);
+        const long long q = p + (long long)o.x * cols + o.y;
+        if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
+            final = true;
+            break;
+        }
+        if (ceiling != nullptr && k >= 4 && (k & 3) == 0) {
+            const double e = __dsub_ru((double)__ldg(&ceiling[q]), dz_prev);
+            if (nonneg && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) {
+                final = true;
+                break;
+            }
+        }
+        const float4 v = __ldg(&geo[q]);
+        s.f = fmax(s.f, (double)v.x - dzk);
+        s.shadowed = s.f > a;
+        if (v.y <= 0.f && v.z <= 0.f && nonneg && s.topmax >= 0.0) {
+            if (s.shadowed) s.veg = false;
+            else s.ever = s.ever || s.veg;
+        } else {
+            const double tq = v.y, bq = v.z;
+            s.topmax = fmax(s.topmax, tq - dzk);
+            if (s.shadowed) {
+                s.veg = false;
+            } else {
+                const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
+                              (int)(bq - dz_prev > a);
+                s.veg = s.veg || (n > 0 && n < 4);
+                s.ever = s.ever || s.veg;
+            }
+        }
+        if (s.shadowed && (!is_wall || s.f - a >= wall)) {
+            final = true;
+            break;
+        }
+        dz_prev = dzk;
+    }
+    if (!final && k < steps) {
+        // First step whose sample is outside the raster: all shifted values are 0.
+        s.f = fmax(s.f, 0.0);
+        s.shadowed = s.f > a;
+        s.topmax = fmax(s.topmax, 0.0);
+        if (s.shadowed) s.veg = false;
+        s.ever = s.ever || s.veg;
+    }
+    return s;
+}
+
+// Per hour, the first step at which the ray from row r (column c) leaves the
+// raster: exits[r] for the rows, exits[rows + c] for the columns (`steps`
+// when it never does).  The offsets of a sun ray are monotone along both
+// axes, so the steps inside form a prefix found by bisection; a table whose
+// offsets are not monotone is scanned linearly.
+__device__ __forceinline__ int first_outside(const int2* __restrict__ ray, int steps, bool row_axis, int pos,
+                                             int extent, bool monotone) {
+    auto inside = [&](int k) {
+        const int2 o = __ldg(&ray[k]);
+        const int v = pos + (row_axis ? o.x : o.y);
+        return v >= 0 && v < extent;
+    };
+    if (!monotone) {
+        for (int k = 0; k < steps; ++k)
+            if (!inside(k)) return k;
+        return steps;
+    }
+    int lo = 0, hi = steps;  // inside on [0, lo), answer in [lo, hi]
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (inside(mid)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ ShadowResult shadow_walk(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,

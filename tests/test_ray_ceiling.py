@@ -31,34 +31,41 @@ def _frame(dxdy, dz, rows, cols):
                 delta=float(delta))
 
 
+def _dilate_minor(Hm, w):
+    """max over +-w along axis 1 (neighbours outside the raster ignored)."""
+    out = Hm.copy()
+    for d in range(1, w + 1):
+        out[:, :-d] = np.maximum(out[:, :-d], Hm[:, d:])
+        out[:, d:] = np.maximum(out[:, d:], Hm[:, :-d])
+    return out
+
+
 def ceiling_planes(H, dxdy, dz):
-    """Ceiling plane of one hour (float64 restatement of the kernel)."""
+    """Ceiling plane of one hour, restating the kernels: H dilated by +-W
+    along the minor axis (the dilation kernel's planes), sampled along each
+    sheared line with the centre clamped to the raster when it lies within W
+    of it, and the discounted backward maximum."""
     rows, cols = H.shape
     f = _frame(dxdy, dz, rows, cols)
-    Ho = H if f["rows_major"] else H.T
-    if f["s_major"] < 0:
-        Ho = Ho[::-1]
-    if f["s_minor"] < 0:
-        Ho = Ho[:, ::-1]
-    nx, nb = Ho.shape
+    W = f["band"]
+    Hm = H if f["rows_major"] else H.T          # [major][minor] in raster order
+    plane = _dilate_minor(Hm, W)
+    nx, nb = Hm.shape
     R = np.arange(nx) * f["m"] // f["d"]
     roff = int(R[-1])
     lines = nb + roff
-    W = f["band"]
-    S = np.full((nx, lines + 2 * W), -np.inf)
-    for x in range(nx):
-        S[x, W + roff - R[x]:W + roff - R[x] + nb] = Ho[x]
-    Sd = np.max(np.stack([S[:, t:t + lines] for t in range(2 * W + 1)]), axis=0)
-    G = Sd.copy()
-    for x in range(nx - 2, -1, -1):
-        G[x] = np.maximum(Sd[x], G[x + 1] - f["delta"])
-    Co = np.empty_like(Ho)
-    for x in range(nx):
-        Co[x] = G[x, roff - R[x]:roff - R[x] + nb]
-    if f["s_minor"] < 0:
-        Co = Co[:, ::-1]
-    if f["s_major"] < 0:
-        Co = Co[::-1]
+    line = np.arange(lines) - roff               # sheared line N of each lane
+    G = np.full(lines, -np.inf)
+    Co = np.empty_like(Hm)
+    for x in range(nx - 1, -1, -1):
+        a = x if f["s_major"] > 0 else nx - 1 - x
+        y = line + R[x]
+        near = (y >= -W) & (y < nb + W)
+        yc = np.clip(y, 0, nb - 1)
+        b = yc if f["s_minor"] > 0 else nb - 1 - yc
+        G = np.maximum(np.where(near, plane[a, b], -np.inf), G - f["delta"])
+        inside = (y >= 0) & (y < nb)
+        Co[a, np.where(f["s_minor"] > 0, y, nb - 1 - y)[inside]] = G[inside]
     return (Co if f["rows_major"] else Co.T), f
 
 
