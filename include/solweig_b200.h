@@ -297,6 +297,19 @@ int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSkyLayout* la
                            const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
                            int first_steps, int second_steps, void* work, int64_t work_bytes,
                            const SolweigDayConfig* config, void* stream);
+/* One part of solweig_day_batched_ex (no counterpart in the reference: it
+ * lets the host plan later hours while earlier ones run).  part 0: the sweep
+ * stage (ray exits, ray ceilings, shadow sweep) of hours [hour_begin,
+ * hour_end); the part starting at hour 0 also builds the day's dilated height
+ * planes.  part 1: the rest of the day (GVF to radiation) over all hours,
+ * hour range ignored.  Part 0 over consecutive ranges covering [0, nhours) in
+ * order, then part 1, all on one stream, equals solweig_day_batched_ex. */
+int solweig_day_batched_part(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                             const SolweigHour* hours, int nhours, const SolweigState* state,
+                             const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                             int first_steps, int second_steps, void* work, int64_t work_bytes,
+                             const SolweigDayConfig* config, int part, int hour_begin, int hour_end,
+                             void* stream);
 /* solweig_day_batched_ex timed with CUDA events on `stream` between its
  * stages; synchronises on the last event and writes 5 host floats (ms):
  * shadow, GVF, weights + tables, patch contraction, radiation. */

@@ -117,7 +117,7 @@ EXPORTED_SYMBOLS = (
     "solweig_step_radiation", "solweig_day", "solweig_step_gvf", "solweig_utci_scalar",
     "solweig_svf_pack", "solweig_svf_reduce", "solweig_step_static_scratch",
     "solweig_day_batched", "solweig_day_batched_work_bytes", "solweig_day_batched_error",
-    "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex",
+    "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex", "solweig_day_batched_part",
     "solweig_day_batched_layout", "solweig_day_grad_work_bytes", "solweig_day_grad_forward",
     "solweig_day_grad_backward", "solweig_svf_ex",
 )
@@ -151,6 +151,7 @@ def _declare(lib):
         "solweig_day_batched_work_bytes": (i64, [i32, i32, i32, i32]),
         "solweig_day_batched_timed": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P, P]),
         "solweig_day_batched_ex": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P]),
+        "solweig_day_batched_part": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, i32, i32, i32, P]),
         "solweig_day_batched_layout": (i32, [i32, i32, i32, i32, P]),
         "solweig_day_grad_work_bytes": (i64, [i32, i32, i32]),
         "solweig_day_grad_forward": (i32, [P, P, P, i32, P, i32, i32, P, i32, P, P, i64, P]),

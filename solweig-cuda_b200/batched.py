@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .engine import HourBuffers, device_ptr, outputs_struct, plan_day, stream_handle
+from .engine import HourBuffers, device_ptr, outputs_struct, plan_day, plan_hours, stream_handle
 
 __all__ = ["BatchedDay", "ChosenDay", "MultiDay", "TileBatch"]
 
@@ -97,18 +97,26 @@ class BatchedDay:
         return {k: self.out[k] for k in names}
 
 
-def day_launches(scene, config):
-    """Kernel launches of one batched day for this scene and launch shapes."""
+def day_launches(scene, config, sweep_parts=1):
+    """Kernel launches of one batched day for this scene and launch shapes,
+    with the sweep stage issued in ``sweep_parts`` hour ranges: per range the
+    ray exits, the ceilings and the sweep; once the height dilation; then the
+    border GVF (+ the hour-vectorized interior kernel), weights, split,
+    tables, contraction and radiation."""
     hv = config.gvf_hours == 1 and not scene.struct.has_water and scene.first_steps == 1 \
         and scene.second_steps == 22
-    return 8 + int(hv) + 2 * int(not config.no_ceiling)
+    c = int(not config.no_ceiling)
+    return sweep_parts * (2 + c) + c + 6 + int(hv)
 
 
 class ChosenDay(BatchedDay):
-    """The batched form: every hour of a day in seven launches
-    (``solweig_day_batched``: per-launch shadow and GVF over all hours, the
-    BF16 tensor-core patch contraction, hour-looping radiation), replayed as
-    one CUDA graph together with the hour-record uploads.
+    """The batched form: every hour of a day in a few launches
+    (``solweig_day_batched``: ray ceilings and shadow sweep over ranges of
+    hours, GVF over all hours, the BF16 tensor-core patch contraction,
+    hour-looping radiation).  Each sweep range is a CUDA graph (with the
+    upload of its hour records) replayed as soon as its hours are planned, so
+    the host plans the next range while the GPU sweeps; the rest of the day is
+    one more graph.
 
     Produces the all-direction planes (Tmrt, UTCI, Kdown, Kup, Ldown, Lup,
     Kside, Lside, shadow, Tg ...); the cardinal E/S/W/N planes are only made
@@ -117,12 +125,18 @@ class ChosenDay(BatchedDay):
     CARDINAL = ("keast", "ksouth", "kwest", "knorth", "least", "lsouth", "lwest", "lnorth")
 
     def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0, hours=24,
-                 outputs=("tmrt", "utci"), use_graph=True):
+                 outputs=("tmrt", "utci"), use_graph=True, pipeline_hours=4):
         bad = [o for o in outputs if o in self.CARDINAL]
         if bad:
             raise ValueError(f"the batched form does not produce {bad}")
         super().__init__(scene, latitude, longitude, site_altitude, utc, hours, outputs, use_graph)
         self.scratch = None
+        # pipeline_hours > 0: the sweep stage runs in ranges of that many hours,
+        # each launched as soon as its hours are planned (the host plans the
+        # next range while the GPU sweeps this one); 0: plan the whole day first.
+        self.ranges = ([(h, min(h + pipeline_hours, hours)) for h in range(0, hours, pipeline_hours)]
+                       if pipeline_hours > 0 else None)
+        self.part_graphs = None
         L = _lib.lib()
         self.work_bytes = int(L.solweig_day_batched_work_bytes(scene.rows, scene.cols, hours,
                                                                int(scene.struct.has_water)))
@@ -133,17 +147,75 @@ class ChosenDay(BatchedDay):
 
     @property
     def launches_per_day(self):
-        """Kernels of one day: height dilation and ray ceilings, ray exits,
-        shadow, GVF (+ the hour-vectorized interior kernel), weights, split,
-        tables, contraction, radiation."""
-        return day_launches(self.scene, self.config)
+        """Kernels of one day (``day_launches``)."""
+        return day_launches(self.scene, self.config, len(self.ranges) if self.ranges else 1)
 
     def set_config(self, config):
-        """Launch shapes (``SolweigDayConfig`` or a tuple of its fields); drops a captured graph."""
+        """Launch shapes (``SolweigDayConfig`` or a tuple of its fields); drops captured graphs."""
         if not isinstance(config, _lib.SolweigDayConfig):
             config = _lib.SolweigDayConfig(*config)
         self.config = config
         self.graph = None
+        self.part_graphs = None
+
+    def _part(self, part, h0=0, h1=0):
+        """One part of the day on the current stream (``solweig_day_batched_part``):
+        part 0 uploads the records and rays of hours [h0, h1) and sweeps them,
+        part 1 runs the rest of the day."""
+        if part == 0:
+            self.buffers.upload(h0, h1 - h0, self.buffers.kmax)
+        sc = self.scene
+        base = outputs_struct(self.out, 0)
+        _lib.check(_lib.lib().solweig_day_batched_part(
+            ctypes.byref(sc.struct), device_ptr(self.layout_dev), self.buffers.ptr(), self.hours,
+            ctypes.byref(_lib.SolweigState()), ctypes.byref(base), sc.pixels, sc.gvf_host_ptr,
+            sc.first_steps, sc.second_steps, device_ptr(self.work), self.work_bytes,
+            ctypes.byref(self.config), part, h0, h1, stream_handle()), "solweig_day_batched_part")
+
+    def run_day(self, met, outputs=None):
+        """Plan the day on the host and run it; with pipelined ranges each sweep
+        range starts as soon as its hours are planned.  Returns {name: [H, rows,
+        cols]} views that stay valid until the next call."""
+        if self.ranges is None:
+            return super().run_day(met, outputs)
+        met = np.asarray(met, dtype=np.float64)
+        if len(met) != self.hours:
+            raise ValueError(f"expected {self.hours} forcing rows, got {len(met)}")
+        self.buffers.wait_free()
+        rows = plan_hours(self.scene, met, self.latitude, self.longitude, self.site_altitude, self.utc)
+        scalars = []
+        capture = self.use_graph and self.part_graphs is None
+        for c, (h0, h1) in enumerate(self.ranges):
+            for i in range(h0, h1):
+                h, ray, scal = next(rows)
+                self.buffers.put(i, h, ray)
+                scalars.append(scal)
+            if self.use_graph and not capture:
+                self.part_graphs[c].replay()
+            else:
+                self._part(0, h0, h1)
+        if self.use_graph and not capture:
+            self.part_graphs[-1].replay()
+        else:
+            self._part(1)
+        if capture:
+            # the eager pass above produced this day; capture the parts for the next ones
+            torch.cuda.synchronize()
+            graphs = []
+            for h0, h1 in self.ranges:
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._part(0, h0, h1)
+                graphs.append(g)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._part(1)
+            graphs.append(g)
+            self.part_graphs = graphs
+        self.last_scalars = scalars
+        self.buffers.mark()
+        names = self.out_names if outputs is None else outputs
+        return {k: self.out[k] for k in names}
 
     def _sequence(self):
         # Each day starts from the reset state (src/series.py:425-436): the

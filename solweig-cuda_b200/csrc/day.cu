@@ -74,10 +74,17 @@ namespace {
 
 constexpr int kDayStages = 5;  // shadow, GVF, weights + tables, contraction, radiation
 
+// Parts of a day: kDaySweep runs the sweep stage (ray exits, ceilings and the
+// shadow sweep) of hours [h0, h1) -- the part that starts at hour 0 also
+// builds the day's dilated height planes; kDayRest runs everything after it
+// (GVF to radiation) over all hours; kDayAll both.
+enum DayPart { kDaySweep = 0, kDayRest = 1, kDayAll = 2 };
+
 int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, const SolweigHour* hours,
                      int nhours, const SolweigState* state, const SolweigOutputs* base, int64_t hour_stride,
                      const int32_t* gvf_dxdy, int first_steps, int second_steps, void* work,
-                     int64_t work_bytes, void* stream, cudaEvent_t* ev, const SolweigDayConfig* cfg_in) {
+                     int64_t work_bytes, void* stream, cudaEvent_t* ev, const SolweigDayConfig* cfg_in,
+                     int part = kDayAll, int h0 = 0, int h1 = -1) {
     SolweigDayConfig cfg{32, 8, 8, 256, 0, 1, 0};
     if (cfg_in) cfg = *cfg_in;
     SOLWEIG_CHECK_ARG(cfg.shadow_bx > 0 && cfg.shadow_by > 0 && cfg.shadow_bx * cfg.shadow_by <= 256 &&
@@ -131,36 +138,56 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     SOLWEIG_CHECK_ARG(sizeof(float4) * (size_t)pitch * (8 + 2 * halo) <= 227 * 1024,
                       "solweig_day_batched: GVF halo %d too large", halo);
 
+    if (h1 < 0) h1 = nhours;
+    SOLWEIG_CHECK_ARG(part == kDaySweep || part == kDayRest || part == kDayAll,
+                      "solweig_day_batched: unknown part %d", part);
+    SOLWEIG_CHECK_ARG(0 <= h0 && h0 < h1 && h1 <= nhours, "solweig_day_batched: hours [%d, %d) outside [0, %d)", h0,
+                      h1, nhours);
+    if (part == kDayAll) {
+        if (ev) cudaEventRecord(ev[0], st);
+        int rc = day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
+                                  second_steps, work, work_bytes, stream, nullptr, &cfg, kDaySweep, 0, nhours);
+        if (rc) return rc;
+        if (ev) cudaEventRecord(ev[1], st);
+        return day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
+                                second_steps, work, work_bytes, stream, ev, &cfg, kDayRest, 0, nhours);
+    }
+    if (part == kDaySweep) {
+        const int nh = h1 - h0;
+        // The ceiling planes (4 B per pixel-hour) live in the GVF region (12 B
+        // per pixel-hour) and the four dilated height planes (16 B per pixel)
+        // in the patch-sum region (at least 16 B per pixel): both are consumed
+        // by the sweep before the GVF kernels and the contraction write those
+        // regions.
+        float* ceiling = cfg.no_ceiling ? nullptr : gvf;
+        float* dil = sums;
+        if (ceiling && h0 == 0) {
+            dim3 dgrid(blocks_for(S.cols, kDilTile), blocks_for(S.rows, kDilTile));
+            if (S.geo32) ceiling_dilate_kernel<true><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
+            else ceiling_dilate_kernel<false><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
+            SOLWEIG_CHECK_LAUNCH("ceiling_dilate_kernel");
+        }
+        if (ceiling) {
+            dim3 grid(blocks_for((long long)S.rows + S.cols, kCeilLanes), 1, nh);
+            day_ray_ceiling_kernel<<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours + h0, dil,
+                                                                                  ceiling + h0 * px);
+            SOLWEIG_CHECK_LAUNCH("day_ray_ceiling_kernel");
+        }
+        // first-outside steps of every row and column per hour (4 B each), in
+        // the GVF region after the ceiling planes (8 B per pixel-hour left)
+        int* exits = reinterpret_cast<int*>(wb + w.gvf + 4LL * px * nhours) + (long long)h0 * (S.rows + S.cols);
+        day_ray_exits_kernel<<<nh, 1024, 0, st>>>(S, hours + h0, exits);
+        SOLWEIG_CHECK_LAUNCH("day_ray_exits_kernel");
+        dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nh);
+        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(
+            S, hours + h0, quads + h0 * px, lup_first ? lup_first + h0 * px : nullptr,
+            ceiling ? ceiling + h0 * px : nullptr, exits);
+        SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
+        return SOLWEIG_OK;
+    }
+    // kDayRest
     cudaMemsetAsync(err, 0, sizeof(int), st);
     cudaMemsetAsync(nosh, 0, 4 * px, st);
-    if (ev) cudaEventRecord(ev[0], st);
-    // The ceiling planes (4 B per pixel-hour) live in the GVF region (12 B per
-    // pixel-hour) and the four dilated height planes (16 B per pixel) in the
-    // patch-sum region (at least 16 B per pixel): both are consumed by the
-    // sweep before the GVF kernels and the contraction write those regions.
-    float* ceiling = cfg.no_ceiling ? nullptr : gvf;
-    if (ceiling) {
-        float* dil = sums;
-        dim3 dgrid(blocks_for(S.cols, kDilTile), blocks_for(S.rows, kDilTile));
-        if (S.geo32) ceiling_dilate_kernel<true><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
-        else ceiling_dilate_kernel<false><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
-        SOLWEIG_CHECK_LAUNCH("ceiling_dilate_kernel");
-        dim3 grid(blocks_for((long long)S.rows + S.cols, kCeilLanes), 1, nhours);
-        day_ray_ceiling_kernel<<<grid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, hours, dil, ceiling);
-        SOLWEIG_CHECK_LAUNCH("day_ray_ceiling_kernel");
-    }
-    // first-outside steps of every row and column per hour (4 B each), in the
-    // GVF region after the ceiling planes (8 B per pixel-hour left there)
-    int* exits = reinterpret_cast<int*>(wb + w.gvf + 4LL * px * nhours);
-    day_ray_exits_kernel<<<nhours, 1024, 0, st>>>(S, hours, exits);
-    SOLWEIG_CHECK_LAUNCH("day_ray_exits_kernel");
-    {
-        dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nhours);
-        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(S, hours, quads, lup_first, ceiling,
-                                                                              exits);
-        SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
-    }
-    if (ev) cudaEventRecord(ev[1], st);
     if (first_steps == 1 && second_steps == 22) {
         GvfTable<22> tab;
         fill_day_table(tab, gvf_dxdy, 22, pitch);
@@ -240,6 +267,28 @@ extern "C" int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSk
                                       const SolweigDayConfig* config, void* stream) {
     return day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
                             second_steps, work, work_bytes, stream, nullptr, config);
+}
+
+// One part of solweig_day_batched_ex (no counterpart in the reference): with
+// part 0 the sweep stage of hours [hour_begin, hour_end), with part 1 the
+// rest of the day over all hours.  Calling part 0 over consecutive ranges
+// covering [0, nhours) in order and then part 1 on one stream gives the
+// results of solweig_day_batched_ex; the host can plan later hours while
+// the earlier ranges run.
+extern "C" int solweig_day_batched_part(const SolweigScene* scene, const SolweigSkyLayout* layout,
+                                        const SolweigHour* hours, int nhours, const SolweigState* state,
+                                        const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
+                                        int first_steps, int second_steps, void* work, int64_t work_bytes,
+                                        const SolweigDayConfig* config, int part, int hour_begin, int hour_end,
+                                        void* stream) {
+    SOLWEIG_CHECK_ARG(part == 0 || part == 1, "solweig_day_batched_part: part must be 0 or 1");
+    if (part == 1) {
+        hour_begin = 0;
+        hour_end = nhours;
+    }
+    return day_batched_impl(scene, layout, hours, nhours, state, base, hour_stride, gvf_dxdy, first_steps,
+                            second_steps, work, work_bytes, stream, nullptr, config,
+                            part == 0 ? kDaySweep : kDayRest, hour_begin, hour_end);
 }
 
 extern "C" int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout* layout,

@@ -746,15 +746,17 @@ class HourBuffers:
         return ctypes.c_void_p(self.h_dev.data_ptr())
 
 
-def plan_day(scene, met, latitude, longitude, site_altitude, utc):
-    """FP64 host plan of every row of one day: [(SolweigHour, ShadowRay|None, HourScalars)]."""
+def plan_hours(scene, met, latitude, longitude, site_altitude, utc):
+    """FP64 host plan of the rows of one day, yielded row by row as
+    (SolweigHour, ShadowRay|None, HourScalars): the sun positions of all rows
+    first, then each row's scalars (the clearness index and the wave-delay
+    clock carry from row to row)."""
     met = np.asarray(met, dtype=np.float64)
     sol = _sun.metdata(met, latitude, longitude, site_altitude, utc)
     dectime = sol.dectime
     timestepdec = (dectime[1] - dectime[0]) if len(met) > 1 else 1 / 24.
     twater = float(np.mean(met[:, 11])) if scene.landcover else None
     firstdaytime, timeadd, CI = 1, 0.0, 1.0
-    out = []
     for i in range(len(met)):
         if dectime[i] - np.floor(dectime[i]) == 0:
             CI = 1.
@@ -763,8 +765,12 @@ def plan_day(scene, met, latitude, longitude, site_altitude, utc):
             scene, latitude, sol.altitude[i], sol.azimuth[i], sol.zen[i], sol.jday[i], dectime[i],
             sol.altmax[i], met[i, 11], met[i, 10], met[i, 14], met[i, 21], met[i, 22], met[i, 12],
             met[i, 9], psi, CI, firstdaytime, timeadd, timestepdec, twater)
-        out.append((h, ray, scal))
-    return out
+        yield h, ray, scal
+
+
+def plan_day(scene, met, latitude, longitude, site_altitude, utc):
+    """FP64 host plan of every row of one day: [(SolweigHour, ShadowRay|None, HourScalars)]."""
+    return list(plan_hours(scene, met, latitude, longitude, site_altitude, utc))
 
 
 def outputs_struct(outputs, index=None):
