@@ -101,12 +101,10 @@ def day_launches(scene, config, sweep_parts=1):
     """Kernel launches of one batched day for this scene and launch shapes,
     with the sweep stage issued in ``sweep_parts`` hour ranges: per range the
     ray exits, the ceilings and the sweep; once the height dilation; then the
-    border GVF (+ the hour-vectorized interior kernel), weights, split,
+    GVF (the hour-vectorized kernel or the per-hour one), weights, split,
     tables, contraction and radiation."""
-    hv = config.gvf_hours == 1 and not scene.struct.has_water and scene.first_steps == 1 \
-        and scene.second_steps == 22
     c = int(not config.no_ceiling)
-    return sweep_parts * (2 + c) + c + 6 + int(hv)
+    return sweep_parts * (2 + c) + c + 6
 
 
 class ChosenDay(BatchedDay):
@@ -125,7 +123,7 @@ class ChosenDay(BatchedDay):
     CARDINAL = ("keast", "ksouth", "kwest", "knorth", "least", "lsouth", "lwest", "lnorth")
 
     def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0, hours=24,
-                 outputs=("tmrt", "utci"), use_graph=True, pipeline_hours=4):
+                 outputs=("tmrt", "utci"), use_graph=True, pipeline_hours=2):
         bad = [o for o in outputs if o in self.CARDINAL]
         if bad:
             raise ValueError(f"the batched form does not produce {bad}")

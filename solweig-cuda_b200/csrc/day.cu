@@ -192,10 +192,8 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
         GvfTable<22> tab;
         fill_day_table(tab, gvf_dxdy, 22, pitch);
         const bool hv = cfg.gvf_hours == 1 && !S.has_water;
-        DayGvfArgs gh = ga;
-        gh.border = hv ? 1 : 0;
-        launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, gh, tab, quads, lup_first, gvf, nosh, st);
-        if (hv) {
+        if (!hv) launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
+        else {
             const size_t smem = hv_smem_bytes();
             set_smem_attr((const void*)day_gvf_hv_kernel, smem);
             dim3 grid(blocks_for(S.cols, kHvTile), blocks_for(S.rows, kHvTile));

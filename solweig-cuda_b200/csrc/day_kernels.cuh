@@ -194,35 +194,7 @@ __global__ void __launch_bounds__(1024) day_ray_exits_kernel(SolweigScene S, con
 
 struct DayGvfArgs {
     int first, second, halo;
-    // border: 1 = the grid is one-dimensional over the blocks outside the
-    // rectangle [bx0, bx1] x [by0, by1] of blocks that the hour-vectorized
-    // kernel covers (gx x gy blocks in all)
-    int border;
-    int gx, gy, bx0, bx1, by0, by1;
 };
-
-// Block (bx, by) of border block i: the rows above the interior rectangle,
-// the left and right flanks beside it, then the rows below it.
-__device__ __forceinline__ void border_block(const DayGvfArgs& g, int i, int& bx, int& by) {
-    const int top = g.by0 * g.gx;
-    if (i < top) {
-        by = i / g.gx;
-        bx = i - by * g.gx;
-        return;
-    }
-    i -= top;
-    const int left = g.bx0, per_row = g.bx0 + (g.gx - 1 - g.bx1);
-    const int mid = (g.by1 - g.by0 + 1) * per_row;
-    if (i < mid) {
-        const int k = i % per_row;
-        by = g.by0 + i / per_row;
-        bx = k < left ? k : g.bx1 + 1 + (k - left);
-        return;
-    }
-    i -= mid;
-    by = g.by1 + 1 + i / g.gx;
-    bx = i % g.gx;
-}
 
 // Tiles of the hour-vectorized GVF kernel: 32 x 32 pixels, halo 21 (the 1 m
 // walk, second = 22).  A tile is interior when its halo lies inside the raster.
@@ -245,8 +217,7 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
-    int bx = blockIdx.x, by = blockIdx.y;
-    if (ga.border) border_block(ga, blockIdx.x, bx, by);
+    const int bx = blockIdx.x, by = blockIdx.y;
     const long long n = (long long)S.rows * S.cols;
     const float4* quad = quads + z * n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -332,6 +303,13 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
 // Same recurrences and the same float32 operation order as
 // gvf_direction_fixed except albedo*shadow, which is rounded once per sample
 // here instead of fused into the sum.
+//
+// Border tiles (halo reaching outside the raster) stage zeros outside and
+// follow the per-hour walk's edge rule: a walk whose first step leaves the
+// raster sees no ground (hit = 0); one that leaves at step L > 0 repeats its
+// last sample (step L - 1) for the remaining second - L steps and never hits.
+// Per direction the kernel keeps `lim` (samples read) and a frozen-tail bit
+// (then hit = second, else hit = lim): 6 bits, 5 directions per word.
 constexpr int kHvN = kHvPitch * kHvPitch;
 constexpr int kHvCh = 4;
 constexpr int kHvThreads = kHvTile * kHvTile;
@@ -344,7 +322,7 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                                                                   float* __restrict__ gvf, float* __restrict__ nosh) {
     constexpr int FIRST = 1, SECOND = 22;
     const int tr = blockIdx.y, tc = blockIdx.x;
-    if (!hv_tile_interior(S.rows, S.cols, tr, tc)) return;
+    const bool interior = hv_tile_interior(S.rows, S.cols, tr, tc);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* LA = reinterpret_cast<float4*>(smem_raw);  // Lup, albsh of pass hours 0, 1
     float4* LB = LA + kHvN;                            // pass hours 2, 3
@@ -368,40 +346,57 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
         const float4* q0 = quads + (long long)dayh[0] * n;
         for (int i = tid; i < kHvN; i += kHvThreads) {
             const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
-            const float4 q = q0[(long long)rr * S.cols + cc];
+            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
+            const float4 q = in ? q0[(long long)rr * S.cols + cc] : make_float4(0.f, 0.f, 0.f, 0.f);
             bits[i] = (uint32_t)__float_as_int(q.w) & kQuadGround;
             albs[i] = q.z;
         }
     }
     __syncthreads();
     const int r = tr * kHvTile + threadIdx.y, c = tc * kHvTile + threadIdx.x;
-    const long long p = (long long)r * S.cols + c;
+    const bool valid = r < S.rows && c < S.cols;  // partial tiles at the far edges
+    const long long p = valid ? (long long)r * S.cols + c : 0;
     const int own = (threadIdx.y + kHvHalo) * kHvPitch + threadIdx.x + kHvHalo;
-    const bool own_ground = (bits[own] & 1u) != 0;
+    const bool own_ground = valid && (bits[own] & 1u) != 0;
     const float ob = own_ground ? 1.f : 0.f;
-    const uint32_t face = S.gvf_face[p];
+    const uint32_t face = valid ? S.gvf_face[p] : 0u;
     constexpr float albedo_b = 0.2f;
     constexpr float inv_first = 1.f / FIRST, inv_first1 = 1.f / (FIRST + 1);
     constexpr float inv_second = 1.f / SECOND, inv_second1 = 1.f / (SECOND + 1);
-    // walk lengths (6 directions x 5 bits per word) and the static plane
-    uint32_t hits[3] = {0u, 0u, 0u};
+    // walk lengths (5 directions x 6 bits per word: lim, frozen-tail bit) and
+    // the static plane
+    uint32_t hits[4] = {0u, 0u, 0u, 0u};
     float nsh = 0.f;
     for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
-        int hit = 0;
+        int hit = 0, lim = 0;
         float s_alb = 0.f, n_alb = 0.f;
         if (own_ground) {
-            hit = SECOND;
+            hit = lim = SECOND;
             for (int m = 0; m < SECOND; ++m) {
+                if (!interior) {
+                    const int2 o = tab.offs[j * SECOND + m];
+                    if (!in_raster(r + o.x, c + o.y, S.rows, S.cols)) {
+                        if (m == 0) {
+                            hit = lim = 0;
+                        } else {  // frozen tail: step m and the rest repeat step m - 1
+                            lim = m;
+                            const float al = albs[own + tab.delta[j * SECOND + m - 1]];
+                            s_alb += al;
+                            s_alb += (SECOND - 1 - m) * al;
+                        }
+                        break;
+                    }
+                }
                 const int off = own + tab.delta[j * SECOND + m];
                 if (!(bits[off] & 1u)) {
-                    hit = m;
+                    hit = lim = m;
                     break;
                 }
                 s_alb += albs[off];
                 if (m + 1 == FIRST) n_alb = s_alb;
             }
         }
-        hits[j / 6] |= (uint32_t)hit << (5 * (j % 6));
+        hits[j / 5] |= ((uint32_t)lim | (hit > lim ? 32u : 0u)) << (6 * (j % 5));
         const int n_wall = SECOND - hit;
         const int n_wall_first = FIRST > hit ? FIRST - hit : 0;
         const float nosh1 = n_wall_first > 0 ? ((float)n_wall_first * albedo_b + n_alb) * inv_first1 : n_alb * inv_first;
@@ -410,19 +405,21 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
     }
     nsh *= ob;
     nsh += 18.f * (albs[own] * (1.f - ob));
-    nosh[p] = nsh / 18.f;
-    const double ambient_e = kSBC * (double)S.emis[p];
+    if (valid) nosh[p] = nsh / 18.f;
+    const double ambient_e = valid ? kSBC * (double)S.emis[p] : 0.0;
 
     for (int g0 = 0; g0 < nd; g0 += kHvCh) {
         const int nc = nd - g0 < kHvCh ? nd - g0 : kHvCh;
         __syncthreads();  // the previous pass no longer reads the tile
         for (int i = tid; i < kHvN; i += kHvThreads) {
-            const long long pix = (long long)(row0 + i / kHvPitch) * S.cols + (col0 + i % kHvPitch);
+            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
+            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
+            const long long pix = in ? (long long)rr * S.cols + cc : 0;
             float v[2 * kHvCh];
             uint32_t b = bits[i] & 1u;
 #pragma unroll
             for (int k = 0; k < kHvCh; ++k) {
-                if (k < nc) {
+                if (k < nc && in) {
                     const float4 q = quads[(long long)dayh[g0 + k] * n + pix];
                     v[2 * k] = q.y;
                     v[2 * k + 1] = q.z * q.x;
@@ -452,14 +449,16 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
         if (own_ground) {
 #pragma unroll 1
             for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
-                const int hit = (int)((hits[j / 6] >> (5 * (j % 6))) & 31u);
+                const uint32_t code = (hits[j / 5] >> (6 * (j % 5))) & 63u;
+                const int lim = (int)(code & 31u);
+                const int hit = (code & 32u) ? SECOND : lim;
                 float sl[kHvCh], sa[kHvCh], l0[kHvCh], a0[kHvCh];
 #pragma unroll
                 for (int k = 0; k < kHvCh; ++k) sl[k] = sa[k] = l0[k] = a0[k] = 0.f;
                 uint32_t seen = 0u, first_pk = 0xFFFFFu;  // 5 bits per hour, 31 = never
 #pragma unroll
                 for (int m = 0; m < SECOND; ++m) {
-                    if (m < hit) {
+                    if (m < lim) {
                         const int off = own + tab.delta[j * SECOND + m];
                         const float4 A = LA[off], B = LB[off];
                         const uint32_t b = (bits[off] >> 1) & 15u;
@@ -479,6 +478,21 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                                 a0[k] = sa[k];
                             }
                         }
+                    }
+                }
+                if (hit > lim) {
+                    // frozen tail (border tiles): step lim and the rest repeat step lim - 1,
+                    // whose sunlit-wall bits are already counted
+                    const int last = own + tab.delta[j * SECOND + lim - 1];
+                    const float4 A = LA[last], B = LB[last];
+                    const float rest = (float)(SECOND - 1 - lim);
+                    const float tl[kHvCh] = {A.x, A.z, B.x, B.z}, ta_[kHvCh] = {A.y, A.w, B.y, B.w};
+#pragma unroll
+                    for (int k = 0; k < kHvCh; ++k) {
+                        sl[k] += tl[k];
+                        sa[k] += ta_[k];
+                        sl[k] += rest * tl[k];
+                        sa[k] += rest * ta_[k];
                     }
                 }
                 const bool fj = (face >> j) & 1u;
@@ -509,7 +523,7 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
         const float own_albsh[4] = {oA.y, oA.w, oB.y, oB.w};
 #pragma unroll
         for (int k = 0; k < kHvCh; ++k) {
-            if (k < nc) {
+            if (k < nc && valid) {
                 const int h = dayh[g0 + k];
                 const SolweigHour& hh = hours[h];
                 const float lt = lup_t[k] + 18.f * (own_lup[k] * (1.f - ob));
@@ -1056,40 +1070,14 @@ void launch_day_gvf_ty(const SolweigScene& S, const SolweigHour* hours, int nhou
                        float* nosh, cudaStream_t st) {
     const size_t smem = sizeof(float4) * (size_t)(32 + 2 * ga.halo) * (TY + 2 * ga.halo);
     dim3 grid(blocks_for(S.cols, 32), blocks_for(S.rows, TY), nhours);
-    DayGvfArgs g = ga;
-    if (g.border) {
-        // interior 32 x 32 tiles form a rectangle; its blocks are left out
-        g.gx = (int)grid.x;
-        g.gy = (int)grid.y;
-        int tr0 = 1 << 30, tr1 = -1, tc0 = 1 << 30, tc1 = -1;
-        for (int tr = 0; tr * kHvTile < S.rows; ++tr)
-            for (int tc = 0; tc * kHvTile < S.cols; ++tc)
-                if (hv_tile_interior(S.rows, S.cols, tr, tc)) {
-                    tr0 = std::min(tr0, tr);
-                    tr1 = std::max(tr1, tr);
-                    tc0 = std::min(tc0, tc);
-                    tc1 = std::max(tc1, tc);
-                }
-        long long count = (long long)g.gx * g.gy;
-        if (tr1 >= 0) {
-            g.bx0 = tc0;
-            g.bx1 = tc1;
-            g.by0 = tr0 * kHvTile / TY;
-            g.by1 = (tr1 + 1) * kHvTile / TY - 1;
-            count -= (long long)(g.bx1 - g.bx0 + 1) * (g.by1 - g.by0 + 1);
-        } else {
-            g.border = 0;  // no interior tile: the plain two-dimensional grid
-        }
-        if (g.border) grid = dim3((unsigned)count, 1, nhours);
-    }
     if (S.has_water) {
         auto k = day_gvf_kernel<TY, FIRST, SECOND, TABLE, true>;
         set_smem_attr((const void*)k, smem);
-        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, g, tab, quads, lup_first, gvf, nosh);
+        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, ga, tab, quads, lup_first, gvf, nosh);
     } else {
         auto k = day_gvf_kernel<TY, FIRST, SECOND, TABLE, false>;
         set_smem_attr((const void*)k, smem);
-        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, g, tab, quads, lup_first, gvf, nosh);
+        k<<<grid, dim3(32, TY), smem, st>>>(S, hours, ga, tab, quads, lup_first, gvf, nosh);
     }
 }
 

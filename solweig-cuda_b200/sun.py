@@ -412,13 +412,19 @@ def metdata(met, latitude, longitude, site_altitude, utc):
     out = {k: np.empty(n) for k in ("year", "altitude", "azimuth", "zen", "jday", "leafon", "altmax")}
     day0s = [_dt.datetime(int(met[i, 0]), 1, 1) + _dt.timedelta(int(met[i, 1]) - 1) for i in range(n)]
     starts = [i for i in range(n) if i == 0 or np.mod(dectime[i], np.floor(dectime[i])) == 0]
-    K = 96  # 15-minute candidates after 10:00 (24 h)
+    K = 24  # 15-minute candidates after 10:00 evaluated up front (6 h); more on demand
+
+    def candidates(i, k0, k1):
+        out, fifteen = [], 0.
+        for k in range(k1):
+            fifteen = fifteen + 15. / 1440.
+            if k >= k0:
+                out.append(_datetime_fields(day0s[i] + _dt.timedelta(days=(60 * 10) / 1440.0 + fifteen)))
+        return out
+
     fields = []
     for i in starts:
-        fifteen = 0.
-        for _ in range(K):
-            fifteen = fifteen + 15. / 1440.
-            fields.append(_datetime_fields(day0s[i] + _dt.timedelta(days=(60 * 10) / 1440.0 + fifteen)))
+        fields += candidates(i, 0, K)
     for i in range(n):
         stamp = (day0s[i] + _dt.timedelta(hours=met[i, 2]) + _dt.timedelta(minutes=met[i, 3])
                  - _dt.timedelta(days=half))
@@ -428,17 +434,16 @@ def metdata(met, latitude, longitude, site_altitude, utc):
                                      longitude, site_altitude)
     altmax_of = {}
     for s_i, i in enumerate(starts):
-        zc = zen_all[s_i * K:(s_i + 1) * K]
+        zc = list(zen_all[s_i * K:(s_i + 1) * K])
         sunmaximum, zenith_max = -90., 90.
         k = 0
         while sunmaximum <= 90. - zenith_max:
             sunmaximum = 90. - zenith_max
-            if k < K:
-                zenith_max = float(zc[k])
-            else:  # beyond the precomputed candidates: continue one by one
-                stamp = day0s[i] + _dt.timedelta(days=(60 * 10) / 1440.0 + (k + 1) * 15. / 1440.)
-                zenith_max, _ = sun_position(*_datetime_fields(stamp), 0, utc, latitude, longitude,
-                                             site_altitude)
+            if k == len(zc):  # the next block of 15-minute candidates
+                g = np.asarray(candidates(i, len(zc), len(zc) + K), dtype=np.int64)
+                zc += list(sun_positions(g[:, 0], g[:, 1], g[:, 2], g[:, 3], g[:, 4], utc, latitude,
+                                         longitude, site_altitude)[0])
+            zenith_max = float(zc[k])
             k += 1
         altmax_of[i] = sunmaximum
     base = len(starts) * K

@@ -157,7 +157,9 @@ def test_tile_batch_and_autotuner(cuda, tmp_path, monkeypatch):
     outs = tb.run(mets)
     outs = [{k: v.clone() for k, v in o.items()} for o in outs]
     for s, met, lat, o in zip(scenes, mets, lats, outs):
-        ref = batched.ChosenDay(s, lat, 0.0, 3.0, 0.0).run_day(met)
+        alone = batched.ChosenDay(s, lat, 0.0, 3.0, 0.0)
+        alone.set_config(cfg)
+        ref = alone.run_day(met)
         torch.cuda.synchronize()
         assert torch.equal(o["tmrt"], ref["tmrt"])
 
