@@ -207,6 +207,19 @@ int solweig_svf_ex(const double* dsm, const double* vegdem, const double* vegdem
                    const double* band_weights, const uint8_t* sectors, double transmissivity,
                    uint32_t* masks, double* planes, float* veg_sums, uint8_t* sky_band_counts,
                    void* stream);
+/* solweig_svf_ex with a 256-byte aligned device work buffer of
+ * solweig_svf_work_bytes(rows, cols) bytes (no counterpart in the reference):
+ * per word of 32 patches, upper bounds of the heights ahead along each patch
+ * ray let the visibility walks stop early, and per-row / per-column exit steps
+ * drop their bounds checks; the masks and planes are identical. */
+int64_t solweig_svf_work_bytes(int rows, int cols);
+int solweig_svf_ex2(const double* dsm, const double* vegdem, const double* vegdem2,
+                    const void* geo32, const uint8_t* flags, int rows, int cols, int patches,
+                    int capacity, const int32_t* ray_dxdy, const double* ray_dz,
+                    const int32_t* lengths, double hmax, const SolweigSkyLayout* layout,
+                    const double* band_weights, const uint8_t* sectors, double transmissivity,
+                    uint32_t* masks, double* planes, float* veg_sums, uint8_t* sky_band_counts,
+                    void* work, int64_t work_bytes, void* stream);
 /* Annulus sums of packed masks (the reduce half of solweig_svf). */
 int solweig_svf_reduce(const uint32_t* masks, const double* vegdem2, int64_t pixels,
                        const SolweigSkyLayout* layout, const double* band_weights,

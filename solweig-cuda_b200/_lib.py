@@ -119,7 +119,7 @@ EXPORTED_SYMBOLS = (
     "solweig_day_batched", "solweig_day_batched_work_bytes", "solweig_day_batched_error",
     "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex", "solweig_day_batched_part",
     "solweig_day_batched_layout", "solweig_day_grad_work_bytes", "solweig_day_grad_forward",
-    "solweig_day_grad_backward", "solweig_svf_ex",
+    "solweig_day_grad_backward", "solweig_svf_ex", "solweig_svf_ex2", "solweig_svf_work_bytes",
 )
 
 _lock = threading.Lock()
@@ -142,6 +142,9 @@ def _declare(lib):
                               P]),
         "solweig_svf_ex": (i32, [P, P, P, P, P, i32, i32, i32, i32, P, P, P, dbl, P, P, P, dbl, P, P, P,
                                  P, P]),
+        "solweig_svf_ex2": (i32, [P, P, P, P, P, i32, i32, i32, i32, P, P, P, dbl, P, P, P, dbl, P, P, P,
+                                  P, P, i64, P]),
+        "solweig_svf_work_bytes": (i64, [i32, i32]),
         "solweig_svf_unpack": (i32, [P, i64, i32, P, P, P, P]),
         "solweig_diffsh": (i32, [P, P, P, i64, fl, P]),
         "solweig_gvf": (i32, [P, P, P, P, dbl, dbl, dbl, dbl, dbl, P, i32, i32, P, P, P]),

@@ -273,19 +273,16 @@ __global__ void __launch_bounds__(256) ceiling_dilate_kernel(SolweigScene S, flo
     }
 }
 
-// grid (ceil((rows + cols) / 32), 1, hours), block (32, 32): the ceiling plane
-// of every daytime hour whose ray has at least kCeilMinSteps steps, from the
-// dilated planes of ceiling_dilate_kernel.
-static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
-    SolweigScene S, const SolweigHour* __restrict__ hours, const float* __restrict__ dil,
-    float* __restrict__ ceiling) {
-    __shared__ float s_seg[kCeilWarps][kCeilLanes];
-    const SolweigHour& h = hours[blockIdx.z];
-    if (!h.daytime || h.steps < kCeilMinSteps) return;
+// The ceiling plane of one ray table (K steps) for the raster of S, by one
+// block of (32, 32) threads owning 32 sheared lines (blockIdx.x); the whole
+// block returns together.  Tables the frame does not fit give a +inf plane.
+__device__ __forceinline__ void ray_ceiling_block(const SolweigScene& S, const int2* __restrict__ ray,
+                                                  const double* __restrict__ dz, int K,
+                                                  const float* __restrict__ dil, float* __restrict__ out,
+                                                  float (*s_seg)[kCeilLanes]) {
+    if (K < kCeilMinSteps) return;
     const long long n = (long long)S.rows * S.cols;
-    float* out = ceiling + (long long)blockIdx.z * n;
-    const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
-    const CeilingFrame f = ceiling_frame(S, ray, h.ray_dz, h.steps);
+    const CeilingFrame f = ceiling_frame(S, ray, dz, K);
     const int tid = threadIdx.y * kCeilLanes + threadIdx.x;
     if (!f.ok || f.band > 2) {
         for (long long p = (long long)blockIdx.x * blockDim.x * blockDim.y + tid; p < n;
@@ -299,6 +296,33 @@ static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceilin
     const int line0 = line_first - (f.lines - f.nb);
     const float* plane = dil + (long long)((f.rows_major ? 0 : 2) + (f.band - 1)) * n;
     ceiling_scan(plane, f, S.cols, line0, s_seg, out);
+}
+
+// grid (ceil((rows + cols) / 32), 1, hours), block (32, 32): the ceiling plane
+// of every daytime hour whose ray has at least kCeilMinSteps steps, from the
+// dilated planes of ceiling_dilate_kernel.
+static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
+    SolweigScene S, const SolweigHour* __restrict__ hours, const float* __restrict__ dil,
+    float* __restrict__ ceiling) {
+    __shared__ float s_seg[kCeilWarps][kCeilLanes];
+    const SolweigHour& h = hours[blockIdx.z];
+    if (!h.daytime) return;
+    ray_ceiling_block(S, reinterpret_cast<const int2*>(h.ray_dxdy), h.ray_dz, h.steps, dil,
+                      ceiling + (long long)blockIdx.z * S.rows * S.cols, s_seg);
+}
+
+// The same for sky-patch rays: grid.z = patch - patch0 of a group of count
+// patches; tables [patch][capacity] with lengths[patch] steps.
+static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) patch_ray_ceiling_kernel(
+    SolweigScene S, const int2* __restrict__ rays, const double* __restrict__ dz,
+    const int32_t* __restrict__ lengths, int capacity, int patch0, int count, const float* __restrict__ dil,
+    float* __restrict__ ceiling) {
+    __shared__ float s_seg[kCeilWarps][kCeilLanes];
+    const int j = blockIdx.z, patch = patch0 + j;
+    if (j >= count) return;
+    const long long base = (long long)patch * capacity;
+    ray_ceiling_block(S, rays + base, dz + base, lengths[patch], dil,
+                      ceiling + (long long)j * S.rows * S.cols, s_seg);
 }
 
 }  // namespace solweig

@@ -173,23 +173,8 @@ __global__ void __launch_bounds__(1024) day_ray_exits_kernel(SolweigScene S, con
                                                              int* __restrict__ exits) {
     const SolweigHour& h = hours[blockIdx.x];
     if (!h.daytime) return;
-    const int K = h.steps;
-    const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
-    int xi = 1, xd = 1, yi = 1, yd = 1;
-    for (int k = 1 + threadIdx.x; k < K; k += blockDim.x) {
-        const int2 o = __ldg(&ray[k]), q = __ldg(&ray[k - 1]);
-        xi &= o.x >= q.x;
-        xd &= o.x <= q.x;
-        yi &= o.y >= q.y;
-        yd &= o.y <= q.y;
-    }
-    const int axi = __syncthreads_and(xi), axd = __syncthreads_and(xd);
-    const int ayi = __syncthreads_and(yi), ayd = __syncthreads_and(yd);
-    const bool mx = axi || axd, my = ayi || ayd;
-    int* e = exits + (long long)blockIdx.x * (S.rows + S.cols);
-    for (int i = threadIdx.x; i < S.rows + S.cols; i += blockDim.x)
-        e[i] = i < S.rows ? first_outside(ray, K, true, i, S.rows, mx)
-                          : first_outside(ray, K, false, i - S.rows, S.cols, my);
+    ray_exits_block(reinterpret_cast<const int2*>(h.ray_dxdy), h.steps, S.rows, S.cols,
+                    exits + (long long)blockIdx.x * (S.rows + S.cols));
 }
 
 struct DayGvfArgs {

@@ -244,6 +244,27 @@ __device__ __forceinline__ int first_outside(const int2* __restrict__ ray, int s
     return lo;
 }
 
+// first_outside of every row (exits[r]) and column (exits[rows + c]) of a
+// rows x cols raster for one ray table, by one block: the offsets are checked
+// for monotony along each axis first (bisection needs it).
+__device__ __forceinline__ void ray_exits_block(const int2* __restrict__ ray, int K, int rows, int cols,
+                                                int* __restrict__ exits) {
+    int xi = 1, xd = 1, yi = 1, yd = 1;
+    for (int k = 1 + threadIdx.x; k < K; k += blockDim.x) {
+        const int2 o = __ldg(&ray[k]), q = __ldg(&ray[k - 1]);
+        xi &= o.x >= q.x;
+        xd &= o.x <= q.x;
+        yi &= o.y >= q.y;
+        yd &= o.y <= q.y;
+    }
+    const int axi = __syncthreads_and(xi), axd = __syncthreads_and(xd);
+    const int ayi = __syncthreads_and(yi), ayd = __syncthreads_and(yd);
+    const bool mx = axi || axd, my = ayi || ayd;
+    for (int i = threadIdx.x; i < rows + cols; i += blockDim.x)
+        exits[i] = i < rows ? first_outside(ray, K, true, i, rows, mx)
+                            : first_outside(ray, K, false, i - rows, cols, my);
+}
+
 __device__ __forceinline__ ShadowResult shadow_walk(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,

@@ -10,6 +10,7 @@
 // Reduce (geometry.cu:121-159): annulus-weighted sums over bands and the four
 // half-sky sectors become per-band popcounts of the packed words, summed in
 // the reference's band order so the float64 planes agree to the last bit.
+#include "ceiling.cuh"
 #include "shadow.cuh"
 
 namespace solweig {
@@ -22,18 +23,25 @@ struct SvfRayParams {
     double hmax;
 };
 
-// grid.x: chunks of 32 consecutive pixels; grid.y: patch word (32 patches).
-// geo32: the packed float4 geometry (exact float32 values) or null.
-__global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
+// grid.x: chunks of 32 consecutive pixels; grid.y: patch word (32 patches)
+// from word0 on.  geo32: the packed float4 geometry (exact float32 values) or
+// null.  With `ceiling` and `exits` (one launch per word, grid.y = 1): the
+// word's ray-ceiling planes [32][pixels] and first-outside steps [32][rows +
+// cols]; the walk then stops on the ceilings and, with geo32, needs no
+// bounds checks.
+// WALK: 0 float64 rasters, 1 packed geometry, 2 packed geometry without
+// bounds checks (`exits` given).
+template <int WALK>
+__global__ void __launch_bounds__(32 * kSvfWarps, 6) svf_visibility_kernel(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
     const int2* __restrict__ ray, const double* __restrict__ dz, const int32_t* __restrict__ lengths,
-    uint32_t* __restrict__ masks) {
+    uint32_t* __restrict__ masks, int word0, const float* __restrict__ ceiling, const int* __restrict__ exits) {
     __shared__ uint8_t state[kSvfPatchGroup][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long pixels = (long long)prm.rows * prm.cols;
     const long long p = (long long)blockIdx.x * 32 + lane;
-    const int word = blockIdx.y;
+    const int word = word0 + blockIdx.y;
     const bool valid = p < pixels;
     const int r = valid ? (int)(p / prm.cols) : 0, c = valid ? (int)(p % prm.cols) : 0;
     const double a = valid ? dsm[p] : 0.0;
@@ -44,11 +52,21 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
         uint8_t st = 0;
         if (valid && patch < prm.patches) {
             const long long base = (long long)patch * prm.capacity;
-            const ShadowResult s =
-                geo32 ? shadow_walk_geo(GeoF32x4{geo32}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
-                                        dz + base, lengths[patch], prm.hmax, true)
-                      : shadow_walk(dsm, top, bot, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
-                                    dz + base, lengths[patch], prm.hmax, true);
+            const int K = lengths[patch];
+            const float* ceil_j = ceiling ? ceiling + (long long)j * pixels : nullptr;
+            ShadowResult s;
+            if (WALK == 2) {
+                const int* e = exits + (long long)j * (prm.rows + prm.cols);
+                const int kend = min(K, min(__ldg(&e[r]), __ldg(&e[prm.rows + c])));
+                s = shadow_walk_packed(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base, K, kend,
+                                       prm.hmax, ceil_j);
+            } else if (WALK == 1) {
+                s = shadow_walk_geo(GeoF32x4{geo32}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
+                                    dz + base, K, prm.hmax, true, ceil_j);
+            } else {
+                s = shadow_walk_geo(GeoF64{dsm, top, bot}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0,
+                                    ray + base, dz + base, K, prm.hmax, true, ceil_j);
+            }
             st = (s.shadowed ? 0 : 1) | (s.ever ? 2 : 0);
         }
         state[j][lane] = st;
@@ -247,6 +265,45 @@ extern "C" int solweig_svf_pack(const float* shmat, const float* vegmat, const f
     return SOLWEIG_OK;
 }
 
+// first_outside tables of a group of patches: block j = patch0 + j.
+__global__ void __launch_bounds__(1024) patch_ray_exits_kernel(int rows, int cols, const int2* __restrict__ rays,
+                                                               const int32_t* __restrict__ lengths, int capacity,
+                                                               int patch0, int count, int* __restrict__ exits) {
+    const int j = blockIdx.x;
+    if (j >= count) return;
+    const int patch = patch0 + j;
+    ray_exits_block(rays + (long long)patch * capacity, lengths[patch], rows, cols,
+                    exits + (long long)j * (rows + cols));
+}
+
+// Work of solweig_svf_ex2: 4 dilated height planes, the 32 ray-ceiling
+// planes of one patch word and its 32 first-outside tables.
+struct SvfWork {
+    long long dil, ceil, exits, total;
+};
+
+SvfWork svf_work_layout(int rows, int cols) {
+    const long long px = (long long)rows * cols;
+    SvfWork w{};
+    w.dil = 0;
+    w.ceil = (4LL * 4 * px + 255) & ~255LL;
+    w.exits = (w.ceil + 4LL * kSvfPatchGroup * px + 255) & ~255LL;
+    w.total = w.exits + 4LL * kSvfPatchGroup * (rows + cols);
+    return w;
+}
+
+extern "C" int64_t solweig_svf_work_bytes(int rows, int cols) {
+    if (rows <= 0 || cols <= 0) return 0;
+    return svf_work_layout(rows, cols).total;
+}
+
+int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, const void* geo32,
+             const uint8_t* flags, int rows, int cols, int patches, int capacity, const int32_t* ray_dxdy,
+             const double* ray_dz, const int32_t* lengths, double hmax, const SolweigSkyLayout* layout,
+             const double* band_weights, const uint8_t* sectors, double transmissivity, uint32_t* masks,
+             double* planes, float* veg_sums, uint8_t* sky_band_counts, void* work, int64_t work_bytes,
+             void* stream);
+
 extern "C" int solweig_svf_ex(const double* dsm, const double* vegdem, const double* vegdem2,
                               const void* geo32, const uint8_t* flags, int rows, int cols, int patches,
                               int capacity, const int32_t* ray_dxdy, const double* ray_dz,
@@ -254,6 +311,33 @@ extern "C" int solweig_svf_ex(const double* dsm, const double* vegdem, const dou
                               const double* band_weights, const uint8_t* sectors, double transmissivity,
                               uint32_t* masks, double* planes, float* veg_sums, uint8_t* sky_band_counts,
                               void* stream) {
+    return svf_impl(dsm, vegdem, vegdem2, geo32, flags, rows, cols, patches, capacity, ray_dxdy, ray_dz, lengths,
+                    hmax, layout, band_weights, sectors, transmissivity, masks, planes, veg_sums, sky_band_counts,
+                    nullptr, 0, stream);
+}
+
+// solweig_svf_ex with a work buffer of solweig_svf_work_bytes (no counterpart
+// in the reference): per patch word, ray ceilings and first-outside tables
+// let the visibility walks stop early with identical masks.
+extern "C" int solweig_svf_ex2(const double* dsm, const double* vegdem, const double* vegdem2,
+                               const void* geo32, const uint8_t* flags, int rows, int cols, int patches,
+                               int capacity, const int32_t* ray_dxdy, const double* ray_dz,
+                               const int32_t* lengths, double hmax, const SolweigSkyLayout* layout,
+                               const double* band_weights, const uint8_t* sectors, double transmissivity,
+                               uint32_t* masks, double* planes, float* veg_sums, uint8_t* sky_band_counts,
+                               void* work, int64_t work_bytes, void* stream) {
+    SOLWEIG_CHECK_ARG(work, "solweig_svf_ex2: null work buffer");
+    return svf_impl(dsm, vegdem, vegdem2, geo32, flags, rows, cols, patches, capacity, ray_dxdy, ray_dz, lengths,
+                    hmax, layout, band_weights, sectors, transmissivity, masks, planes, veg_sums, sky_band_counts,
+                    work, work_bytes, stream);
+}
+
+int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, const void* geo32,
+             const uint8_t* flags, int rows, int cols, int patches, int capacity, const int32_t* ray_dxdy,
+             const double* ray_dz, const int32_t* lengths, double hmax, const SolweigSkyLayout* layout,
+             const double* band_weights, const uint8_t* sectors, double transmissivity, uint32_t* masks,
+             double* planes, float* veg_sums, uint8_t* sky_band_counts, void* work, int64_t work_bytes,
+             void* stream) {
     SOLWEIG_CHECK_ARG(dsm && vegdem && vegdem2 && flags && ray_dxdy && ray_dz && lengths && layout &&
                           band_weights && sectors && masks && planes && veg_sums && sky_band_counts,
                       "solweig_svf: null pointer");
@@ -272,11 +356,53 @@ extern "C" int solweig_svf_ex(const double* dsm, const double* vegdem, const dou
     }
     SvfRayParams rp{rows, cols, patches, capacity, hmax};
     const int words = (patches + 31) / 32;
-    dim3 grid(blocks_for(pixels, 32), words);
-    svf_visibility_kernel<<<grid, 32 * kSvfWarps, 0, st>>>(
-        dsm, vegdem, vegdem2, reinterpret_cast<const float4*>(geo32), flags, rp,
-        reinterpret_cast<const int2*>(ray_dxdy), ray_dz, lengths, masks);
-    SOLWEIG_CHECK_LAUNCH("svf_visibility_kernel");
+    const int2* rays = reinterpret_cast<const int2*>(ray_dxdy);
+    const float4* g4 = reinterpret_cast<const float4*>(geo32);
+    if (!work) {
+        dim3 grid(blocks_for(pixels, 32), words);
+        if (g4) svf_visibility_kernel<1><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp, rays,
+                                                                          ray_dz, lengths, masks, 0, nullptr, nullptr);
+        else svf_visibility_kernel<0><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp, rays,
+                                                                       ray_dz, lengths, masks, 0, nullptr, nullptr);
+        SOLWEIG_CHECK_LAUNCH("svf_visibility_kernel");
+    } else {
+        const SvfWork w = svf_work_layout(rows, cols);
+        SOLWEIG_CHECK_ARG(work_bytes >= w.total, "solweig_svf_ex2: work buffer of %lld bytes, need %lld",
+                          (long long)work_bytes, w.total);
+        SOLWEIG_CHECK_ARG(((uintptr_t)work & 255) == 0, "solweig_svf_ex2: work buffer not 256-byte aligned");
+        char* wb = static_cast<char*>(work);
+        float* dil = reinterpret_cast<float*>(wb + w.dil);
+        float* ceil = reinterpret_cast<float*>(wb + w.ceil);
+        int* exits = reinterpret_cast<int*>(wb + w.exits);
+        SolweigScene S{};
+        S.rows = rows;
+        S.cols = cols;
+        S.dsm = dsm;
+        S.vegdem = vegdem;
+        S.vegdem2 = vegdem2;
+        S.geo32 = geo32;
+        dim3 dgrid(blocks_for(cols, kDilTile), blocks_for(rows, kDilTile));
+        if (geo32) ceiling_dilate_kernel<true><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
+        else ceiling_dilate_kernel<false><<<dgrid, dim3(32, 8), 0, st>>>(S, dil);
+        SOLWEIG_CHECK_LAUNCH("ceiling_dilate_kernel");
+        for (int wd = 0; wd < words; ++wd) {
+            const int p0 = wd * kSvfPatchGroup, cnt = std::min(kSvfPatchGroup, patches - p0);
+            dim3 cgrid(blocks_for((long long)rows + cols, kCeilLanes), 1, cnt);
+            patch_ray_ceiling_kernel<<<cgrid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, rays, ray_dz, lengths,
+                                                                                     capacity, p0, cnt, dil, ceil);
+            SOLWEIG_CHECK_LAUNCH("patch_ray_ceiling_kernel");
+            patch_ray_exits_kernel<<<cnt, 1024, 0, st>>>(rows, cols, rays, lengths, capacity, p0, cnt, exits);
+            SOLWEIG_CHECK_LAUNCH("patch_ray_exits_kernel");
+            dim3 grid(blocks_for(pixels, 32), 1);
+            if (g4) svf_visibility_kernel<2><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
+                                                                              rays, ray_dz, lengths, masks, wd, ceil,
+                                                                              exits);
+            else svf_visibility_kernel<0><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
+                                                                           rays, ray_dz, lengths, masks, wd, ceil,
+                                                                           nullptr);
+            SOLWEIG_CHECK_LAUNCH("svf_visibility_kernel");
+        }
+    }
     return solweig_svf_reduce(masks, vegdem2, pixels, layout, band_weights, sectors, transmissivity,
                               planes, veg_sums, sky_band_counts, stream);
 }

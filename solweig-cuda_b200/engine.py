@@ -370,15 +370,17 @@ class Scene:
         self.sky_band_counts = torch.empty((nb, self.rows, self.cols), dtype=torch.uint8, device=dev)
         lay = self.layout
         self.geo32 = self._packed_geometry()
-        _lib.check(L.solweig_svf_ex(
+        # ray ceilings and exit tables of one patch word (solweig_svf_ex2)
+        svf_work = torch.empty(int(L.solweig_svf_work_bytes(self.rows, self.cols)), dtype=torch.uint8, device=dev)
+        _lib.check(L.solweig_svf_ex2(
             device_ptr(self.dsm), device_ptr(self.vegdem), device_ptr(self.vegdem2), device_ptr(self.geo32),
             device_ptr(self.flags), self.rows, self.cols, lay.struct.patches, cap,
             device_ptr(t_dxdy), device_ptr(t_dz), device_ptr(t_len), self.hmax,
             ctypes.byref(lay.struct), lay.band_weights.ctypes.data_as(ctypes.c_void_p),
             lay.sectors.ctypes.data_as(ctypes.c_void_p), CONSTANTS["transVeg"],
             device_ptr(self.masks), device_ptr(planes), device_ptr(self.veg_sums),
-            device_ptr(self.sky_band_counts), st), "solweig_svf")
-        del t_dxdy, t_dz, t_len
+            device_ptr(self.sky_band_counts), device_ptr(svf_work), svf_work.numel(), st), "solweig_svf")
+        del t_dxdy, t_dz, t_len, svf_work
         # Derived statics after the float32 round trip of the SVF planes.
         self.svf32 = torch.empty((15, self.rows, self.cols), **f32)
         self.svfbuveg = torch.empty(self.shape, **f32)

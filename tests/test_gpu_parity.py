@@ -168,3 +168,49 @@ def test_step_gvf_planes_match_oracle(cuda, tile_rows):
     for k, j in enumerate(order):
         err = np.max(np.abs(got[k] - planes[j]) / (np.abs(planes[j]) + 1.0))
         assert err < 2e-5, (k, err)
+
+
+@pytest.mark.parametrize("packed", [True, False])
+def test_svf_ray_ceilings_are_bit_identical(cuda, packed):
+    """solweig_svf_ex2 (ray ceilings + exit tables, one launch per patch word)
+    against solweig_svf_ex (every ray walked to its clearance): identical
+    masks, planes and band counts on a 150 x 134 city, packed and float64
+    geometry."""
+    import ctypes
+    import torch
+    from solweig_cuda_b200 import _lib, engine, rays, synthetic
+    from solweig_cuda_b200.engine import device_ptr, stream_handle
+    s = synthetic.make_scene(150, 134, seed=11)
+    scene = engine.Scene(s.dsm, s.trees, s.dem, 1.0, landcover=s.landcover)
+    L = _lib.lib()
+    dxdy, dz, lengths, cap = rays.svf_rays(2, scene.shape, scene.amaxvalue, scene.scale)
+    t_dxdy = torch.from_numpy(np.ascontiguousarray(dxdy, dtype=np.int32)).to(cuda)
+    t_dz = torch.from_numpy(np.ascontiguousarray(dz, dtype=np.float64)).to(cuda)
+    t_len = torch.from_numpy(np.ascontiguousarray(lengths, dtype=np.int32)).to(cuda)
+    lay = scene.layout
+    nb = lay.struct.nbands
+    geo = scene.geo32 if packed else None
+    if packed:
+        assert geo is not None
+    out = {}
+    for ex2 in (False, True):
+        masks = torch.zeros((2 * _lib.MASK_WORDS, scene.rows, scene.cols), dtype=torch.int32, device=cuda)
+        planes = torch.zeros((16, scene.rows, scene.cols), dtype=torch.float64, device=cuda)
+        veg = torch.zeros((4, scene.rows, scene.cols), dtype=torch.float32, device=cuda)
+        cnt = torch.zeros((nb, scene.rows, scene.cols), dtype=torch.uint8, device=cuda)
+        args = [device_ptr(scene.dsm), device_ptr(scene.vegdem), device_ptr(scene.vegdem2), device_ptr(geo),
+                device_ptr(scene.flags), scene.rows, scene.cols, lay.struct.patches, cap, device_ptr(t_dxdy),
+                device_ptr(t_dz), device_ptr(t_len), scene.hmax, ctypes.byref(lay.struct),
+                lay.band_weights.ctypes.data_as(ctypes.c_void_p), lay.sectors.ctypes.data_as(ctypes.c_void_p),
+                0.03, device_ptr(masks), device_ptr(planes), device_ptr(veg), device_ptr(cnt)]
+        if ex2:
+            work = torch.empty(int(L.solweig_svf_work_bytes(scene.rows, scene.cols)), dtype=torch.uint8,
+                               device=cuda)
+            _lib.check(L.solweig_svf_ex2(*args, device_ptr(work), work.numel(), stream_handle()), "svf_ex2")
+        else:
+            _lib.check(L.solweig_svf_ex(*args, stream_handle()), "svf_ex")
+        torch.cuda.synchronize()
+        out[ex2] = (masks, planes, veg, cnt)
+    for a, b in zip(out[False], out[True]):
+        assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
+    assert torch.equal(out[True][0], scene.masks)
