@@ -43,10 +43,14 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
     __shared__ uint8_t state[kSvfPatchGroup][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long pixels = (long long)prm.rows * prm.cols;
-    const long long p = (long long)blockIdx.x * 32 + lane;
+    // the block's 32 pixels: an 8 x 4 (columns x rows) tile, whose walks are
+    // more alike than those of 32 pixels in a row
+    const int tiles_x = (prm.cols + 7) / 8;
+    const int rr = (blockIdx.x / tiles_x) * 4 + (lane >> 3), cc = (blockIdx.x % tiles_x) * 8 + (lane & 7);
     const int word = word0 + blockIdx.y;
-    const bool valid = p < pixels;
-    const int r = valid ? (int)(p / prm.cols) : 0, c = valid ? (int)(p % prm.cols) : 0;
+    const bool valid = rr < prm.rows && cc < prm.cols;
+    const int r = valid ? rr : 0, c = valid ? cc : 0;
+    const long long p = (long long)r * prm.cols + c;
     const double a = valid ? dsm[p] : 0.0;
     const double top_p = valid ? top[p] : 0.0;
     const bool bush = valid && (flags[p] & 2);
@@ -268,6 +272,9 @@ extern "C" int solweig_svf_pack(const float* shmat, const float* vegmat, const f
     return SOLWEIG_OK;
 }
 
+// Blocks of the visibility kernel: 8 x 4 pixel tiles.
+unsigned svf_tiles(int rows, int cols) { return (unsigned)(((cols + 7) / 8) * ((rows + 3) / 4)); }
+
 // first_outside tables of a group of patches: block j = patch0 + j.
 __global__ void __launch_bounds__(1024) patch_ray_exits_kernel(int rows, int cols, const int2* __restrict__ rays,
                                                                const int32_t* __restrict__ lengths, int capacity,
@@ -362,7 +369,7 @@ int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, con
     const int2* rays = reinterpret_cast<const int2*>(ray_dxdy);
     const float4* g4 = reinterpret_cast<const float4*>(geo32);
     if (!work) {
-        dim3 grid(blocks_for(pixels, 32), words);
+        dim3 grid(svf_tiles(rows, cols), words);
         if (g4) svf_visibility_kernel<1><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp, rays,
                                                                           ray_dz, lengths, masks, 0, nullptr, nullptr);
         else svf_visibility_kernel<0><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp, rays,
@@ -396,7 +403,7 @@ int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, con
             SOLWEIG_CHECK_LAUNCH("patch_ray_ceiling_kernel");
             patch_ray_exits_kernel<<<cnt, 1024, 0, st>>>(rows, cols, rays, lengths, capacity, p0, cnt, exits);
             SOLWEIG_CHECK_LAUNCH("patch_ray_exits_kernel");
-            dim3 grid(blocks_for(pixels, 32), 1);
+            dim3 grid(svf_tiles(rows, cols), 1);
             if (g4) svf_visibility_kernel<2><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
                                                                               rays, ray_dz, lengths, masks, wd, ceil,
                                                                               exits);
