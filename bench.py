@@ -42,7 +42,7 @@ def _args():
     p.add_argument("--impl", choices=("solweig", "reference"), default="solweig")
     p.add_argument("--size", type=int, default=2000)
     p.add_argument("--form", choices=("plain", "batched", "chosen"), default="chosen")
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient"), default="day",
                    help="day: the headline 2000^2 x 24 h line; month: 2000^2 x 720 h in one graph; "
@@ -567,7 +567,9 @@ def main():
         if i > 0:
             e2e_times.append(dt)
         h2d, d2h = res["h2d_bytes"], res["d2h_bytes"]
-    e2e_s = float(np.mean(e2e_times)) if e2e_times else float("nan")
+    # median over the steps (a step that meets a cold allocator or a busy host
+    # would otherwise dominate a short run); every step is listed in the line
+    e2e_s = float(np.median(e2e_times)) if e2e_times else float("nan")
     if dist is not None:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -596,6 +598,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_s,
+                    "seconds_each_step": [round(t, 4) for t in e2e_times],
                     "includes": "H2D rasters, walls, 153-patch SVF, 24 h, D2H Tmrt+UTCI"},
             "gpu_launches": launches_per_day * a.steps,
             "clocks": clocks.summary(),
