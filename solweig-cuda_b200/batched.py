@@ -245,7 +245,7 @@ class ChosenDay(BatchedDay):
         return {
             "day_shadow_kernel": pixels * day_hours * 101,
             "day_gvf_kernel": pixels * day_hours * 40,
-            "day_tables_kernel": hours * 9552,
+            "day_tables_kernel": hours * 9680,
             "patch_gemm_kernel": pixels * (40 + 16 * hours),
             "day_radiation_kernel": pixels * (125 + 28 * day_hours + 8 * hours),
         }
