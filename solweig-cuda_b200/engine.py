@@ -222,10 +222,11 @@ def wall_aspect(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
     return aspect, walls
 
 
-def wall_aspect_device(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
+def wall_aspect_device(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None, host_work=None):
     """Wall aspect in degrees as a float64 device tensor (``src/walls.py:83-129``):
     the template kernel on the device, the gradient fall-back only at the few
-    wall pixels the templates leave unresolved (from ``dsm_host`` when given)."""
+    wall pixels the templates leave unresolved (from ``dsm_host`` when given).
+    ``host_work`` (optional) runs on the host while the template kernel runs."""
     rows, cols = dsm_dev.shape
     key = float(pixel_size)
     if key not in _TEMPLATE_CACHE:
@@ -234,6 +235,8 @@ def wall_aspect_device(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
     mask = walls_dev > 0
     aspect = torch.zeros_like(dsm_dev)
     if not bool(mask.any()):
+        if host_work is not None:
+            host_work()
         return aspect
     if rows > 2 * radius + 2 and cols > 2 * radius + 2:
         dev = dsm_dev.device
@@ -242,6 +245,8 @@ def wall_aspect_device(dsm_host, dsm_dev, walls_dev, pixel_size, stream=None):
             device_ptr(dsm_dev), device_ptr(walls_dev), device_ptr(aspect), rows, cols, radius,
             device_ptr(t[0][0]), device_ptr(t[0][1]), device_ptr(t[1][0]), device_ptr(t[1][1]),
             device_ptr(t[2][0]), device_ptr(t[2][1]), stream_handle(stream)), "solweig_wall_aspect")
+    if host_work is not None:
+        host_work()
     unresolved = torch.nonzero((mask & (aspect == 0)).flatten()).flatten()
     if unresolved.numel():
         host = dsm_host if dsm_host is not None else dsm_dev.cpu().numpy()
@@ -304,19 +309,8 @@ class Scene:
         L = _lib.lib()
         st = stream_handle(stream)
         n = self.pixels
-        # Walls from the unraised DSM, rounded through float32 (src/series.py:213-236).
-        if walls is None:
-            walls_dev = wall_heights_device(dsm_in, wall_threshold, stream)
-            aspect_dev = wall_aspect_device(dsm if isinstance(dsm, np.ndarray) else None, dsm_in, walls_dev,
-                                            pixel_size, stream)
-        else:
-            walls_dev = _raster_to_device(walls, dev)
-            aspect_dev = _raster_to_device(aspect, dev)
-        self.walls = walls_dev.to(torch.float32).to(torch.float64)
-        self._aspect_deg = aspect_dev.to(torch.float32).to(torch.float64)
-        self.aspect = ((self._aspect_deg * math.pi) / 180.).contiguous()
-        del walls_dev, aspect_dev
-        # Raise / clip semantics of src/series.py:252-291.
+        # Raise / clip semantics of src/series.py:252-291 (host syncs, so before
+        # the wall kernels: the SVF rays are built on the host while they run).
         raise_dsm = max(0.0, -float(dsm_in.min()))
         raise_dem = max(0.0, -float(dem_in.min()))
         a_min, a_max = float(dsm_in.min()) + raise_dsm, float(dsm_in.max()) + raise_dsm
@@ -324,6 +318,23 @@ class Scene:
         self.amaxvalue = float(max(a_max - a_min, t1_max))
         self.dsm_max = a_max
         self.hmax = float(a_max + max(t1_max, 0.0))
+        svf_ray_tables = []
+
+        def build_svf_rays():
+            svf_ray_tables.append(rays.svf_rays(patch_option, self.shape, self.amaxvalue, self.scale))
+
+        # Walls from the unraised DSM, rounded through float32 (src/series.py:213-236).
+        if walls is None:
+            walls_dev = wall_heights_device(dsm_in, wall_threshold, stream)
+            aspect_dev = wall_aspect_device(dsm if isinstance(dsm, np.ndarray) else None, dsm_in, walls_dev,
+                                            pixel_size, stream, host_work=build_svf_rays)
+        else:
+            walls_dev = _raster_to_device(walls, dev)
+            aspect_dev = _raster_to_device(aspect, dev)
+        self.walls = walls_dev.to(torch.float32).to(torch.float64)
+        self._aspect_deg = aspect_dev.to(torch.float32).to(torch.float64)
+        self.aspect = ((self._aspect_deg * math.pi) / 180.).contiguous()
+        del walls_dev, aspect_dev
         lc_in = _raster_to_device(landcover, dev) if landcover is not None else None
         self.landcover = 1 if landcover is not None else 0
         f64 = dict(dtype=torch.float64, device=dev)
@@ -357,7 +368,9 @@ class Scene:
         del dsm_in, trees_in, dem_in, lc_in
         self.has_water = int(bool(((self.flags & 4) != 0).any().item())) if landcover is not None else 0
         # Sky view factor: bit-packed visibility + the 16 reduce planes.
-        dxdy, dz, lengths, cap = rays.svf_rays(patch_option, self.shape, self.amaxvalue, self.scale)
+        if not svf_ray_tables:
+            build_svf_rays()
+        dxdy, dz, lengths, cap = svf_ray_tables[0]
         self.svf_steps = int(lengths.sum())
         t_dxdy = _upload(dxdy, np.int32, dev)
         t_dz = _upload(dz, np.float64, dev)
