@@ -123,17 +123,19 @@ class ChosenDay(BatchedDay):
     CARDINAL = ("keast", "ksouth", "kwest", "knorth", "least", "lsouth", "lwest", "lnorth")
 
     def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0, hours=24,
-                 outputs=("tmrt", "utci"), use_graph=True, pipeline_hours=2):
+                 outputs=("tmrt", "utci"), use_graph=True, pipeline_hours=(2, 2, 2, 2, 4, 4, 8)):
         bad = [o for o in outputs if o in self.CARDINAL]
         if bad:
             raise ValueError(f"the batched form does not produce {bad}")
         super().__init__(scene, latitude, longitude, site_altitude, utc, hours, outputs, use_graph)
         self.scratch = None
-        # pipeline_hours > 0: the sweep stage runs in ranges of that many hours,
-        # each launched as soon as its hours are planned (the host plans the
-        # next range while the GPU sweeps this one); 0: plan the whole day first.
-        self.ranges = ([(h, min(h + pipeline_hours, hours)) for h in range(0, hours, pipeline_hours)]
-                       if pipeline_hours > 0 else None)
+        # pipeline_hours: the sweep stage runs in ranges of hours, each launched
+        # as soon as its hours are planned (the host plans the next range while
+        # the GPU sweeps this one): an int gives ranges of that many hours, a
+        # sequence the successive range lengths (the last one repeats), 0 plans
+        # the whole day first.  The default starts with short ranges, so the
+        # GPU starts early, and grows them, so fewer launches are paid for.
+        self.ranges = self._ranges(hours, pipeline_hours)
         self.part_graphs = None
         L = _lib.lib()
         self.work_bytes = int(L.solweig_day_batched_work_bytes(scene.rows, scene.cols, hours,
@@ -142,6 +144,23 @@ class ChosenDay(BatchedDay):
             raise ValueError("bad batched-day shape")
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=scene.device)
         self.config = _lib.SolweigDayConfig.default()
+
+    @staticmethod
+    def _ranges(hours, pipeline_hours):
+        if isinstance(pipeline_hours, int):
+            if pipeline_hours <= 0:
+                return None
+            lengths = [pipeline_hours]
+        else:
+            lengths = [int(x) for x in pipeline_hours]
+            if not lengths or min(lengths) <= 0:
+                raise ValueError("pipeline_hours: range lengths must be positive")
+        out, h, i = [], 0, 0
+        while h < hours:
+            n = lengths[min(i, len(lengths) - 1)]
+            out.append((h, min(h + n, hours)))
+            h, i = h + n, i + 1
+        return out
 
     @property
     def launches_per_day(self):

@@ -267,7 +267,8 @@ def test_ray_ceiling_exit_is_bit_identical(cuda, doy, lat, shift):
             assert torch.equal(o1[k].view(torch.int32), o0[k].view(torch.int32)), (packed, k)
 
 
-def test_pipelined_sweep_ranges_match_whole_day(scene64):
+@pytest.mark.parametrize("ranges", [5, (1, 2, 3, 7)])
+def test_pipelined_sweep_ranges_match_whole_day(scene64, ranges):
     """Sweep ranges launched as their hours are planned (eager first day, then
     graph replays) give the whole-day results bit for bit, on two forcings."""
     import torch
@@ -275,7 +276,7 @@ def test_pipelined_sweep_ranges_match_whole_day(scene64):
     sc, scene = scene64
     outs = ("tmrt", "utci", "shadow", "kdown")
     whole = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, outputs=outs, pipeline_hours=0)
-    piped = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, outputs=outs, pipeline_hours=5)
+    piped = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, outputs=outs, pipeline_hours=ranges)
     assert piped.launches_per_day > whole.launches_per_day
     for doy, seed in ((172, 0), (200, 3), (172, 0)):
         met = synthetic.make_met(doy=doy, latitude=53.0, longitude=0.0, seed=seed)
