@@ -12,7 +12,7 @@ import threading
 import numpy as np
 import torch
 
-from . import engine
+from . import engine, tune
 from .batched import BatchedDay, ChosenDay
 
 __all__ = ["simulate_day"]
@@ -51,6 +51,11 @@ def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixe
     if form == "chosen":
         runner = ChosenDay(scene, latitude, longitude, site_altitude, utc, hours=len(met),
                            use_graph=False)
+        # launch shapes tuned earlier for this device and tile size, if any
+        # (the call itself never tunes)
+        cached = tune.lookup(runner)
+        if cached is not None:
+            runner.set_config(cached)
     elif form == "batched":
         runner = BatchedDay(scene, latitude, longitude, site_altitude, utc, hours=len(met),
                             use_graph=False)

@@ -383,6 +383,13 @@ class Scene:
         self.sky_band_counts = torch.empty((nb, self.rows, self.cols), dtype=torch.uint8, device=dev)
         lay = self.layout
         self.geo32 = self._packed_geometry()
+        self._geo_checked = True
+        # GVF step offsets, uploaded before the SVF launch: nothing after it
+        # waits for the device, so the host returns (and can plan the day)
+        # while the SVF runs
+        self.gvf_dxdy_host, self.first_steps, self.second_steps = rays.gvf_offsets(self.scale)
+        self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
+        self.gvf_host_ptr = self.gvf_dxdy_host.ctypes.data_as(ctypes.c_void_p)
         # ray ceilings and exit tables of one patch word (solweig_svf_ex2)
         svf_work = torch.empty(int(L.solweig_svf_work_bytes(self.rows, self.cols)), dtype=torch.uint8, device=dev)
         _lib.check(L.solweig_svf_ex2(
@@ -408,9 +415,6 @@ class Scene:
             device_ptr(self.svf32), device_ptr(self.svfbuveg), device_ptr(self.svfalfa),
             device_ptr(self.tan_asvf), device_ptr(self.gvf_face), st), "solweig_scene_finalize")
         self.planes = planes if keep_planes else None
-        self.gvf_dxdy_host, self.first_steps, self.second_steps = rays.gvf_offsets(self.scale)
-        self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
-        self.gvf_host_ptr = self.gvf_dxdy_host.ctypes.data_as(ctypes.c_void_p)
         self.struct = self._make_struct()
 
     @classmethod
