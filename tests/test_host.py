@@ -120,3 +120,18 @@ def test_shard_split_is_a_partition():
         parts = [shard.split(units, r, world) for r in range(world)]
         assert sum(parts, []) == units
         assert max(map(len, parts)) - min(map(len, parts)) <= 1
+
+
+def test_pipelined_sweep_ranges_cover_the_day():
+    """Hour ranges of the pipelined batched day: consecutive, covering every
+    hour once, the last length repeating; 0 turns pipelining off."""
+    from solweig_cuda_b200.batched import ChosenDay
+    assert ChosenDay._ranges(24, 0) is None
+    for hours, spec in ((24, (2, 2, 2, 2, 4, 4, 8)), (24, 5), (7, (1, 2)), (30, (3, 9)), (1, 4)):
+        r = ChosenDay._ranges(hours, spec)
+        assert r[0][0] == 0 and r[-1][1] == hours
+        assert all(a[1] == b[0] and a[0] < a[1] for a, b in zip(r, r[1:]))
+    assert ChosenDay._ranges(24, (2, 2, 2, 2, 4, 4, 8)) == [(0, 2), (2, 4), (4, 6), (6, 8), (8, 12), (12, 16),
+                                                             (16, 24)]
+    with pytest.raises(ValueError):
+        ChosenDay._ranges(24, (2, 0))
