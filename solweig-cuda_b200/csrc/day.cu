@@ -1,20 +1,28 @@
-// The batched form of a SOLWEIG day: all hours of one day in seven launches
+// The batched form of a SOLWEIG day: all hours of one day in a few launches
 // (instead of three per hour), with the luminance-weighted patch sums of all
-// hours as one BF16 tensor-core contraction.
+// hours as one BF16 tensor-core contraction.  The sweep stage can be issued
+// in hour ranges (solweig_day_batched_part) while the host plans later hours.
 //
-//  0 ceiling_dilate_kernel, day_ray_ceiling_kernel (grid.z = hour): upper
-//                           bounds of the heights ahead along the sun ray
-//                           (early exit of the sweep)
+//  0 ceiling_dilate_kernel  once per day: height planes dilated along rows /
+//                           columns; day_ray_ceiling_kernel, grid.z = hour:
+//                           upper bounds of the heights ahead along the sun
+//                           ray (early exit of the sweep);
+//                           day_ray_exits_kernel: first step outside the
+//                           raster of every row and column
 //  1 day_shadow_kernel      grid.z = hour: shadow sweep + GVF field quads
-//  2 day_gvf_kernel         grid.z = hour: all-direction GVF (Lup, albedo) +
-//                           the pixel's shadow; the hour-independent
+//  2 day_gvf_hv_kernel      32 x 32 tiles, every daytime hour per block (4 per
+//                           shared-memory pass): all-direction GVF (Lup,
+//                           albedo) + the pixel's shadow, the hour-independent
 //                           albedo-without-shadow GVF once per day
+//                           (day_gvf_kernel, grid.z = hour, for other walk
+//                           lengths and water scenes)
 //  3 day_weights_kernel     per-hour patch weights (luminance, luminance*cos*omega)
 //  4 split_bf16_kernel      weights -> BF16 hi/lo pair in the canonical
 //                           K-major shared-memory layout of the contraction
 //  5 day_tables_kernel      per hour: exact thresholds on tan(asvf) for the
 //                           sunlit / shaded split of building patches, sorted,
-//                           with the prefix/suffix patch masks
+//                           with the prefix/suffix patch masks, bucket start
+//                           tables and the hour's flux scalars
 //  6 patch_gemm_kernel      tcgen05: [128 px x 160 patches] 0/1 sky (vegetation)
 //                           masks x [160 x 2H] weights, FP32 in tensor memory
 //  7 day_radiation_kernel   one thread per pixel loops over the hours: wave
@@ -32,8 +40,8 @@
 // (src/umep_solweig.py:1362-1397) compares fl(tan(asvf) + yi_k) against
 // fixed per-patch limits; for each patch and hour that is equivalent to one
 // compare of tan(asvf) with a float64 threshold found by bisection over the
-// doubles, so a pixel-hour needs two binary searches and band popcounts
-// instead of a loop over its building patches.
+// doubles, so a pixel-hour needs two short scans from a 256-bucket start
+// table and band popcounts instead of a loop over its building patches.
 #include "day_kernels.cuh"
 
 using namespace solweig;
