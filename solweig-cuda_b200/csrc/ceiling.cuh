@@ -42,7 +42,8 @@
 // consecutive floats.
 //
 // Scan layout: a block owns 32 consecutive sheared lines (one per lane) and
-// splits the major axis into 32 segments (one per warp).  Phase 1 scans each
+// splits the major axis into 16 segments (one per warp; 512 threads, so two
+// blocks fit per SM).  Phase 1 scans each
 // segment backwards from -inf; phase 2 carries the later segments' maxima in
 // and rescans, writing the plane.
 #pragma once
@@ -51,7 +52,7 @@
 namespace solweig {
 
 constexpr int kCeilLanes = 32;     // sheared lines per block
-constexpr int kCeilWarps = 32;     // major-axis segments per block
+constexpr int kCeilWarps = 16;     // major-axis segments per block
 constexpr int kCeilMaxBand = 3;    // largest dilation W handled
 constexpr int kCeilMinSteps = 5;   // the sweep consults the plane from step 4 on
 
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(256) ceiling_dilate_kernel(SolweigScene S, flo
 }
 
 // The ceiling plane of one ray table (K steps) for the raster of S, by one
-// block of (32, 32) threads owning 32 sheared lines (blockIdx.x); the whole
+// block of (32, kCeilWarps) threads owning 32 sheared lines (blockIdx.x); the whole
 // block returns together.  Tables the frame does not fit give a +inf plane.
 __device__ __forceinline__ void ray_ceiling_block(const SolweigScene& S, const int2* __restrict__ ray,
                                                   const double* __restrict__ dz, int K,
@@ -298,7 +299,7 @@ __device__ __forceinline__ void ray_ceiling_block(const SolweigScene& S, const i
     ceiling_scan(plane, f, S.cols, line0, s_seg, out);
 }
 
-// grid (ceil((rows + cols) / 32), 1, hours), block (32, 32): the ceiling plane
+// grid (ceil((rows + cols) / 32), 1, hours), block (32, kCeilWarps): the ceiling plane
 // of every daytime hour whose ray has at least kCeilMinSteps steps, from the
 // dilated planes of ceiling_dilate_kernel.
 static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
