@@ -1,14 +1,19 @@
 """Command line of the B200 engine, mirroring the reference's ``run.py``.
 
-    python run.py --case case.json [--output DIR] [--dtype float32|float64]
+    python run.py [--case case.json] [--output DIR] [--dtype float32]
                   [--output-core ROW COL ROWS COLS] [--output-chunk-steps N]
                   [--sync-output] [--output-queue-size N] [--no-write] [--progress]
-                  [--check]
+                  [--check] [--form chosen|batched]
 
 Case keys follow the reference's ``examples/case.json`` (paths relative to the
-case file).  Rasters are ``.npy`` arrays (GeoTIFF where rasterio/GDAL is
+case file; the default case is ``examples/case.json`` beside this file, as in
+the reference).  Rasters are ``.npy`` arrays (GeoTIFF where rasterio/GDAL is
 installed).  ``case_type: open_data`` needs network downloads and is not
-supported; ``core_area_m`` / ``buffer_area_m`` tile the rasters with halos.
+supported; ``core_area_m`` / ``buffer_area_m`` tile the rasters with halos and
+every group of tiles runs day by day in one captured graph per day
+(``series.run_tiles``).  Under ``torchrun`` each rank takes a share of the
+days (one tile) or of the tiles (tiled cases).  Only ``--dtype float32`` runs:
+the reference's float64 radiation switch is not provided.
 """
 from __future__ import annotations
 
@@ -50,32 +55,37 @@ def load_case(path):
 
 
 def _tile_jobs(case, settings):
-    if "core_area_m" not in settings:
-        return [(settings.get("case_name", "tile"), dict(case), None)]
+    """Tiles of a tiled case (``run.py:113-129`` of the reference): dicts with
+    the tile id, the input-window arrays and the output core, for
+    ``series.run_tiles``."""
     import numpy as np
     from solweig_cuda_b200.series import load_raster
     from solweig_cuda_b200 import tiling
     res = float(settings.get("resolution_m", 1))
     core, halo = (int(round(settings[k] / res)) for k in ("core_area_m", "buffer_area_m"))
-    rasters = {k: load_raster(case[k]) for k in ("building_dsm_path", "tree_path", "dem_path")}
+    names = {"building_dsm_path": "dsm", "tree_path": "trees", "dem_path": "dem"}
     if case.get("landcover_path"):
-        rasters["landcover_path"] = load_raster(case["landcover_path"])
-    h, w = rasters["building_dsm_path"].shape
+        names["landcover_path"] = "landcover"
+    rasters = {names[k]: load_raster(case[k]) for k in names}
+    h, w = rasters["dsm"].shape
     jobs = []
     for t in tiling.tile_windows(h, w, core=core, halo=halo):
-        opts = dict(case)
+        job = {"tile_id": t["tile_id"], "output_core": t["output_core"]}
         for k, arr in rasters.items():
-            opts[k] = np.ascontiguousarray(tiling.extract(arr, t))
-        opts["output_core"] = t["output_core"]
-        jobs.append((t["tile_id"], opts, t))
+            job[k] = np.ascontiguousarray(tiling.extract(arr, t))
+        jobs.append(job)
     return jobs
 
 
 def main(argv=None):
     parser = argparse.ArgumentParser(description="Run SOLWEIG on the GPU for the supplied rasters and forcing.")
-    parser.add_argument("--case", type=Path, required=True)
+    parser.add_argument("--case", type=Path, default=Path(ROOT) / "examples" / "case.json",
+                        help="JSON case file (default: examples/case.json beside run.py); paths are relative to it")
     parser.add_argument("--output", type=Path)
-    parser.add_argument("--dtype", choices=("float32", "float64"), default="float32")
+    parser.add_argument("--dtype", choices=("float32",), default="float32",
+                        help="radiation precision (float32 only; the float64 switch is not provided)")
+    parser.add_argument("--form", choices=("chosen", "batched"), default="chosen",
+                        help="chosen: batched day with tensor-core patch sums; batched: per-hour kernels in a graph")
     parser.add_argument("--output-core", type=int, nargs=4, metavar=("ROW", "COL", "ROWS", "COLS"))
     parser.add_argument("--output-chunk-steps", type=int)
     parser.add_argument("--sync-output", action="store_true")
@@ -110,14 +120,24 @@ def main(argv=None):
     from solweig_cuda_b200.series import load_meteorology, run_timeseries
     forcing = load_meteorology(case["met_file"])
     case["met_file"] = forcing
-    for label, options, tile in _tile_jobs(case, settings):
-        dest = output / label if tile is not None else output
+    pixel_size = float(settings.get("resolution_m", 1))
+    if "core_area_m" in settings:
+        from solweig_cuda_b200.series import run_tiles
+        known = {"longitude", "latitude", "utc_offset_hours", "site_altitude_m", "output_chunk_steps",
+                 "async_output", "output_queue_size", "save_tmrt", "save_kup", "save_kdown", "save_lup",
+                 "save_ldown", "save_shadow", "dsm_wall_threshold_m"}
+        kwargs = {k: v for k, v in case.items() if k in known}
+        run_tiles(_tile_jobs(case, settings), forcing, output, dtype=np.dtype(args.dtype), no_write=args.no_write,
+                  progress=args.progress, pixel_size=pixel_size, **kwargs)
+    else:
         known = {"building_dsm_path", "tree_path", "dem_path", "met_file", "longitude", "latitude",
                  "landcover_path", "utc_offset_hours", "site_altitude_m", "output_core",
-                 "output_chunk_steps", "async_output", "output_queue_size"}
-        kwargs = {k: v for k, v in options.items() if k in known}
-        run_timeseries(output_path=dest, dtype=np.dtype(args.dtype), no_write=args.no_write,
-                       progress=args.progress, pixel_size=float(settings.get("resolution_m", 1)), **kwargs)
+                 "output_chunk_steps", "async_output", "output_queue_size", "save_tmrt", "save_svf",
+                 "save_kup", "save_kdown", "save_lup", "save_ldown", "save_shadow", "dsm_wall_threshold_m",
+                 "output_valid_mask"}
+        kwargs = {k: v for k, v in case.items() if k in known}
+        run_timeseries(output_path=output, dtype=np.dtype(args.dtype), no_write=args.no_write,
+                       progress=args.progress, pixel_size=pixel_size, form=args.form, **kwargs)
     if args.progress and not args.no_write:
         print(f"[{datetime.now():%H:%M:%S}] Results: {output}", flush=True)
     return 0

@@ -306,6 +306,16 @@ class ChosenDay(BatchedDay):
                    "solweig_day_batched_layout")
         return dict(zip(self.WORK_FIELDS, (int(x) for x in off)))
 
+    def quads(self):
+        """The sweep's per-pixel GVF inputs of the last day as a [H, rows, cols, 4]
+        float32 view: shadow, Lup excess, albedo and the ground (1) / sunlit-wall
+        (2) bits as an int32 bit pattern (daytime hours only; night hours hold
+        stale values)."""
+        o = self.work_offsets()
+        n = 16 * self.hours * self.scene.pixels
+        return self.work[o["quads"]:o["quads"] + n].view(torch.float32).view(self.hours, self.scene.rows,
+                                                                                 self.scene.cols, 4)
+
     def patch_sums(self):
         """The contraction's output of the last day as a [2, 2H, pixels] view:
         [sky|vegetation][2h + (0: luminance, 1: luminance*cos*omega)]."""

@@ -9,8 +9,11 @@
 // a per-call allocation can fail part way through a long run).  Such a caller
 // would otherwise have to reserve and manage 20 scratch planes itself.
 //
-// The array lives in its own translation unit so its module (and its 20 MiB)
-// is only loaded by processes that call this entry point.
+// The array is reserved on a device when the library's device code is loaded
+// there.  Under CUDA's default lazy module loading that happens at the first
+// call of this entry point on the device, so other processes do not pay the
+// 20 MiB; with CUDA_MODULE_LOADING=EAGER every process that creates a context
+// after loading libsolweig_b200.so reserves it on that device.
 #include <mutex>
 
 #include "common.cuh"

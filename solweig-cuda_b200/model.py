@@ -88,6 +88,33 @@ class _StepRunner:
 
 _RUNNERS = {}
 
+# prepare_model results of calls without ``prepared``, keyed by the identity
+# of the static inputs (the arrays are held here, so their ids stay unique).
+_STATIC_ARGS = ("dsm", "svf", "svfN", "svfW", "svfE", "svfS", "svfveg", "svfNveg", "svfEveg", "svfSveg",
+                "svfWveg", "svfaveg", "svfEaveg", "svfSaveg", "svfWaveg", "svfNaveg", "vegdem", "vegdem2",
+                "buildings", "lc_grid", "dirwalls", "walls", "bush", "TgK", "Tstart", "alb_grid",
+                "emis_grid", "TmaxLST", "svfalfa", "svfbuveg", "diffsh", "shmat", "vegshmat",
+                "vbshvegshmat", "asvf")
+_STATIC_SCALARS = ("scale", "amaxvalue", "landcover", "patch_option", "first", "second")
+_PREPARED = []  # [(key, held arrays, PreparedModel)], most recent last
+_PREPARED_MAX = 2
+
+
+def _prepared_for(args, dtype):
+    key = tuple(id(args[k]) for k in _STATIC_ARGS) + tuple(
+        float(args[k]) if np.ndim(args[k]) == 0 else id(args[k]) for k in _STATIC_SCALARS) + (str(np.dtype(dtype)),)
+    for i, (k, _, prep) in enumerate(_PREPARED):
+        if k == key:
+            _PREPARED.append(_PREPARED.pop(i))
+            return prep
+    inputs = {k: v for k, v in args.items() if k not in ("prepared", "dtype")}
+    prep = prepare_model(dtype=dtype, **inputs)
+    _PREPARED.append((key, tuple(args[k] for k in _STATIC_ARGS), prep))
+    while len(_PREPARED) > _PREPARED_MAX:
+        old = _PREPARED.pop(0)
+        _RUNNERS.pop(id(old[2].scene), None)
+    return prep
+
 
 def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, svfveg, svfNveg, svfEveg, svfSveg,
                        svfWveg, svfaveg, svfEaveg, svfSaveg, svfWaveg, svfNaveg, vegdem, vegdem2, albedo_b, absK, absL,
@@ -97,7 +124,14 @@ def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, s
                        TmaxLST_wall, first, second, svfalfa, svfbuveg, firstdaytime, timeadd, timestepdec, Tgmap1,
                        Tgmap1E, Tgmap1S, Tgmap1W, Tgmap1N, CI, TgOut1, diffsh, shmat, vegshmat, vbshvegshmat,
                        anisotropic_sky, asvf, patch_option, *, dtype=np.float32, prepared=None):
-    """One SOLWEIG 2022a hour on the device; returns the reference's 39-tuple."""
+    """One SOLWEIG 2022a hour on the device; returns the reference's 39-tuple.
+
+    Without ``prepared`` the device geometry is built on the first call and
+    reused by later calls given the same static array objects (the two most
+    recent sets are kept); arrays changed in place between calls need a new
+    ``prepare_model``.  ``dtype`` float64 returns float64 planes computed by
+    the float32 step (the reference's float64 radiation switch is not
+    provided)."""
     args = dict(locals())
     _check_switches(args)
     constants = dict(albedo_b=0.2, absK=0.7, absL=0.95, ewall=0.9, Fside=0.22, Fup=0.06, Fcyl=0.28,
@@ -106,8 +140,7 @@ def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, s
         if abs(float(args[k]) - v) > 1e-12:
             raise NotImplementedError(f"{k}={args[k]} differs from the compiled constant {v}")
     if prepared is None:
-        inputs = {k: v for k, v in args.items() if k not in ("prepared", "dtype")}
-        prepared = prepare_model(dtype=dtype, **inputs)
+        prepared = _prepared_for(args, dtype)
     scene = prepared.scene
     key = id(scene)
     if key not in _RUNNERS:

@@ -7,10 +7,12 @@ arguments and day grouping (``src/series.py:91-194``).  Differences, by design:
   works only where ``rasterio`` or GDAL is importable;
 * outputs are written as ``.npy`` stacks [steps, rows, cols] float32 with a
   JSON sidecar of timestamps instead of DEFLATE GeoTIFFs;
-* each day runs as one captured CUDA graph (:class:`batched.BatchedDay`) and
-  its outputs are copied to pinned host memory on a separate stream while the
+* each day runs in the batched form (:class:`batched.ChosenDay`: all hours
+  of the day in a few launches, replayed from captured CUDA graphs) and its
+  outputs are copied to pinned host memory on a separate stream while the
   next day computes; a bounded writer thread stores them
-  (``src/output.py:11-102``, ``src/runtime.py:79-163``).
+  (``src/output.py:11-102``, ``src/runtime.py:79-163``);
+* calendar days can be split over ranks (one process per GPU, no exchange).
 """
 from __future__ import annotations
 
@@ -25,11 +27,11 @@ from pathlib import Path
 import numpy as np
 import torch
 
-from . import engine
-from .batched import BatchedDay
+from . import engine, shard
+from .batched import BatchedDay, ChosenDay
 
 __all__ = ["DayForcing", "Meteorology", "load_meteorology", "run_timeseries", "load_raster",
-           "OutputWriter"]
+           "OutputWriter", "rank_and_world"]
 
 
 @dataclass(frozen=True)
@@ -157,14 +159,79 @@ class OutputWriter:
             self._thread = None
 
 
-def _write_chunk(folder, names, host, steps, copy_done, crop, meta):
+def _write_chunk(folder, names, host, steps, copy_done, crop, meta, valid=None):
+    """Writer job of one output chunk: waits for its device-to-host copy, crops
+    to the output core and, with an output mask, sets the pixels outside it
+    to NaN on the cropped array (``src/output.py:205-216``)."""
     copy_done.synchronize()
     folder.mkdir(parents=True, exist_ok=True)
     r, c = crop
     for name in names:
-        arr = host[name][:steps][:, r, c]
-        np.save(folder / f"{name}.npy", np.ascontiguousarray(arr))
+        arr = np.array(host[name][:steps][:, r, c], dtype=np.float32)
+        if valid is not None:
+            arr[:, ~valid] = np.nan
+        np.save(folder / f"{name}.npy", arr)
     (folder / "timestamps.json").write_text(json.dumps(meta))
+
+
+class _HostCopy:
+    """Device-to-host copy of one day's output planes into page-locked memory
+    on a side stream; ``synchronize`` waits for it (a no-op on CPU tensors)."""
+
+    def __init__(self, planes, copy_stream):
+        self.host = {}
+        self.event = None
+        if copy_stream is None:
+            for k, v in planes.items():
+                self.host[k] = v.detach().cpu().numpy().copy()
+            return
+        copy_stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(copy_stream):
+            for k, v in planes.items():
+                h = torch.empty(v.shape, dtype=torch.float32, pin_memory=True)
+                h.copy_(v, non_blocking=True)
+                self.host[k] = h.numpy()
+            self.event = torch.cuda.Event()
+            self.event.record(copy_stream)
+        # the next day writes the same device buffers: the compute stream waits for the copy
+        torch.cuda.current_stream().wait_event(self.event)
+
+    def synchronize(self):
+        if self.event is not None:
+            self.event.synchronize()
+
+
+def rank_and_world(rank=None, world_size=None):
+    """This process's rank and the number of ranks: the arguments, else an
+    initialised ``torch.distributed`` group, else RANK / WORLD_SIZE from the
+    environment (as ``torchrun`` sets them), else (0, 1)."""
+    if rank is not None or world_size is not None:
+        r, w = int(rank or 0), int(world_size or 1)
+    else:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            r, w = dist.get_rank(), dist.get_world_size()
+        else:
+            r, w = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    if w < 1 or not 0 <= r < w:
+        raise ValueError(f"rank {r} outside a world of {w}")
+    return r, w
+
+
+def _default_device(rank, world):
+    if world > 1:
+        return f"cuda:{int(os.environ.get('LOCAL_RANK', rank)) % max(1, torch.cuda.device_count())}"
+    return "cuda"
+
+
+def _make_runner(scene, latitude, longitude, site_altitude, utc, hours, outputs, form):
+    """Runner of one day length: the batched form (``ChosenDay``: every hour
+    of the day in a few launches, tensor-core patch sums) for days of up to
+    64 rows, the per-hour kernels in one captured graph (``BatchedDay``) for
+    longer days or ``form="batched"``."""
+    if form == "chosen" and hours <= 64:
+        return ChosenDay(scene, latitude, longitude, site_altitude, utc, hours=hours, outputs=outputs)
+    return BatchedDay(scene, latitude, longitude, site_altitude, utc, hours=hours, outputs=outputs)
 
 
 def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path,
@@ -176,14 +243,34 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
                    save_lup=False, save_ldown=False, save_shadow=False, dtype=np.float32,
                    no_write=False, output_core=None, output_chunk_steps=24,
                    async_output=True, output_queue_size=2, output_valid_mask=None, progress=False,
-                   pixel_size=1.0, device="cuda"):
+                   pixel_size=1.0, device=None, form="chosen", rank=None, world_size=None,
+                   scene_factory=None, runner_factory=None):
     """Simulate every day of the forcing on one tile (``src/series.py:91-156``).
 
-    Returns ``{"static": {...}, "days": {date: {variable: [paths]}}}``.
+    Days run in the batched form (``form="chosen"``, :class:`batched.ChosenDay`)
+    unless ``form="batched"``.  With several ranks (``rank``/``world_size``, an
+    initialised process group, or RANK/WORLD_SIZE from ``torchrun``) each rank
+    runs a contiguous share of the calendar days on its own GPU
+    (``LOCAL_RANK``) and writes those days' folders; rank 0 also writes the
+    static rasters.  Days are independent (the thermal state resets every
+    day), so ranks exchange nothing.  ``dtype`` must be float32: the float64
+    radiation switch of the reference is not provided.  ``scene_factory`` and
+    ``runner_factory`` replace :class:`engine.Scene` and the day runner (for
+    tests of the host logic).
+
+    Returns ``{"static": {...}, "days": {date: {variable: [paths]}}}`` with the
+    days this rank ran.
     """
     if str(wall_method).strip().lower() != "dsm":
         raise NotImplementedError("only wall_method='dsm' is supported")
+    if np.dtype(dtype) != np.float32:
+        raise NotImplementedError("only dtype=float32 is supported: the float64 radiation switch of "
+                                  "the reference is not provided by this engine")
+    if form not in ("chosen", "batched"):
+        raise ValueError(f"form must be 'chosen' or 'batched', not {form!r}")
+    rank, world = rank_and_world(rank, world_size)
     forcing = load_meteorology(met_file)
+    days = shard.split(forcing.days, rank, world)
     output = Path(output_path).resolve()
     dsm = load_raster(building_dsm_path)
     trees = load_raster(tree_path)
@@ -191,17 +278,28 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
     lc = load_raster(landcover_path) if landcover_path is not None else None
     utc = float(longitude) / 15.0 if utc_offset_hours is None else float(utc_offset_hours)
     stamp = lambda msg: print(f"[{datetime.now():%H:%M:%S}] {msg}", flush=True) if progress else None  # noqa: E731
-    stamp("Spatial preparation started")
-    scene = engine.Scene(dsm, trees, dem, pixel_size, landcover=lc, wall_threshold=dsm_wall_threshold_m,
-                         device=device, keep_planes=save_svf)
-    files = {"static": {}, "days": {}}
-    writer = OutputWriter(enabled=bool(async_output and not no_write), max_inflight=output_queue_size)
     if output_core is None:
         crop = (slice(None), slice(None))
+        cropped = dsm.shape
     else:
-        row, col, nr, nc = output_core
+        row, col, nr, nc = (int(x) for x in output_core)
         crop = (slice(row, row + nr), slice(col, col + nc))
-    if not no_write:
+        cropped = (nr, nc)
+    valid = None
+    if output_valid_mask is not None:
+        valid = np.array(output_valid_mask, dtype=bool, copy=True)
+        if valid.shape != tuple(cropped):
+            raise ValueError(f"output_valid_mask has shape {valid.shape}; the cropped output is {tuple(cropped)}")
+        valid.setflags(write=False)
+    stamp("Spatial preparation started")
+    if device is None:
+        device = _default_device(rank, world)
+    make_scene = scene_factory or engine.Scene
+    scene = make_scene(dsm, trees, dem, pixel_size, landcover=lc, wall_threshold=dsm_wall_threshold_m,
+                       device=device, keep_planes=save_svf)
+    files = {"static": {}, "days": {}}
+    writer = OutputWriter(enabled=bool(async_output and not no_write), max_inflight=output_queue_size)
+    if not no_write and rank == 0:
         static = output / "static"
         static.mkdir(parents=True, exist_ok=True)
         np.save(static / "walls.npy", scene.walls_host.astype(np.float32))
@@ -216,35 +314,22 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
                                             ("Shadow", save_shadow)) if on]
     abi = {"UTCI": "utci", "TMRT": "tmrt", "Kup": "kup", "Kdown": "kdown", "Lup": "lup",
            "Ldown": "ldown", "Shadow": "shadow"}
+    make = runner_factory or _make_runner
     runners = {}
-    copy_stream = torch.cuda.Stream(device=scene.device)
+    on_gpu = torch.device(scene.device).type == "cuda"
+    copy_stream = torch.cuda.Stream(device=scene.device) if on_gpu and not no_write else None
     stamp("Time-series simulation started")
-    pending = []
     try:
-        for day in forcing.days:
+        for day in days:
             writer.check()
             nh = len(day.values)
             if nh not in runners:
-                runners[nh] = BatchedDay(scene, float(latitude), float(longitude), float(site_altitude_m),
-                                         utc, hours=nh, outputs=tuple(abi[v] for v in variables))
+                runners[nh] = make(scene, float(latitude), float(longitude), float(site_altitude_m), utc, nh,
+                                   tuple(abi[v] for v in variables), form)
             res = runners[nh].run_day(day.values)
             if no_write:
                 continue
-            done = torch.cuda.Event()
-            host = {}
-            copy_stream.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(copy_stream):
-                for v in variables:
-                    h = torch.empty(res[abi[v]].shape, dtype=torch.float32, pin_memory=True)
-                    h.copy_(res[abi[v]], non_blocking=True)
-                    host[v] = h.numpy()
-                done.record(copy_stream)
-            # the next day's graph writes the same device buffers: wait for the copy
-            torch.cuda.current_stream().wait_event(done)
-            if output_valid_mask is not None:
-                mask = np.asarray(output_valid_mask, dtype=bool)
-            else:
-                mask = None
+            copy = _HostCopy({v: res[abi[v]] for v in variables}, copy_stream)
             folder = output / day.date
             chunks = []
             step = max(1, int(output_chunk_steps))
@@ -253,18 +338,126 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
                 sub = folder if nh <= step else folder / f"chunk_{k + 1:04d}"
                 meta = {"timestamps": [t.isoformat() for t in day.timestamps[start:stop]],
                         "utc_offset_hours": utc}
-                view = {v: host[v][start:stop] for v in variables}
-                if mask is not None:
-                    for v in variables:
-                        view[v] = np.where(mask[None], view[v], np.nan)
+                view = {v: copy.host[v][start:stop] for v in variables}
                 writer.submit(lambda sub=sub, view=view, n=stop - start, meta=meta:
-                              _write_chunk(sub, variables, view, n, done, crop, meta))
+                              _write_chunk(sub, variables, view, n, copy, crop, meta, valid))
                 chunks.append(str(sub))
             files["days"][day.date] = {v: [str(Path(c) / f"{v}.npy") for c in chunks] for v in variables}
-            pending.append(done)
             stamp(f"Daily calculation completed: {day.date}")
         writer.finish()
-        torch.cuda.synchronize()
+        if on_gpu:
+            torch.cuda.synchronize(scene.device)
+        return files
+    except BaseException:
+        writer.abort()
+        raise
+
+
+def run_tiles(tiles, met_file, output_path, longitude, latitude, *, utc_offset_hours=None,
+              site_altitude_m=3., dsm_wall_threshold_m=3., save_tmrt=True, save_kup=False,
+              save_kdown=False, save_lup=False, save_ldown=False, save_shadow=False, dtype=np.float32,
+              no_write=False, output_chunk_steps=24, async_output=True, output_queue_size=2,
+              progress=False, pixel_size=1.0, device=None, rank=None, world_size=None,
+              group_pixels=48_000_000):
+    """Every tile of a tiled case, day by day, with all tiles of a group in ONE
+    captured graph per day (:class:`batched.TileBatch`); the reference runs
+    ``run_timeseries`` once per tile (``run.py:62-68``, ``:113-129``).
+
+    ``tiles``: sequence of dicts with ``tile_id``, ``dsm``, ``trees``, ``dem``,
+    optional ``landcover`` (2-D arrays of the tile's input window) and
+    ``output_core`` (row, col, rows, cols of the core inside the window).
+    Tiles are grouped so that a group holds at most ``group_pixels`` pixels;
+    each group's scenes stay on the device while its days run.  With several
+    ranks each takes a contiguous share of the tiles.  Outputs go to
+    ``output_path/<tile_id>/<date>/<VAR>.npy`` (cropped to the core) and
+    ``output_path/<tile_id>/static``.  Days longer than 64 rows run tile by
+    tile in the per-hour graph form.
+
+    Returns ``{tile_id: {"static": {...}, "days": {date: {variable: [paths]}}}}``.
+    """
+    from .batched import TileBatch
+    if np.dtype(dtype) != np.float32:
+        raise NotImplementedError("only dtype=float32 is supported: the float64 radiation switch of "
+                                  "the reference is not provided by this engine")
+    rank, world = rank_and_world(rank, world_size)
+    forcing = load_meteorology(met_file)
+    mine = shard.split(list(tiles), rank, world)
+    output = Path(output_path).resolve()
+    utc = float(longitude) / 15.0 if utc_offset_hours is None else float(utc_offset_hours)
+    stamp = lambda msg: print(f"[{datetime.now():%H:%M:%S}] {msg}", flush=True) if progress else None  # noqa: E731
+    if device is None:
+        device = _default_device(rank, world)
+    variables = ["UTCI"] + [n for n, on in (("TMRT", save_tmrt), ("Kup", save_kup), ("Kdown", save_kdown),
+                                            ("Lup", save_lup), ("Ldown", save_ldown),
+                                            ("Shadow", save_shadow)) if on]
+    abi = {"UTCI": "utci", "TMRT": "tmrt", "Kup": "kup", "Kdown": "kdown", "Lup": "lup",
+           "Ldown": "ldown", "Shadow": "shadow"}
+    outs = tuple(abi[v] for v in variables)
+    groups, cur, size = [], [], 0
+    for t in mine:
+        px = int(np.prod(np.shape(t["dsm"])))
+        if cur and size + px > group_pixels:
+            groups.append(cur)
+            cur, size = [], 0
+        cur.append(t)
+        size += px
+    if cur:
+        groups.append(cur)
+    files = {}
+    writer = OutputWriter(enabled=bool(async_output and not no_write), max_inflight=output_queue_size)
+    copy_stream = None if no_write else torch.cuda.Stream(device=torch.device(device))
+    try:
+        for group in groups:
+            scenes = []
+            for t in group:
+                stamp(f"Tile {t['tile_id']}: spatial preparation")
+                sc = engine.Scene(t["dsm"], t["trees"], t["dem"], pixel_size, landcover=t.get("landcover"),
+                                  wall_threshold=dsm_wall_threshold_m, device=device)
+                scenes.append(sc)
+                rec = files.setdefault(t["tile_id"], {"static": {}, "days": {}})
+                if not no_write:
+                    static = output / t["tile_id"] / "static"
+                    static.mkdir(parents=True, exist_ok=True)
+                    np.save(static / "walls.npy", sc.walls_host.astype(np.float32))
+                    np.save(static / "aspect.npy", sc.aspect_host.astype(np.float32))
+                    rec["static"] = {"walls": str(static / "walls.npy"), "aspect": str(static / "aspect.npy")}
+            batches = {}
+            for day in forcing.days:
+                writer.check()
+                nh = len(day.values)
+                if nh <= 64:
+                    if nh not in batches:
+                        batches[nh] = TileBatch(scenes, [float(latitude)] * len(scenes),
+                                                [float(longitude)] * len(scenes), float(site_altitude_m), utc,
+                                                hours=nh, outputs=outs)
+                    results = batches[nh].run([day.values] * len(scenes))
+                else:
+                    results = [BatchedDay(sc, float(latitude), float(longitude), float(site_altitude_m), utc,
+                                          hours=nh, outputs=outs).run_day(day.values) for sc in scenes]
+                if no_write:
+                    continue
+                for t, res in zip(group, results):
+                    copy = _HostCopy({v: res[abi[v]] for v in variables}, copy_stream)
+                    row, col, nr, nc = (int(x) for x in t["output_core"])
+                    crop = (slice(row, row + nr), slice(col, col + nc))
+                    folder = output / t["tile_id"] / day.date
+                    chunks = []
+                    step = max(1, int(output_chunk_steps))
+                    for k, start in enumerate(range(0, nh, step)):
+                        stop = min(nh, start + step)
+                        sub = folder if nh <= step else folder / f"chunk_{k + 1:04d}"
+                        meta = {"timestamps": [s.isoformat() for s in day.timestamps[start:stop]],
+                                "utc_offset_hours": utc}
+                        view = {v: copy.host[v][start:stop] for v in variables}
+                        writer.submit(lambda sub=sub, view=view, n=stop - start, meta=meta, crop=crop, copy=copy:
+                                      _write_chunk(sub, variables, view, n, copy, crop, meta))
+                        chunks.append(str(sub))
+                    files[t["tile_id"]]["days"][day.date] = {v: [str(Path(c) / f"{v}.npy") for c in chunks]
+                                                             for v in variables}
+                stamp(f"Daily calculation completed: {day.date} ({len(group)} tiles)")
+            torch.cuda.synchronize(torch.device(device))
+            del batches, scenes
+        writer.finish()
         return files
     except BaseException:
         writer.abort()

@@ -54,7 +54,8 @@ def make_scene(rows, cols=None, seed=0, pixel_size=1.0, building_cover=0.30, tre
     roof = np.zeros((rows, cols), dtype=bool)
     m_to_px = 1.0 / pixel_size
     attempts = 0
-    while roof.sum() < building_cover * area and attempts < 100000:
+    covered = 0  # roof.sum(), kept incrementally
+    while covered < building_cover * area and attempts < 100000:
         attempts += 1
         h = max(1, int(round(rng.uniform(8, 30) * m_to_px)))
         w = max(1, int(round(rng.uniform(8, 30) * m_to_px)))
@@ -65,11 +66,14 @@ def make_scene(rows, cols=None, seed=0, pixel_size=1.0, building_cover=0.30, tre
         height = np.float32(rng.uniform(5, 40))
         block = dsm[r0:r0 + h, c0:c0 + w]
         np.maximum(block, height, out=block)
-        roof[r0:r0 + h, c0:c0 + w] = True
+        footprint = roof[r0:r0 + h, c0:c0 + w]
+        covered += int(footprint.size - np.count_nonzero(footprint))
+        footprint[...] = True
     trees = np.zeros((rows, cols), dtype=np.float32)
     crown = np.zeros((rows, cols), dtype=bool)
     attempts = 0
-    while crown.sum() < tree_cover * area and attempts < 200000:
+    crowned = 0  # crown.sum(), kept incrementally
+    while crowned < tree_cover * area and attempts < 200000:
         attempts += 1
         rc = int(rng.integers(0, rows))
         cc = int(rng.integers(0, cols))
@@ -87,7 +91,10 @@ def make_scene(rows, cols=None, seed=0, pixel_size=1.0, building_cover=0.30, tre
         value = (height * np.exp(-d2 / (2 * sigma * sigma))).astype(np.float32)
         patch = trees[r0:r1, c0:c1]
         np.copyto(patch, np.maximum(patch, value), where=inside)
-        crown[r0:r1, c0:c1] |= inside & (value > 0)
+        cells = crown[r0:r1, c0:c1]
+        grown = inside & (value > 0) & ~cells
+        crowned += int(np.count_nonzero(grown))
+        cells |= grown
     dem = np.zeros((rows, cols), dtype=np.float32)
     landcover = np.ones((rows, cols), dtype=np.float32)
     landcover[trees > 0] = 5

@@ -158,3 +158,27 @@ def test_oracle_gvf_matches_umep_live(umep):
                      0.9, alb, 5.67051e-8, 0.2, 18.0, lc, 1)
     for x, y in zip(ref, mine):
         assert np.array_equal(np.asarray(x, float), np.asarray(y, float))
+
+
+def test_oracle_c1_day_matches_umep_200():
+    """The oracle at the CPU-baseline configuration (200 x 200 px, seed 0,
+    53 N, DOY 172), with its own walls, aspect and 153-patch SVF, against UMEP's
+    Solweig_2022a_calc fed by the reference's compiled wall and SVF kernels
+    (day200.npz, float32-rounded): Tmrt within 1e-4 K, the shadow plane
+    exact to float32, UTCI within the 2e-3 K of the float32 reference UTCI."""
+    from oracle import step as ST
+    from solweig_cuda_b200 import synthetic
+    g = gold("day200.npz")
+    sc = synthetic.make_scene(200, seed=0)
+    s = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    hours = [int(h) for h in g["hours"]]
+    res = ST.run_day(s, g["met"], dict(latitude=53.0, longitude=0.0, altitude=3.0), 0.0,
+                     outputs=("Tmrt", "UTCI", "shadow"))
+    for j, h in enumerate(hours):
+        assert np.max(np.abs(res[h]["Tmrt"] - g["Tmrt"][j])) < 1e-4, h
+        sh = np.broadcast_to(res[h]["shadow"], (200, 200)).astype(np.float32)
+        assert np.array_equal(sh, g["shadow"][j]), h
+        want = g["UTCI"][j]
+        assert np.array_equal(np.isnan(res[h]["UTCI"]), np.isnan(want)), h
+        ok = ~np.isnan(want)
+        assert np.max(np.abs(res[h]["UTCI"][ok] - want[ok])) < 2e-3, h

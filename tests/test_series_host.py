@@ -61,3 +61,84 @@ def test_bad_forcing_and_raster_shapes_are_rejected():
     from solweig_cuda_b200 import engine
     with pytest.raises((ValueError, RuntimeError)):
         engine.Scene(np.zeros((10, 10)), np.zeros((10, 11)), np.zeros((10, 10)))
+
+
+class StubScene:
+    """Host stand-in for engine.Scene: the driver only needs the static planes."""
+
+    def __init__(self, dsm, trees, dem, pixel_size=1.0, landcover=None, wall_threshold=3.0, device="cpu",
+                 keep_planes=False):
+        self.shape = np.shape(dsm)
+        self.device = "cpu"
+        self.walls_host = np.zeros(self.shape)
+        self.aspect_host = np.zeros(self.shape)
+
+
+class StubRunner:
+    """Day runner whose planes depend on the day's forcing and the pixel, so
+    every (day, hour, pixel, variable) value is distinct."""
+
+    def __init__(self, scene, latitude, longitude, site_altitude, utc, hours, outputs, form):
+        import torch
+        self.outputs = outputs
+        r, c = scene.shape
+        self.pix = torch.arange(r * c, dtype=torch.float32).reshape(r, c)
+        self.buf = {k: torch.empty((hours, r, c)) for k in outputs}
+
+    def run_day(self, values):
+        import torch
+        for j, k in enumerate(self.outputs):
+            for h, row in enumerate(values):
+                self.buf[k][h] = float(row[1]) * 1000 + float(row[2]) * 10 + j + self.pix / 1e4
+        return self.buf
+
+
+def _forcing(days=4):
+    from solweig_cuda_b200 import synthetic
+    return synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, days=days)
+
+
+def run_stub(tmp, **kw):
+    from solweig_cuda_b200 import series
+    z = np.zeros((12, 10))
+    return series.run_timeseries(z, z, z, _forcing(kw.pop("days", 4)), tmp, 0.0, 53.0, scene_factory=StubScene,
+                                 runner_factory=StubRunner, device="cpu", **kw)
+
+
+def test_run_timeseries_masks_cropped_outputs_after_the_copy(tmp_path):
+    """output_valid_mask applies to the cropped output core, after the
+    device-to-host copy (src/output.py:205-216): masked files equal the
+    unmasked run with NaN outside the mask."""
+    core = (2, 3, 7, 5)
+    mask = np.ones((7, 5), dtype=bool)
+    mask[1:3, 2:4] = False
+    a = run_stub(tmp_path / "plain", output_core=core, save_kup=True)
+    b = run_stub(tmp_path / "masked", output_core=core, save_kup=True, output_valid_mask=mask)
+    assert a["days"].keys() == b["days"].keys() and len(a["days"]) == 4
+    for date, rec in a["days"].items():
+        for var, paths in rec.items():
+            x = np.load(paths[0])
+            y = np.load(b["days"][date][var][0])
+            assert x.shape == (24, 7, 5)
+            assert not np.isnan(x).any()
+            want = np.where(mask[None], x, np.nan)
+            assert np.array_equal(np.isnan(y), np.isnan(want))
+            assert np.array_equal(y[:, mask], x[:, mask])
+
+
+def test_run_timeseries_rejects_bad_mask_and_float64(tmp_path):
+    with pytest.raises(ValueError, match="cropped output"):
+        run_stub(tmp_path / "a", output_core=(0, 0, 4, 4), output_valid_mask=np.ones((12, 10), bool))
+    with pytest.raises(NotImplementedError, match="float64"):
+        run_stub(tmp_path / "b", dtype=np.float64)
+
+
+def test_run_timeseries_rank_shares_cover_all_days(tmp_path):
+    whole = run_stub(tmp_path / "one", days=5)
+    parts = [run_stub(tmp_path / "two", days=5, rank=r, world_size=2) for r in range(2)]
+    assert parts[0]["static"] and not parts[1]["static"]
+    got = {**parts[0]["days"], **parts[1]["days"]}
+    assert sorted(got) == sorted(whole["days"]) and not set(parts[0]["days"]) & set(parts[1]["days"])
+    for date, rec in whole["days"].items():
+        for var, paths in rec.items():
+            assert np.array_equal(np.load(paths[0]), np.load(got[date][var][0]))
