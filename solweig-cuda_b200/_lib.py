@@ -99,14 +99,14 @@ class SolweigDayConfig(ctypes.Structure):
     _fields_ = [("shadow_bx", ctypes.c_int32), ("shadow_by", ctypes.c_int32),
                 ("gvf_rows", ctypes.c_int32), ("rad_threads", ctypes.c_int32),
                 ("gemm_ctas_per_sm", ctypes.c_int32), ("gvf_hours", ctypes.c_int32),
-                ("no_ceiling", ctypes.c_int32)]
+                ("no_ceiling", ctypes.c_int32), ("sweep_window", ctypes.c_int32)]
 
     def astuple(self):
         return tuple(getattr(self, f) for f, _ in self._fields_)
 
     @classmethod
     def default(cls):
-        return cls(32, 8, 8, 256, 0, 1, 0)
+        return cls(32, 8, 8, 256, 0, 2, 0, 1)
 
 
 EXPORTED_SYMBOLS = (

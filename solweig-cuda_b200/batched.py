@@ -295,16 +295,27 @@ class ChosenDay(BatchedDay):
         self.buffers.mark()
         return dict(zip(self.STAGES, (float(x) for x in ms)))
 
-    WORK_FIELDS = ("quads", "lup_first", "gvf", "nosh", "sums", "wf32", "bw", "tables", "error", "total")
+    WORK_FIELDS = ("quads", "lup_first", "gvf", "nosh", "sums", "wf32", "bw", "tables", "error", "bounds",
+                   "total")
 
     def work_offsets(self):
         """{field: byte offset} of the work buffer (``solweig_day_batched_layout``)."""
         sc = self.scene
-        off = (ctypes.c_int64 * 10)()
+        off = (ctypes.c_int64 * 11)()
         _lib.check(_lib.lib().solweig_day_batched_layout(sc.rows, sc.cols, self.hours,
                                                          int(sc.struct.has_water), off),
                    "solweig_day_batched_layout")
         return dict(zip(self.WORK_FIELDS, (int(x) for x in off)))
+
+    def quads(self):
+        """The sweep's per-pixel GVF inputs of the last day as a [H, rows, cols, 4]
+        float32 view: shadow, Lup excess, albedo and the ground (1) / sunlit-wall
+        (2) bits as an int32 bit pattern (daytime hours only; night hours hold
+        stale values)."""
+        o = self.work_offsets()
+        n = 16 * self.hours * self.scene.pixels
+        return self.work[o["quads"]:o["quads"] + n].view(torch.float32).view(self.hours, self.scene.rows,
+                                                                                 self.scene.cols, 4)
 
     def quads(self):
         """The sweep's per-pixel GVF inputs of the last day as a [H, rows, cols, 4]

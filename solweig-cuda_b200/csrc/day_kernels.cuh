@@ -8,6 +8,7 @@
 #include "gvf_fields.cuh"
 #include "hour.cuh"
 #include "radiation.cuh"
+#include "sweep_tma.cuh"
 #include "tcgen05.cuh"
 
 namespace solweig {
@@ -179,17 +180,21 @@ __global__ void __launch_bounds__(256, 8) day_shadow_kernel(SolweigScene S,
                                                                    float4* __restrict__ quads,
                                                                    float* __restrict__ lup_first,
                                                                    const float* __restrict__ ceiling,
-                                                                   const int* __restrict__ exits) {
+                                                                   const int* __restrict__ exits,
+                                                                   uint32_t* __restrict__ bounds, int nhours, int h0) {
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
     int r, c;
     warp_tile_pixel(blockDim.x, blockDim.y, r, c);
-    if (r >= S.rows || c >= S.cols) return;
+    const bool in = r < S.rows && c < S.cols;
     const long long n = (long long)S.rows * S.cols;
-    shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
-                      ceiling ? ceiling + z * n : nullptr,
-                      exits ? exits + (long long)z * (S.rows + S.cols) : nullptr);
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (in)
+        q = shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
+                              ceiling ? ceiling + z * n : nullptr,
+                              exits ? exits + (long long)z * (S.rows + S.cols) : nullptr);
+    if (bounds) gvf_bounds_reduce(in && (__float_as_int(q.w) & kQuadGround), q.y, q.z * q.x, bounds, nhours, h0 + z);
 }
 
 // Per daytime hour, the first-outside step of every row and column of the
@@ -549,6 +554,277 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                 gvf[(3LL * h) * n + p] = (float)((double)(lt / 18.f) + ambient);
                 gvf[(3LL * h + 1) * n + p] = at / 18.f;
                 gvf[(3LL * h + 2) * n + p] = quads[(long long)h * n + p].x;
+            }
+        }
+    }
+}
+
+// Hour-vectorized GVF with 8 daytime hours per shared-memory pass, the hour
+// values as 16-bit fixed point.  Per cell and hour one 32-bit word holds
+// (Lup - Lmin_h) * sL_h in its high half and albedo*shadow * sA_h in its low
+// half, both rounded to integers in [0, kGvfQMax]; the walk sums the words
+// with plain integer adds: 22 * kGvfQMax < 2^16, so the low half never
+// carries into the high one.  Lmin_h / Lmax_h and the largest
+// albedo*shadow of each hour come from the sweep (over ground pixels, the
+// only ones a walk sums), so the scales follow each hour's range:
+// quantisation error <= range / (2 kGvfQMax) per sample (~0.034 W/m2 for a
+// 200 W/m2 Lup range).  Per sample two 16-byte shared loads and 8 integer
+// adds serve 8 hours (the float kernel above: the same loads and 8 float
+// adds for 4 hours), and a 16-hour day takes 2 passes instead of 4.
+//
+// The own pixel is step 0 of every direction, so the first-ring terms
+// (lup1, alb1: FIRST = 1) are the same in all 18 directions and use the
+// pixel's exact float values; the second-ring sums are the dequantised
+// word sums.  Walk lengths, sunlit-wall first steps, the frozen tails of
+// border tiles and the albedo-without-shadow plane follow day_gvf_hv_kernel.
+constexpr int kHv8 = 8;
+constexpr uint32_t kGvfQMax = 2978;
+static_assert(22u * kGvfQMax < 65536u, "a 22-step sum of the low half must not carry");
+
+__global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv8_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
+                                                                   int nhours, GvfTable<22> tab,
+                                                                   const float4* __restrict__ quads,
+                                                                   const uint32_t* __restrict__ bounds,
+                                                                   float* __restrict__ gvf, float* __restrict__ nosh) {
+    constexpr int FIRST = 1, SECOND = 22;
+    static_assert(FIRST == 1, "the first ring is the own pixel only");
+    const int tr = blockIdx.y, tc = blockIdx.x;
+    const bool interior = hv_tile_interior(S.rows, S.cols, tr, tc);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4* PA = reinterpret_cast<uint4*>(smem_raw);  // packed words of pass hours 0..3
+    uint4* PB = PA + kHvN;                          // pass hours 4..7
+    uint32_t* bits = reinterpret_cast<uint32_t*>(PB + kHvN);  // bit0 ground, bits 1..8 sunlit wall
+    float* albs = reinterpret_cast<float*>(bits + kHvN);      // albedo, then the walk lengths
+    int* dayh = reinterpret_cast<int*>(albs + kHvN);          // daytime hour indices
+    __shared__ int nday;
+    __shared__ float qs[4][kHv8];  // per pass hour: Lmin, 1/sL, 1/sA, wall Lup
+    const int tid = threadIdx.y * kHvTile + threadIdx.x;
+    const long long n = (long long)S.rows * S.cols;
+    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
+    if (tid == 0) {
+        int k = 0;
+        for (int h = 0; h < nhours && k < 64; ++h)
+            if (hours[h].daytime) dayh[k++] = h;
+        nday = k;
+    }
+    __syncthreads();
+    const int nd = nday;
+    if (nd == 0) return;
+    {
+        const float4* q0 = quads + (long long)dayh[0] * n;
+        for (int i = tid; i < kHvN; i += kHvThreads) {
+            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
+            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
+            const float4 q = in ? q0[(long long)rr * S.cols + cc] : make_float4(0.f, 0.f, 0.f, 0.f);
+            bits[i] = (uint32_t)__float_as_int(q.w) & kQuadGround;
+            albs[i] = q.z;
+        }
+    }
+    __syncthreads();
+    const int lw_ = tid >> 5, ll = tid & 31;
+    const int tx = (lw_ & 3) * 8 + (ll & 7), ty = (lw_ >> 2) * 4 + (ll >> 3);
+    const int r = tr * kHvTile + ty, c = tc * kHvTile + tx;
+    const bool valid = r < S.rows && c < S.cols;
+    const long long p = valid ? (long long)r * S.cols + c : 0;
+    const int own = (ty + kHvHalo) * kHvPitch + tx + kHvHalo;
+    const bool own_ground = valid && (bits[own] & 1u) != 0;
+    const float ob = own_ground ? 1.f : 0.f;
+    const uint32_t face = valid ? S.gvf_face[p] : 0u;
+    constexpr float albedo_b = 0.2f;
+    constexpr float inv_first = 1.f / FIRST, inv_first1 = 1.f / (FIRST + 1);
+    constexpr float inv_second = 1.f / SECOND, inv_second1 = 1.f / (SECOND + 1);
+    uint32_t hits[4] = {0u, 0u, 0u, 0u};
+    float nsh = 0.f;
+    for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
+        int hit = 0, lim = 0;
+        float s_alb = 0.f, n_alb = 0.f;
+        if (own_ground) {
+            hit = lim = SECOND;
+            for (int m = 0; m < SECOND; ++m) {
+                if (!interior) {
+                    const int2 o = tab.offs[j * SECOND + m];
+                    if (!in_raster(r + o.x, c + o.y, S.rows, S.cols)) {
+                        if (m == 0) {
+                            hit = lim = 0;
+                        } else {  // frozen tail: step m and the rest repeat step m - 1
+                            lim = m;
+                            const float al = albs[own + tab.delta[j * SECOND + m - 1]];
+                            s_alb += al;
+                            s_alb += (SECOND - 1 - m) * al;
+                        }
+                        break;
+                    }
+                }
+                const int off = own + tab.delta[j * SECOND + m];
+                if (!(bits[off] & 1u)) {
+                    hit = lim = m;
+                    break;
+                }
+                s_alb += albs[off];
+                if (m + 1 == FIRST) n_alb = s_alb;
+            }
+        }
+        hits[j / 5] |= ((uint32_t)lim | (hit > lim ? 32u : 0u)) << (6 * (j % 5));
+        const int n_wall = SECOND - hit;
+        const int n_wall_first = FIRST > hit ? FIRST - hit : 0;
+        const float nosh1 = n_wall_first > 0 ? ((float)n_wall_first * albedo_b + n_alb) * inv_first1 : n_alb * inv_first;
+        const float nosh2 = n_wall > 0 ? ((float)n_wall * albedo_b + s_alb) * inv_second : s_alb * inv_second;
+        nsh += (nosh1 * 0.5f + nosh2 * 0.4f) * (1.f / 0.9f);
+    }
+    nsh *= ob;
+    nsh += 18.f * (albs[own] * (1.f - ob));
+    if (valid) nosh[p] = nsh / 18.f;
+    // the albedo array is not read again: it holds each thread's walk lengths
+    // from here on (4 words per thread), which frees their registers
+    __syncthreads();
+    uint32_t* hits_sm = reinterpret_cast<uint32_t*>(albs) + 4 * tid;
+    static_assert(4 * kHvThreads <= kHvN, "walk lengths must fit in the albedo array");
+#pragma unroll
+    for (int i = 0; i < 4; ++i) hits_sm[i] = hits[i];
+
+    for (int g0 = 0; g0 < nd; g0 += kHv8) {
+        const int nc = nd - g0 < kHv8 ? nd - g0 : kHv8;
+        __syncthreads();  // the previous pass no longer reads the tile or qs
+        if (tid < kHv8) {
+            float lmin = 0.f, il = 0.f, ia = 0.f, lw = 0.f;
+            if (tid < nc) {
+                const int h = dayh[g0 + tid];
+                if (bounds[nhours + h] != 0u) {  // the hour has ground pixels
+                    const float lo = ord2f(bounds[h]), hi = ord2f(bounds[nhours + h]);
+                    const float am = ord2f(bounds[2 * nhours + h]);
+                    lmin = lo;
+                    il = hi > lo ? (hi - lo) / (float)kGvfQMax : 0.f;
+                    ia = am > 0.f ? am / (float)kGvfQMax : 0.f;
+                }
+                const SolweigHour& hh = hours[h];
+                lw = (float)(kSBC * 0.9 * pow4(hh.tgwall + hh.ta + 273.15) - kSBC * 0.9 * pow4(hh.ta + 273.15));
+            }
+            qs[0][tid] = lmin;
+            qs[1][tid] = il;
+            qs[2][tid] = ia;
+            qs[3][tid] = lw;
+        }
+        __syncthreads();
+        for (int i = tid; i < kHvN; i += kHvThreads) {
+            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
+            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
+            const long long pix = in ? (long long)rr * S.cols + cc : 0;
+            uint32_t b = bits[i] & 1u;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {  // 4 hours at a time: fewer live registers
+                uint32_t wv[4];
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int k = 4 * half + kk;
+                    wv[kk] = 0u;
+                    if (k < nc && in) {
+                        const float4 q = quads[(long long)dayh[g0 + k] * n + pix];
+                        const float sl = qs[1][k] > 0.f ? 1.f / qs[1][k] : 0.f;
+                        const float sa = qs[2][k] > 0.f ? 1.f / qs[2][k] : 0.f;
+                        const float lq = fminf(fmaxf(rintf((q.y - qs[0][k]) * sl), 0.f), (float)kGvfQMax);
+                        const float aq = fminf(fmaxf(rintf(q.z * q.x * sa), 0.f), (float)kGvfQMax);
+                        wv[kk] = ((uint32_t)lq << 16) | (uint32_t)aq;
+                        b |= (((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u) << (1 + k);
+                    }
+                }
+                (half ? PB : PA)[i] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            }
+            bits[i] = b;
+        }
+        __syncthreads();
+        float lup_t[kHv8], alb_t[kHv8];
+#pragma unroll
+        for (int k = 0; k < kHv8; ++k) lup_t[k] = alb_t[k] = 0.f;
+        if (own_ground) {
+#pragma unroll 1
+            for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
+                const uint32_t code = (hits_sm[j / 5] >> (6 * (j % 5))) & 63u;
+                const int lim = (int)(code & 31u);
+                const int hit = (code & 32u) ? SECOND : lim;
+                uint32_t acc[kHv8];
+#pragma unroll
+                for (int k = 0; k < kHv8; ++k) acc[k] = 0u;
+                uint32_t seen = 0u;
+#pragma unroll
+                for (int m = 0; m < SECOND; ++m) {
+                    if (m < lim) {
+                        const int off = own + tab.delta[j * SECOND + m];
+                        const uint4 A = PA[off], B = PB[off];
+                        seen |= bits[off];
+                        acc[0] += A.x; acc[1] += A.y; acc[2] += A.z; acc[3] += A.w;
+                        acc[4] += B.x; acc[5] += B.y; acc[6] += B.z; acc[7] += B.w;
+                    }
+                }
+                // first step of each hour's sunlit-wall bit (5 bits per hour, 31 =
+                // never); sunlit walls are rare, so they are located by a second,
+                // short scan only when the walk met one
+                unsigned long long first_pk = ~0ull;
+                seen = (seen >> 1) & 0xFFu;
+                if (seen) {
+                    uint32_t pending = seen;
+                    for (int m = 0; m < lim && pending; ++m) {
+                        const uint32_t nb = (bits[own + tab.delta[j * SECOND + m]] >> 1) & pending;
+                        for (uint32_t t = nb; t; t &= t - 1) {
+                            const int k = __ffs(t) - 1;
+                            first_pk = (first_pk & ~(31ull << (5 * k))) | ((unsigned long long)m << (5 * k));
+                        }
+                        pending &= ~nb;
+                    }
+                }
+                // frozen tail (border tiles): step lim and the rest repeat step lim - 1
+                const float rest = (float)(SECOND - lim);
+                const uint32_t* lastw = nullptr;
+                if (hit > lim) lastw = reinterpret_cast<const uint32_t*>(&PA[own + tab.delta[j * SECOND + lim - 1]]);
+                const bool fj = (face >> j) & 1u;
+#pragma unroll
+                for (int k = 0; k < kHv8; ++k) {
+                    float sl = (float)(acc[k] >> 16) * qs[1][k] + (float)lim * qs[0][k];
+                    float sa = (float)(acc[k] & 0xFFFFu) * qs[2][k];
+                    if (lastw != nullptr) {
+                        // PB[last] lies kHvN uint4 (4 kHvN words) past PA[last]
+                        const uint32_t wk = k < 4 ? lastw[k] : lastw[4 * kHvN + (k - 4)];
+                        sl = fmaf(rest, (float)(wk >> 16) * qs[1][k] + qs[0][k], sl);
+                        sa = fmaf(rest, (float)(wk & 0xFFFFu) * qs[2][k], sa);
+                    }
+                    const int f = (int)((first_pk >> (5 * k)) & 31ull);
+                    const int n_sun = f < hit ? SECOND - f : 0;
+                    const float s_wall = (float)n_sun;
+                    float s_lwall = s_wall * qs[3][k], s_albwall = s_wall * albedo_b;
+                    if (n_sun == SECOND && fj) {
+                        s_lwall = 0.f;
+                        s_albwall = 0.f;
+                    }
+                    const bool sun_far = n_sun > 0;
+                    const float lup2 = sun_far ? (s_lwall + sl) * inv_second1 : sl * inv_second;
+                    const float alb2 = sun_far ? (s_albwall + sa) * inv_second1 : sa * inv_second;
+                    lup_t[k] += lup2 * (0.4f / 0.9f);
+                    alb_t[k] += alb2 * (0.4f / 0.9f);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kHv8; ++k) {
+            if (k < nc && valid) {
+                const int h = dayh[g0 + k];
+                const SolweigHour& hh = hours[h];
+                const float4 oq = quads[(long long)h * n + p];
+                const float own_lup = oq.y, own_albsh = oq.z * oq.x;
+                // first ring (the own pixel, step 0 of all 18 directions): a sunlit
+                // wall is seen there iff the own pixel carries the bit
+                const bool own_sun = ((uint32_t)__float_as_int(oq.w) & kQuadSunwall) != 0;
+                float lt = lup_t[k], at = alb_t[k];
+                if (own_ground) {
+                    const float lup1 = own_sun ? (qs[3][k] + own_lup) * inv_first1 : own_lup * inv_first;
+                    const float alb1 = own_sun ? (albedo_b + own_albsh) * inv_first1 : own_albsh * inv_first;
+                    lt += 18.f * (lup1 * (0.5f / 0.9f));
+                    at += 18.f * (alb1 * (0.5f / 0.9f));
+                }
+                lt += 18.f * (own_lup * (1.f - ob));
+                at += 18.f * (own_albsh * (1.f - ob));
+                const double ambient = kSBC * (double)S.emis[p] * pow4(hh.ta + 273.15);
+                gvf[(3LL * h) * n + p] = (float)((double)(lt / 18.f) + ambient);
+                gvf[(3LL * h + 1) * n + p] = at / 18.f;
+                gvf[(3LL * h + 2) * n + p] = oq.x;
             }
         }
     }
@@ -1031,7 +1307,7 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
 inline long long align256(long long x) { return (x + 255) & ~255LL; }
 
 struct DayWork {
-    long long quads, lup_first, gvf, nosh, sums, wf32, bw, tables, error, total;
+    long long quads, lup_first, gvf, nosh, sums, wf32, bw, tables, error, bounds, total;
 };
 
 DayWork day_work_layout(long long px, int nhours, bool water) {
@@ -1048,6 +1324,7 @@ DayWork day_work_layout(long long px, int nhours, bool water) {
     w.bw = o; o = align256(o + 2LL * 2 * nb * kK);
     w.tables = o; o = align256(o + (long long)sizeof(DayTable) * nhours);
     w.error = o; o = align256(o + 16);
+    w.bounds = o; o = align256(o + 4LL * 3 * nhours);
     w.total = o;
     return w;
 }

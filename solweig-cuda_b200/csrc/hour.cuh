@@ -22,11 +22,11 @@ __device__ __forceinline__ double lup_excess(double emis, double tg, double shad
 }
 
 // Shadow sweep of pixel (r, c) for hour h and the per-pixel GVF inputs: the
-// float4 quad (shadow, Lup, albedo, ground|sunwall bits) and, for scenes with
-// water, the Lup of the first GVF search direction.
+// float4 quad (shadow, Lup, albedo, ground|sunwall bits; also returned) and,
+// for scenes with water, the Lup of the first GVF search direction.
 // `exits` (optional): the hour's first-outside step of every row and column
 // (first_outside); with the packed geometry the walk then needs no bounds checks.
-__device__ __forceinline__ void shadow_quad_pixel(const SolweigScene& S, const SolweigHour& h, int r, int c,
+__device__ __forceinline__ float4 shadow_quad_pixel(const SolweigScene& S, const SolweigHour& h, int r, int c,
                                                   float4* __restrict__ quad, float* __restrict__ lup_first,
                                                   const float* __restrict__ ceiling = nullptr,
                                                   const int* __restrict__ exits = nullptr) {
@@ -69,8 +69,10 @@ __device__ __forceinline__ void shadow_quad_pixel(const SolweigScene& S, const S
     if (lup_first) lup_first[p] = (float)lup_excess(emis, tg, shadow, h.ta);
     if (S.has_water && (fl & 4)) tg = h.twater - h.ta;
     const float lup = (float)lup_excess(emis, tg, shadow, h.ta);
-    quad[p] = make_float4((float)shadow, lup, S.alb[p],
-                          __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+    const float4 q = make_float4((float)shadow, lup, S.alb[p],
+                                 __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+    quad[p] = q;
+    return q;
 }
 
 }  // namespace solweig

@@ -1,0 +1,401 @@
+// The batched day's shadow sweep on shared-memory windows staged by TMA.
+//
+// A block sweeps a 16 x 16 pixel tile for one daytime hour.  All rays of the
+// hour leave the tile towards the sun, and their offsets grow monotonically,
+// so the first steps of every walk stay inside a 48 x 48 pixel window that
+// holds the tile in the corner away from the sun.  Thread 0 stages that
+// window of the packed (dsm, canopy, trunk, 0) geometry from HBM into shared
+// memory with one cp.async.bulk.tensor load (a 2-D tensor map over the
+// raster viewed as rows x (4 * cols) float32) completing on an mbarrier,
+// while the block computes the tile's per-pixel statics and the step at
+// which each tile row / column leaves the window.  A walk then takes its
+// samples from shared memory up to that step and from the raster (L1/L2)
+// after it.
+//
+// Warp-vote exit: after the stage, the block reduces the window's maximum
+// height M.  Every 4 steps the lanes of a warp vote (__all_sync) on
+// M - dz_{k-1} < dsm_p; once it holds for the whole warp, no sample left in
+// the window can change any lane's outputs and the warp jumps to the first
+// step outside the window together.
+//
+// The per-step recurrences are those of shadow_walk_packed (shadow.cuh), in
+// the same float64 operations: every output is bit-identical.  The raster
+// must carry the packed float32 geometry (SolweigScene::geo32).
+//
+// The kernel also reduces, per hour, the range of the GVF inputs over ground
+// pixels (gvf_bounds_reduce) for the fixed-point GVF of the batched day.
+#pragma once
+#include <cuda.h>
+
+#include "hour.cuh"
+
+namespace solweig {
+
+// Everything lives in an anonymous namespace: each translation unit that
+// includes this header instantiates its own copy.
+namespace {
+
+constexpr int kSwTile = 16;              // tile side (pixels)
+constexpr int kSwWin = 48;               // window side (pixels)
+constexpr int kSwThreads = kSwTile * kSwTile;
+constexpr int kSwWinBytes = kSwWin * kSwWin * 16;
+constexpr int kSwScanLimit = 4 * kSwWin;  // window exits are found by a linear scan up to here
+constexpr uint32_t kSwWaitPolls = 1u << 22;
+
+struct SweepSmem {
+    float4 win[kSwWin * kSwWin];  // 128-byte aligned at the start of dynamic shared memory
+    unsigned long long bar;
+    int row_exit[kSwTile], col_exit[kSwTile];
+    float wmax[kSwThreads / 32];
+};
+
+// Order-preserving map of floats to unsigned ints (for atomicMin / atomicMax).
+__device__ __forceinline__ uint32_t f2ord(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Per-hour ranges of the GVF inputs over ground pixels, reduced by the sweep:
+// b[h] = ordered min Lup, b[H + h] = ordered max Lup, b[2H + h] = ordered max
+// albedo*shadow (0 = no ground pixel yet).  Every thread of the block calls
+// it (valid = it has a daytime ground pixel).
+__device__ __forceinline__ void gvf_bounds_reduce(bool valid, float lup, float albsh, uint32_t* b, int H, int h) {
+    __shared__ uint32_t red[3][32];
+    uint32_t lo = valid ? f2ord(lup) : 0xffffffffu;
+    uint32_t hi = valid ? f2ord(lup) : 0u;
+    uint32_t ah = valid ? f2ord(albsh) : 0u;
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    ah = __reduce_max_sync(0xffffffffu, ah);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    const int w = tid >> 5, nw = (nt + 31) >> 5;
+    if ((tid & 31) == 0) {
+        red[0][w] = lo;
+        red[1][w] = hi;
+        red[2][w] = ah;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int i = 1; i < nw; ++i) {
+            lo = min(lo, red[0][i]);
+            hi = max(hi, red[1][i]);
+            ah = max(ah, red[2][i]);
+        }
+        if (hi != 0u) {  // the block had a ground pixel
+            atomicMin(&b[h], lo);
+            atomicMax(&b[H + h], hi);
+            atomicMax(&b[2 * H + h], ah);
+        }
+    }
+}
+
+__device__ __forceinline__ void sw_mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(bar))
+                 : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arrive on the barrier expecting `bytes` and start the 2-D tile load of the
+// box at (x, y) (elements) of `map` into `dst`.  No multicast: the window
+// comes from this GPU's own raster into this CTA's shared memory.
+__device__ __forceinline__ void sw_tma_load(void* dst, const CUtensorMap* map, int x, int y,
+                                            unsigned long long* bar, uint32_t bytes) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            (uint32_t)__cvta_generic_to_shared(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(b)
+        : "memory");
+}
+
+__device__ __forceinline__ bool sw_mbar_wait(unsigned long long* bar, uint32_t parity, uint32_t limit) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// shadow_walk_packed with the samples of steps [0, kw) read from the window
+// (`wbase` = the pixel's own index in it, `wpitch` its row pitch) and the
+// warp vote on the window maximum (`wclear`: dz_prev >= wclear means the
+// window's maximum minus dz_prev lies below the pixel).  Every lane of the
+// warp calls it (lanes without a pixel pass in = false): the window phase
+// is a warp-uniform loop so that the vote sees the whole warp.
+//
+// Samples skipped after a vote all compare below the pixel in every test of
+// the walk (building height, canopy top and trunk against dz_k and
+// dz_{k-1}), so they would change neither the shadow, the vegetation flags
+// nor a canopy top that reaches above the pixel; a canopy top left below the
+// pixel does not enter any output.
+__device__ __forceinline__ ShadowResult shadow_walk_window(
+    bool in, const float4* __restrict__ win, int wpitch, int wbase, int kw, double wclear,
+    const float4* __restrict__ geo, int cols, long long p, double a, double top_p, bool bush, double wall,
+    const int2* __restrict__ ray, const double* __restrict__ dz, int steps, int kend, double hmax,
+    const float* __restrict__ ceiling) {
+    ShadowResult s;
+    s.f = a;
+    s.topmax = top_p;
+    s.shadowed = false;
+    s.veg = bush;
+    s.ever = false;
+    const bool is_wall = wall > 0.0;
+    const bool nonneg = a >= 0.0;
+    const double pinf = __longlong_as_double(0x7ff0000000000000ll);
+    const double clear = nonneg ? nextafter(hmax - a, pinf) : pinf;
+    double dz_prev = 0.0;
+    bool final = false;
+    auto step = [&](const float4 v, double dzk) -> bool {  // true: the walk is over
+        s.f = fmax(s.f, (double)v.x - dzk);
+        s.shadowed = s.f > a;
+        if (v.y <= 0.f && v.z <= 0.f && nonneg && s.topmax >= 0.0) {
+            if (s.shadowed) s.veg = false;
+            else s.ever = s.ever || s.veg;
+        } else {
+            const double tq = v.y, bq = v.z;
+            s.topmax = fmax(s.topmax, tq - dzk);
+            if (s.shadowed) {
+                s.veg = false;
+            } else {
+                const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
+                              (int)(bq - dz_prev > a);
+                s.veg = s.veg || (n > 0 && n < 4);
+                s.ever = s.ever || s.veg;
+            }
+        }
+        return s.shadowed && (!is_wall || s.f - a >= wall);
+    };
+    // true: nothing further can change (the exits of shadow_walk_packed)
+    auto settled = [&](long long q, int k, double dzk) {
+        if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) return true;
+        if (ceiling != nullptr && k >= 4 && (k & 3) == 0) {
+            const double e = __dsub_ru((double)__ldg(&ceiling[q]), dz_prev);
+            if (nonneg && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) return true;
+        }
+        return false;
+    };
+    // phase 1: samples from the window, the warp stepping together
+    bool active = in && kw > 0;
+    int k = 0;
+    const int kwm = __reduce_max_sync(0xffffffffu, active ? kw : 0);
+    for (int kk = 0; kk < kwm; ++kk) {
+        if (kk >= 4 && (kk & 3) == 0 && __all_sync(0xffffffffu, !active || (nonneg && dz_prev >= wclear)))
+            break;  // no window sample left can reach above any lane's pixel
+        if (active) {
+            if (kk >= kw) {
+                active = false;
+            } else {
+                const int2 o = __ldg(&ray[kk]);
+                const double dzk = __ldg(&dz[kk]);
+                if (settled(p + (long long)o.x * cols + o.y, kk, dzk) || step(win[wbase + o.x * wpitch + o.y], dzk)) {
+                    final = true;
+                    active = false;
+                } else {
+                    dz_prev = dzk;
+                    k = kk + 1;
+                }
+            }
+        }
+    }
+    if (in && !final) {
+        // samples skipped by the vote all lie below the pixel: resume at the
+        // first step outside the window, with dz_prev of the step before it
+        if (k < kw) {
+            k = kw;
+            dz_prev = __ldg(&dz[k - 1]);
+        }
+        // phase 2: samples from the raster
+        for (; k < kend; ++k) {
+            const int2 o = __ldg(&ray[k]);
+            const double dzk = __ldg(&dz[k]);
+            const long long q = p + (long long)o.x * cols + o.y;
+            if (settled(q, k, dzk) || step(__ldg(&geo[q]), dzk)) {
+                final = true;
+                break;
+            }
+            dz_prev = dzk;
+        }
+        if (!final && k < steps) {
+            // First step whose sample is outside the raster: all shifted values are 0.
+            s.f = fmax(s.f, 0.0);
+            s.shadowed = s.f > a;
+            s.topmax = fmax(s.topmax, 0.0);
+            if (s.shadowed) s.veg = false;
+            s.ever = s.ever || s.veg;
+        }
+    }
+    return s;
+}
+
+// Quad epilogue of shadow_quad_pixel for a walk result (returns the quad).
+__device__ __forceinline__ float4 write_quad(const SolweigScene& S, const SolweigHour& h, long long p, double a,
+                                             double wall, uint8_t fl, const ShadowResult& s,
+                                             float4* __restrict__ quad) {
+    const double wallbol = wall > 0.0 ? 1.0 : 0.0;
+    const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);
+    double wallsun = wall - (s.f - a);
+    if (wallsun < 0.0) wallsun = 0.0;
+    if (facesh == 1.0) wallsun = 0.0;
+    const double wallsh = wall - wallsun;
+    double wallshve = (s.topmax - a) * (s.veg ? 1.0 : 0.0) * wallbol - wallsh;
+    if (wallshve < 0.0) wallshve = 0.0;
+    if (wallshve > wall) wallshve = wall;
+    wallsun = wallsun - wallshve;
+    if (wallsun < 0.0) wallsun = 0.0;
+    const double ground = (fl & 1) ? 1.0 : 0.0;
+    const bool sunwall = (wallsun / wall * ground) == 1.0;
+    const double sh = s.shadowed ? 0.0 : 1.0;
+    const double vegsh = s.veg ? 0.0 : 1.0;
+    const double shadow = (double)(float)(sh - (1.0 - vegsh) * (1.0 - h.psi));
+    const double tg = ground_tg(S, h, p);
+    const float lup = (float)lup_excess((double)S.emis[p], tg, shadow, h.ta);
+    const float4 q = make_float4((float)shadow, lup, S.alb[p],
+                                 __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+    quad[p] = q;
+    return q;
+}
+
+// grid (tiles along columns, tiles along rows, hours of the range); kSwThreads
+// threads; dynamic shared memory sweep_smem_bytes().  Scenes with water use
+// the raster sweep kernel (they also need the first direction's Lup).
+// `bounds` (optional): per-hour GVF input ranges of the day ([3][nhours]),
+// grid.z = hour h0 + blockIdx.z.
+__global__ void __launch_bounds__(kSwThreads, 6) day_sweep_tma_kernel(const __grid_constant__ CUtensorMap geo_map,
+                                                                      SolweigScene S,
+                                                                      const SolweigHour* __restrict__ hours,
+                                                                      float4* __restrict__ quads,
+                                                                      const float* __restrict__ ceiling,
+                                                                      const int* __restrict__ exits,
+                                                                      int* __restrict__ error,
+                                                                      uint32_t* __restrict__ bounds, int nhours,
+                                                                      int h0) {
+    const SolweigHour& h = hours[blockIdx.z];
+    if (!h.daytime) return;
+    extern __shared__ unsigned char sw_raw[];
+    SweepSmem& sm = *reinterpret_cast<SweepSmem*>(
+        (reinterpret_cast<uintptr_t>(sw_raw) + 127) & ~static_cast<uintptr_t>(127));
+    const int tid = threadIdx.x;
+    const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
+    const int K = h.steps;
+    const int r0 = blockIdx.y * kSwTile, c0 = blockIdx.x * kSwTile;
+    // the window holds the tile in its corner away from the sun
+    const int2 last = K > 0 ? __ldg(&ray[K - 1]) : make_int2(0, 0);
+    const int wr0 = last.x < 0 ? r0 + kSwTile - kSwWin : r0;
+    const int wc0 = last.y < 0 ? c0 + kSwTile - kSwWin : c0;
+    if (tid == 0) sw_mbar_init(&sm.bar);
+    __syncthreads();  // the barrier is initialised before anyone polls it
+    if (tid == 0) sw_tma_load(sm.win, &geo_map, 4 * wc0, wr0, &sm.bar, kSwWinBytes);
+    // first step at which each tile row / column leaves the window (linear
+    // scan, capped: a smaller value only moves samples to the raster path)
+    if (tid < 2 * kSwTile) {
+        const bool row = tid < kSwTile;
+        const int i = row ? tid : tid - kSwTile;
+        const int pos = row ? r0 + i - wr0 : c0 + i - wc0;
+        const int lim = K < kSwScanLimit ? K : kSwScanLimit;
+        int k = 0;
+        for (; k < lim; ++k) {
+            const int2 o = __ldg(&ray[k]);
+            const int v = pos + (row ? o.x : o.y);
+            if (v < 0 || v >= kSwWin) break;
+        }
+        (row ? sm.row_exit : sm.col_exit)[i] = k;
+    }
+    // this thread's pixel: warps take 8 x 4 (columns x rows) pieces
+    const int w = tid >> 5, l = tid & 31;
+    const int tx = (w & 1) * 8 + (l & 7), ty = (w >> 1) * 4 + (l >> 3);
+    const int r = r0 + ty, c = c0 + tx;
+    const bool in = r < S.rows && c < S.cols;
+    const long long p = in ? (long long)r * S.cols + c : 0;
+    const double a = in ? S.dsm[p] : 0.0;
+    const double wall = in ? S.walls[p] : 0.0;
+    const uint8_t fl = in ? S.flags[p] : 0;
+    const double top_p = in ? S.vegdem[p] : 0.0;
+    int kend = 0;
+    if (in) kend = min(K, min(__ldg(&exits[r]), __ldg(&exits[S.rows + c])));
+    // wait for the window (bounded); on a timeout record the error, wait once
+    // more for the copy in flight and walk from the raster only
+    const bool got = sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
+    if (!got) {
+        if (tid == 0) atomicExch(error, 2);
+        sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
+    }
+    const bool staged = __syncthreads_and(got) != 0;
+    // window maximum of the three heights
+    float m = -__int_as_float(0x7f800000);
+    if (staged) {
+        for (int i = tid; i < kSwWin * kSwWin; i += kSwThreads) {
+            const float4 v = sm.win[i];
+            m = fmaxf(m, fmaxf(v.x, fmaxf(v.y, v.z)));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (l == 0) sm.wmax[w] = m;
+    __syncthreads();
+    m = sm.wmax[0];
+#pragma unroll
+    for (int i = 1; i < kSwThreads / 32; ++i) m = fmaxf(m, sm.wmax[i]);
+    const int kw = staged && in ? min(kend, min(sm.row_exit[ty], sm.col_exit[tx])) : 0;
+    const double pinf = __longlong_as_double(0x7ff0000000000000ll);
+    const double wclear = a >= 0.0 ? nextafter((double)m - a, pinf) : pinf;
+    const ShadowResult s = shadow_walk_window(in, sm.win, kSwWin, (r - wr0) * kSwWin + (c - wc0), kw, wclear,
+                                              reinterpret_cast<const float4*>(S.geo32), S.cols, p, a, top_p,
+                                              (fl & 2) != 0, wall, ray, h.ray_dz, K, kend, S.hmax, ceiling);
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (in) q = write_quad(S, h, p, a, wall, fl, s, quads + (long long)blockIdx.z * S.rows * S.cols);
+    if (bounds) gvf_bounds_reduce(in && (fl & 1), q.y, q.z * q.x, bounds, nhours, h0 + blockIdx.z);
+}
+
+// Tensor map of the packed geometry viewed as a rows x (4 * cols) float32
+// array, box kSwWin rows x 4 * kSwWin floats (one window); elements outside
+// the raster read as zero (the walks never use them: they stop at the raster
+// edge).  The x coordinate of a window is 4 * its first column, so every
+// copy starts on a 16-byte boundary.  The driver's encoder is looked up once
+// through the runtime.
+inline int sweep_geo_map(const SolweigScene& S, CUtensorMap* map) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    static int looked_up = 0;
+    if (!looked_up) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        const cudaError_t e = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000,
+                                                               cudaEnableDefault, &q);
+        if (e == cudaSuccess && q == cudaDriverEntryPointSuccess) encode = reinterpret_cast<Encode>(fn);
+        looked_up = 1;
+    }
+    SOLWEIG_CHECK_ARG(encode != nullptr, "day sweep: cuTensorMapEncodeTiled is not available");
+    SOLWEIG_CHECK_ARG(S.geo32 && ((uintptr_t)S.geo32 & 15) == 0, "day sweep: packed geometry missing or unaligned");
+    const cuuint64_t dims[2] = {4ull * (cuuint64_t)S.cols, (cuuint64_t)S.rows};
+    const cuuint64_t strides[1] = {16ull * (cuuint64_t)S.cols};
+    const cuuint32_t box[2] = {4u * kSwWin, (cuuint32_t)kSwWin};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(S.geo32), dims, strides,
+                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("day sweep: cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return SOLWEIG_ERR_CUDA;
+    }
+    return SOLWEIG_OK;
+}
+
+inline size_t sweep_smem_bytes() { return sizeof(SweepSmem) + 128; }
+
+}  // namespace
+
+}  // namespace solweig
