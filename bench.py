@@ -14,7 +14,10 @@ With N > 1 (torchrun, one rank per GPU) every rank runs its own day of the
 same tile (days are independent: the thermal state resets daily), so the
 work per GPU is fixed ("weak" scaling) and there is no data-path collective.
 ``--impl reference`` times the float64 CPU port of the reference path on the
-host cores (a process pool over independent tiles) and prints its own line.
+host cores (one process per core, each stepping the 200 x 200 px, 24 h CPU
+configuration of the reference's benchmark) and prints its own line.  The
+headline line also carries the 720 h target (30 days in one CUDA graph vs the
+plain form over the same days) and a per-stage roofline.
 """
 from __future__ import annotations
 
@@ -44,6 +47,8 @@ def _args():
     p.add_argument("--form", choices=("plain", "batched", "chosen"), default="chosen")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-month", action="store_true",
+                   help="skip the 720 h (30 days in one graph) figure of the headline line")
     p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient"), default="day",
                    help="day: the headline 2000^2 x 24 h line; month: 2000^2 x 720 h in one graph; "
                         "tiles: 64 uneven tiles in one graph; precision: 4000^2 patch-sum error report")
@@ -56,60 +61,88 @@ def _args():
 # CPU reference arm: the float64 port of the reference path on host cores
 # ----------------------------------------------------------------------------
 
-CPU_TILE = 96
+# The CPU configuration of the reference's headline (C1): the 200 x 200 px
+# synthetic scene (seed 0, 53 N, DOY 172, 24 hourly steps) through the
+# float64 numpy port of the reference path (walls, 153-patch SVF, hourly
+# Solweig_2022a_calc restatement, UTCI).  Static preparation is done once per
+# process, untimed (as the GPU arm prepares walls and SVF before timing);
+# timed samples are consecutive hours of the day with the thermal state
+# carried, a new day starting after hour 23.
+C1 = 200
+C1_LOC = dict(latitude=53.0, longitude=0.0, altitude=3.0)
+_C1 = {}
 
 
-def _cpu_tile(seed):
-    import numpy as np
+def _c1_init():
     from oracle import step as ST
     from solweig_cuda_b200 import synthetic
-    sc = synthetic.make_scene(CPU_TILE, seed=seed)
-    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
-    t0 = time.perf_counter()
-    s = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
-    ST.run_day(s, met, dict(latitude=53.0, longitude=0.0, altitude=3.0), 0.0)
-    return CPU_TILE * CPU_TILE * 24, time.perf_counter() - t0, float(np.float64(0))
+    sc = synthetic.make_scene(C1, seed=0)
+    _C1["met"] = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    _C1["s"] = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    _C1["gen"] = None
 
 
-def cpu_port_throughput(workers, tiles):
-    """pixel-hours/s of the oracle port over ``tiles`` independent tiles on ``workers`` processes."""
-    import multiprocessing as mp
+def _c1_step(hours):
+    """The next ``hours`` hours of the C1 day in this process: (pixel-hours, seconds)."""
+    from oracle import step as ST
+    if not _C1:
+        _c1_init()
     t0 = time.perf_counter()
-    if workers <= 1:
-        res = [_cpu_tile(s) for s in range(tiles)]
-    else:
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(workers) as pool:
-            res = pool.map(_cpu_tile, range(tiles))
-    wall = time.perf_counter() - t0
-    work = sum(r[0] for r in res)
-    return work / wall, wall
+    done = 0
+    while done < hours:
+        if _C1["gen"] is None:
+            _C1["gen"] = ST.day_hours(_C1["s"], _C1["met"], C1_LOC, 0.0)
+        try:
+            next(_C1["gen"])
+            done += 1
+        except StopIteration:
+            _C1["gen"] = None
+    return C1 * C1 * hours, time.perf_counter() - t0
 
 
 def run_reference(a, rank, world):
+    """pixel-hours/s of the port on every host core: one process per core, each
+    stepping its own C1 day 4 hours per timed step."""
     if rank != 0:
         return
-    workers = os.cpu_count() or 1
+    import multiprocessing as mp
+    workers = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    hours = 4
+    ctx = mp.get_context("spawn")
     vals = []
-    for i in range(a.warmup + a.steps):
-        v, wall = cpu_port_throughput(workers, workers)
-        if i >= a.warmup:
-            vals.append((v, wall))
+    with ctx.Pool(workers, initializer=_c1_init) as pool:
+        pool.map(_c1_step, [0] * workers, chunksize=1)  # every process prepared
+        for i in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_c1_step, [hours] * workers, chunksize=1)
+            wall = time.perf_counter() - t0
+            if i >= a.warmup:
+                vals.append((sum(r[0] for r in res) / wall, wall))
     value = sum(v for v, _ in vals) / len(vals)
     ms = 1000.0 * sum(w for _, w in vals) / len(vals)
+    sample = (f"{workers} processes x {hours} consecutive hours of the {C1}x{C1} px day (state carried) "
+              f"per step; walls + 153-patch SVF prepared per process before timing")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"float64 CPU port of the reference path: {workers} tiles of "
-                               f"{CPU_TILE}x{CPU_TILE} px x 24 h (walls, 153-patch SVF, hourly "
-                               f"Tmrt+UTCI) per step, one tile per host process",
-                   "size": CPU_TILE, "hours": 24},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
-                         "sample": f"{workers} x ({CPU_TILE}^2 px x 24 h) per step"},
+        "config": {"workload": f"float64 CPU port of the reference path on the {C1}x{C1} px, 24 h CPU "
+                               f"configuration (seed 0, 53N, DOY 172): hourly Tmrt+UTCI",
+                   "size": C1, "hours": 24, "cores": workers},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_single():
+    """The port on one host core: 12 consecutive hours (0-11) of the C1 day."""
+    _c1_init()
+    work, sec = _c1_step(12)
+    return {"value": work / sec, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{C1}x{C1} px (seed 0, 53N, DOY 172), hours 0-11 with the thermal state carried, "
+                      f"walls + 153-patch SVF prepared before timing; float64 numpy port of the reference "
+                      f"path, {sec:.1f} s"}
 
 
 # ----------------------------------------------------------------------------
@@ -174,13 +207,38 @@ class ClockSampler:
 
 
 def _peaks():
+    """(HBM GB/s, sustained BF16 TFLOP/s, source): the measured copy bandwidth and
+    cuBLAS BF16 throughput of this pool's B200s, else the recorded fallback."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        return 6650.0, "fallback"
+        tf = d.get("bf16_tflops_sustained", d.get("bf16_tflops"))
+        return float(d["hbm_gbs"]), float(tf), "measured (MEASURED_PEAKS.json hbm_gbs, bf16_tflops_sustained)"
+    except (OSError, KeyError, ValueError, TypeError):
+        return 6650.0, 1400.0, "fallback (6.65 TB/s, 1.4 PFLOP/s sustained BF16)"
+
+
+# What bounds each stage of the batched day (from the ncu summaries in
+# profiles/): the HBM fraction of the gather-bound stages is small by nature.
+STAGE_LIMITER = {
+    "day_shadow_kernel": "latency of the ray-step gathers (shared-memory window, then L1/L2)",
+    "day_gvf_kernel": "shared-memory wavefronts of the 18 x 22 walks",
+    "day_tables_kernel": "negligible (one block per hour)",
+    "patch_gemm_kernel": "tensor pipe and the FP32 sum stores",
+    "day_radiation_kernel": "latency of the per-pixel hour loop",
+}
+
+
+def _stage_kernels(cfg):
+    """The kernel that does the work of each timed stage for a launch config."""
+    return {
+        "day_shadow_kernel": "day_sweep_tma_kernel" if cfg.sweep_window else "day_shadow_kernel",
+        "day_gvf_kernel": {2: "day_gvf_hv8_kernel", 1: "day_gvf_hv_kernel"}.get(cfg.gvf_hours, "day_gvf_kernel"),
+        "day_tables_kernel": "day_tables_kernel",
+        "patch_gemm_kernel": "patch_gemm_kernel",
+        "day_radiation_kernel": "day_radiation_kernel",
+    }
 
 
 def _traffic(kernel):
@@ -521,26 +579,35 @@ def main():
     value_plain = world * work / (ms_plain / 1000.0)
 
     # Per-kernel timing of one instrumented day (events on the launching stream).
-    peak, peak_kind = _peaks()
-    peak_src = (peak_kind + " (MEASURED_PEAKS.json hbm_gbs)") if peak_kind == "measured" else "fallback"
+    peak, peak_tf, peak_src = _peaks()
     roof = None
     if a.form == "chosen":
         stage_ms = chosen.profile_day(met)
         day_hours = int(sum(1 for x in sun_alt if x > 0))
         px = n * n
         bytes_per = batched.ChosenDay.stage_bytes(px, 24, day_hours)
-        stages = {k: {"ms": v, "launches": 1, "bytes_per_launch": bytes_per[k]} for k, v in stage_ms.items()}
-        dom = max(stages, key=lambda k: stages[k]["ms"])
-        info = stages[dom]
-        achieved = info["bytes_per_launch"] / (info["ms"] / 1000.0) / 1e9
-        total = sum(v["ms"] for v in stages.values())
         gemm_flops = batched.ChosenDay.gemm_flops(px, 24, scene.layout.host.count)
-        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_src, "traffic": _traffic(dom),
-                "launch_ms": info["ms"],
-                "share": {k: round(v["ms"] / total, 4) for k, v in stages.items()},
-                "stages_ms": {k: round(v["ms"], 4) for k, v in stages.items()},
-                "patch_gemm_tflops": gemm_flops / (stage_ms["patch_gemm_kernel"] / 1000.0) / 1e12}
+        kernels = _stage_kernels(chosen.config)
+        total = sum(stage_ms.values())
+        stages = {}
+        for k, v in stage_ms.items():
+            if k == "patch_gemm_kernel":
+                ach = gemm_flops / (v / 1000.0) / 1e12
+                e = {"bound": "tensor", "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": ach / peak_tf, "algorithmic": gemm_flops}
+            else:
+                ach = bytes_per[k] / (v / 1000.0) / 1e9
+                e = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "algorithmic": bytes_per[k]}
+            e.update({"kernel": kernels[k], "ms": round(v, 4), "share": round(v / total, 4),
+                      "limiter": STAGE_LIMITER[k], "traffic": _traffic(kernels[k])})
+            stages[k] = e
+        dom = max(stages, key=lambda k: stages[k]["ms"])
+        d = stages[dom]
+        roof = {"bound": d["bound"], "kernel": d["kernel"], "achieved": d["achieved"], "peak": d["peak"],
+                "unit": d["unit"], "frac": d["frac"], "peak_source": peak_src, "traffic": d["traffic"],
+                "launch_ms": d["ms"], "limiter": d["limiter"], "stages": stages,
+                "patch_gemm_tflops": stages["patch_gemm_kernel"]["achieved"]}
     else:
         kern = plain.profile_day(met)
         dom = max(kern, key=lambda k: kern[k]["ms"])
@@ -550,6 +617,42 @@ def main():
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                 "traffic": _traffic(dom), "launch_ms": info["ms"] / info["launches"],
                 "share": {k: round(v["ms"] / sum(x["ms"] for x in kern.values()), 4) for k, v in kern.items()}}
+
+    # The 720 h target of the metric: 30 days (state reset daily) in ONE graph
+    # replay against the plain per-hour form over the same 30 days.
+    month = None
+    if a.form == "chosen" and world == 1 and not a.no_month:
+        met30 = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, days=30)
+        md = batched.MultiDay(scene, 53.0, 0.0, 3.0, 0.0, days=30, config=chosen.config)
+        t0 = time.perf_counter()
+        md.plan(met30)
+        plan_s = time.perf_counter() - t0
+        md.capture()
+        month_ms = _events_ms(md.replay, 2, 1, flush)
+        launches_month = md.launches
+        del md
+        torch.cuda.empty_cache()
+        torch.cuda.synchronize()
+        flush.zero_()
+        torch.cuda.synchronize()
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_ev.record()
+        for d in range(30):
+            plain.run_day(met30[24 * d:24 * (d + 1)], outputs=("tmrt", "utci"))
+        e_ev.record()
+        torch.cuda.synchronize()
+        plain_month_ms = s_ev.elapsed_time(e_ev)
+        work30 = n * n * 720
+        month = {"value": work30 / (month_ms / 1000.0), "ms_per_step": month_ms,
+                 "value_with_host_plan": work30 / (month_ms / 1000.0 + plan_s),
+                 "plain_value": work30 / (plain_month_ms / 1000.0), "plain_ms": plain_month_ms,
+                 "ratio_vs_plain": plain_month_ms / month_ms,
+                 "ratio_vs_plain_with_host_plan": plain_month_ms / (month_ms + 1000.0 * plan_s),
+                 "kernel_launches": launches_month, "host_plan_s": plan_s,
+                 "workload": f"{n}x{n} px x 720 h (DOY 172-201, thermal state reset daily): the batched "
+                             "form in one CUDA-graph replay (host plan of the 30 days outside it; also "
+                             "reported with it) vs the plain per-hour form over the same days (its host "
+                             "plan interleaved); L2 flushed before each"}
 
     # End to end through the public API with host buffers.
     from solweig_cuda_b200 import api
@@ -580,20 +683,19 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, wall = cpu_port_throughput(1, 1)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"one {CPU_TILE}x{CPU_TILE} px tile x 24 h (walls, SVF, hourly step, UTCI), "
-                         f"float64 numpy port of the reference path, {wall:.1f} s"}
+        cpu = cpu_baseline_single()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32+f64+bf16" if a.form == "chosen" else "f32+f64",
+            "data": "synthetic",
             "config": {"workload": f"{n}x{n} px at 1 m, 24 hourly steps (one day, DOY 172, 53N), "
                                    f"static walls + 153-patch SVF prepared before timing",
                        "form": a.form, "size": n, "hours": 24, "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"days over {world} GPU(s)"},
-            "plain": {"value": value_plain, "ms_per_step": ms_plain},
+            "plain": {"value": value_plain, "ms_per_step": ms_plain, "ratio": value / value_plain},
+            "month_720h": month,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,

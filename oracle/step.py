@@ -269,14 +269,12 @@ def hour_step(s, location, altitude, azimuth, zen, jday, psi, dectime, altmax, T
     return dict(zip(OUTPUT_NAMES, values))
 
 
-def run_day(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI"), psi=None):
-    """Hour loop of one calendar day (``src/series.py:396-495``).
-
-    ``met`` is the (rows, 24) forcing table of one day.  Returns a list (one
-    entry per hour) of dicts with the requested outputs; ``UTCI`` has NaN on
-    roofs (``buildings != 1``).  ``psi`` (scalar or per-pixel array), when
-    given, replaces the leaf-on/off transmissivity of every hour.
-    """
+def day_hours(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI"), psi=None):
+    """The hour loop of one calendar day (``src/series.py:396-495``) as a
+    generator: one dict of the requested outputs per hour, the thermal state
+    carried from hour to hour.  ``UTCI`` has NaN on roofs (``buildings != 1``).
+    ``psi`` (scalar or per-pixel array), when given, replaces the
+    leaf-on/off transmissivity of every hour."""
     sol = sun.metdata(met, location["latitude"], location["longitude"], location["altitude"], utc)
     doy = met[:, 1]
     leaf = (doy > CONSTANTS["firstdayleaf"]) & (doy < CONSTANTS["lastdayleaf"])
@@ -290,7 +288,6 @@ def run_day(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI"), psi=Non
     timestepdec = (dectime[1] - dectime[0]) if len(met) > 1 else 1 / 24.
     timeadd, firstdaytime, CI = 0., 1., 1.
     Twater = float(np.mean(met[:, 11])) if s["landcover"] else None
-    results = []
     for i in range(len(met)) if hours is None else hours:
         if dectime[i] - np.floor(dectime[i]) == 0:
             CI = 1.
@@ -307,5 +304,13 @@ def run_day(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI"), psi=Non
                 rec["UTCI"] = np.where(s["buildings"] == 1, u, np.nan)
             else:
                 rec[name] = o[name]
-        results.append(rec)
-    return results
+        yield rec
+
+
+def run_day(s, met, location, utc, hours=None, outputs=("Tmrt", "UTCI"), psi=None):
+    """Hour loop of one calendar day (``src/series.py:396-495``).
+
+    ``met`` is the (rows, 24) forcing table of one day.  Returns a list (one
+    entry per hour) of dicts with the requested outputs (see :func:`day_hours`).
+    """
+    return list(day_hours(s, met, location, utc, hours, outputs, psi))
