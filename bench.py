@@ -681,6 +681,27 @@ def main():
     if not e2e_times:
         e2e_s = None
 
+    # the reference's driver call (series.run_timeseries, no files written):
+    # rasters from host arrays, walls + SVF, 3 calendar days in the batched form
+    series_e2e = None
+    if rank == 0 and world == 1 and a.e2e_steps > 0:
+        import tempfile
+        from solweig_cuda_b200 import series
+        met3 = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, days=3)
+        with tempfile.TemporaryDirectory() as tmp:
+            def run_series(m):
+                series.run_timeseries(sc.dsm, sc.trees, sc.dem, m, tmp, 0.0, 53.0, landcover_path=sc.landcover,
+                                      utc_offset_hours=0.0, no_write=True, device=dev)
+            run_series(met3[:24])  # warm-up: kernel attributes, allocator
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            run_series(met3)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        series_e2e = {"value": n * n * 72 / dt, "unit": UNIT, "seconds": dt,
+                      "includes": "series.run_timeseries(no_write=True): H2D rasters, walls, 153-patch SVF, "
+                                  "3 days x 24 h in the batched form"}
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_single()
@@ -701,7 +722,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_s,
                     "seconds_each_step": [round(t, 4) for t in e2e_times],
-                    "includes": "H2D rasters, walls, 153-patch SVF, 24 h, D2H Tmrt+UTCI"},
+                    "includes": "H2D rasters, walls, 153-patch SVF, 24 h, D2H Tmrt+UTCI",
+                    "run_timeseries_no_write": series_e2e},
             "gpu_launches": launches_per_day * a.steps,
             "clocks": clocks.summary(),
         }

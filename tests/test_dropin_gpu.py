@@ -154,3 +154,30 @@ def test_run_timeseries_and_cli_write_outputs(cuda, tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     tiles = sorted(p.name for p in (tmp_path / "cli_out").iterdir())
     assert tiles == ["r000_c000", "r000_c001", "r001_c000", "r001_c001"]
+
+
+def test_run_tiles_equals_run_timeseries_per_tile(cuda, tmp_path):
+    """The tiled driver (every tile of a group in one captured graph per day,
+    series.run_tiles, as run.py uses it) writes, for each tile, exactly what
+    run_timeseries writes for that tile's input window cropped to its core."""
+    from solweig_cuda_b200 import series, synthetic, tiling
+    sc = small_scene(52, seed=9)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, seed=3)
+    jobs = []
+    for t in tiling.tile_windows(52, 52, core=30, halo=8):
+        jobs.append({"tile_id": t["tile_id"], "output_core": t["output_core"],
+                     **{k: np.ascontiguousarray(tiling.extract(v, t))
+                        for k, v in (("dsm", sc.dsm), ("trees", sc.trees), ("dem", sc.dem),
+                                     ("landcover", sc.landcover))}})
+    got = series.run_tiles(jobs, met, tmp_path / "tiles", 0.0, 53.0, utc_offset_hours=0.0, save_kdown=True)
+    assert sorted(got) == sorted(j["tile_id"] for j in jobs)
+    for j in jobs:
+        ref = series.run_timeseries(j["dsm"], j["trees"], j["dem"], met, tmp_path / "single" / j["tile_id"],
+                                    0.0, 53.0, landcover_path=j["landcover"], utc_offset_hours=0.0,
+                                    output_core=j["output_core"], save_kdown=True)
+        (date,) = ref["days"]
+        for var in ("UTCI", "TMRT", "Kdown"):
+            a = np.load(got[j["tile_id"]]["days"][date][var][0])
+            b = np.load(ref["days"][date][var][0])
+            assert a.shape == (24,) + tuple(j["output_core"][2:])
+            assert np.array_equal(a.view(np.int32), b.view(np.int32)), (j["tile_id"], var)
