@@ -391,12 +391,11 @@ def run_precision(a):
             W[2 * h + 1] = lum * L.cos_alt * L.steradian
     Wt = torch.from_numpy(W).to(dev)
     ref_sky, ref_veg = sky @ Wt.T, veg @ Wt.T
-    got_sky = sums[0][:, idx].T.to(torch.float64)
-    got_veg = sums[1][:, idx].T.to(torch.float64)
+    gsum = sums[:, idx].T.to(torch.float64)
+    rsum = ref_sky + 0.03 * ref_veg
     scale = Wt.abs().sum(dim=1).clamp_min(1e-30)
-    err_sky = ((got_sky - ref_sky).abs() / scale).max().item()
-    err_veg = ((got_veg - ref_veg).abs() / scale).max().item()
-    abs_sky = (got_sky - ref_sky).abs().max().item()
+    err_sum = ((gsum - rsum).abs() / scale).max().item()
+    abs_sum = (gsum - rsum).abs().max().item()
     # the per-hour FP32 form (per-patch loop, no tensor cores) beside it
     plain = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
     ref = plain.run_day(met, outputs=outs)
@@ -409,8 +408,9 @@ def run_precision(a):
         "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
         "config": {"workload": f"{n}x{n} px at 1 m, DOY 172, 53N, BF16 hi/lo weights, FP32 accumulation",
                    "sample_pixels": 65536},
-        "patch_sums_max_rel_error_vs_fp64": {"sky": err_sky, "vegetation": err_veg},
-        "patch_sums_max_abs_error_vs_fp64": abs_sky,
+        "patch_sums_max_rel_error_vs_fp64": err_sum,
+        "patch_sums_max_abs_error_vs_fp64": abs_sum,
+        "patch_sums": "sky + 0.03 x vegetation sums of luminance and luminance*cos*omega, per hour",
         "max_abs_diff_vs_fp32_form": diffs,
         "stages_ms": stage,
         "patch_gemm_tflops": gemm_flops / (stage["patch_gemm_kernel"] / 1000.0) / 1e12}), flush=True)

@@ -339,13 +339,18 @@ int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout*
                               void* stream, float* stage_ms);
 /* Byte offsets inside the batched-day work buffer: quads [H][px] float4,
  * first-direction Lup [H][px], GVF [H][3][px] (Lup, albedo, shadow),
- * albedo-without-shadow GVF [px], patch sums [2][2H][px] (sky, vegetation x
- * (luminance, luminance*cos*omega) per hour), weights f32 [2H][160], BF16
- * operand, per-hour tables, error flag, per-hour GVF input ranges [3][H]
+ * albedo-without-shadow GVF [px], patch sums (room for [2][2H][px]; the day
+ * writes [2H][px]: sky plus 0.03 x vegetation sums of luminance and
+ * luminance*cos*omega per hour), weights f32 [2H][160], BF16 operands (hi/lo
+ * of the weights and of 0.03 x the weights), per-hour tables, error flag,
+ * per-hour GVF input ranges [3][H]
  * (ordered-int min Lup, max Lup, max albedo*shadow), total size:
  * offsets[0..10]. */
 int solweig_day_batched_layout(int rows, int cols, int nhours, int has_water, int64_t* offsets);
-/* Copy the device error flag of the last batched day in `work` to out_device. */
+/* Copy the device error flag of the last batched day in `work` to out_device:
+ * 0 = none, 1 = a tensor-core wait of the contraction timed out (results
+ * invalid), 2 = a sweep window's TMA wait timed out (that tile walked from the
+ * raster instead; results still exact). */
 int solweig_day_batched_error(const void* work, int rows, int cols, int nhours, int has_water,
                               int* out_device, void* stream);
 /* The patch contraction alone: out[c][p] = sum_k sky(p,k) * weights[c][k] for

@@ -101,10 +101,10 @@ def day_launches(scene, config, sweep_parts=1):
     """Kernel launches of one batched day for this scene and launch shapes,
     with the sweep stage issued in ``sweep_parts`` hour ranges: per range the
     ray exits, the ceilings and the sweep; once the height dilation; then the
-    GVF (the hour-vectorized kernel or the per-hour one), weights, split,
-    tables, contraction and radiation."""
+    GVF (the hour-vectorized kernel or the per-hour one), weights, two
+    splits (sky and vegetation weights), tables, contraction and radiation."""
     c = int(not config.no_ceiling)
-    return sweep_parts * (2 + c) + c + 6
+    return sweep_parts * (2 + c) + c + 7
 
 
 class ChosenDay(BatchedDay):
@@ -257,16 +257,17 @@ class ChosenDay(BatchedDay):
         (101 B); GVF: 16 B quad + 4 B face
         bits + 4 B emissivity read, 3 planes + the albedo-without-shadow plane
         written (40 B); tables: per-hour tables (negligible); contraction: 40 B
-        of mask words per pixel read, 2 x 2 sums per pixel-hour written
-        (16 B); radiation: 109 B of per-pixel statics and 16 B of state per
-        day, 28 B per daytime pixel-hour (3 GVF planes, 4 sums) and 8 B per
-        pixel-hour written (Tmrt, UTCI)."""
+        of mask words per pixel read, 2 sums per pixel-hour written (8 B: sky
+        plus transmitted vegetation, luminance and luminance*cos*omega);
+        radiation: 109 B of per-pixel statics and 16 B of state per day, 20 B
+        per daytime pixel-hour (3 GVF planes, 2 sums) and 8 B per pixel-hour
+        written (Tmrt, UTCI)."""
         return {
             "day_shadow_kernel": pixels * day_hours * 101,
             "day_gvf_kernel": pixels * day_hours * 40,
             "day_tables_kernel": hours * 9680,
-            "patch_gemm_kernel": pixels * (40 + 16 * hours),
-            "day_radiation_kernel": pixels * (125 + 28 * day_hours + 8 * hours),
+            "patch_gemm_kernel": pixels * (40 + 8 * hours),
+            "day_radiation_kernel": pixels * (125 + 20 * day_hours + 8 * hours),
         }
 
     @staticmethod
@@ -317,26 +318,17 @@ class ChosenDay(BatchedDay):
         return self.work[o["quads"]:o["quads"] + n].view(torch.float32).view(self.hours, self.scene.rows,
                                                                                  self.scene.cols, 4)
 
-    def quads(self):
-        """The sweep's per-pixel GVF inputs of the last day as a [H, rows, cols, 4]
-        float32 view: shadow, Lup excess, albedo and the ground (1) / sunlit-wall
-        (2) bits as an int32 bit pattern (daytime hours only; night hours hold
-        stale values)."""
-        o = self.work_offsets()
-        n = 16 * self.hours * self.scene.pixels
-        return self.work[o["quads"]:o["quads"] + n].view(torch.float32).view(self.hours, self.scene.rows,
-                                                                                 self.scene.cols, 4)
-
     def patch_sums(self):
-        """The contraction's output of the last day as a [2, 2H, pixels] view:
-        [sky|vegetation][2h + (0: luminance, 1: luminance*cos*omega)]."""
+        """The contraction's output of the last day as a [2H, pixels] view: row
+        2h + 0 the luminance and 2h + 1 the luminance*cos*omega summed over the
+        sky patches plus 0.03 x the same over the vegetation patches."""
         o = self.work_offsets()
-        n = 2 * 2 * self.hours * self.scene.pixels
-        return self.work[o["sums"]:o["sums"] + 4 * n].view(torch.float32).view(2, 2 * self.hours,
-                                                                              self.scene.pixels)
+        n = 2 * self.hours * self.scene.pixels
+        return self.work[o["sums"]:o["sums"] + 4 * n].view(torch.float32).view(2 * self.hours, self.scene.pixels)
 
     def error_flag(self):
-        """Device error flag of the last day (0 = ok, 1 = a tensor-core wait timed out)."""
+        """Device error flag of the last day (0 = ok, 1 = a tensor-core wait timed
+        out, 2 = a sweep window's TMA wait timed out: that tile walked from the raster)."""
         flag = torch.zeros(1, dtype=torch.int32, device=self.scene.device)
         sc = self.scene
         _lib.check(_lib.lib().solweig_day_batched_error(

@@ -254,12 +254,16 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     const int nb = (ncols + 15) / 16 * 16;
     day_weights_kernel<<<blocks_for((long long)ncols * kK, 256), 256, 0, st>>>(layout, hours, nhours, wf32);
     SOLWEIG_CHECK_LAUNCH("day_weights_kernel");
+    // sky weights, then the vegetation weights prescaled by the diffuse
+    // transmissivity of vegetation (0.03, src/svf.py:117-131): one set of sums
     split_bf16_kernel<<<blocks_for((long long)nb * kK, 256), 256, 0, st>>>(wf32, ncols, nb, S.patches, bw);
+    split_bf16_kernel<<<blocks_for((long long)nb * kK, 256), 256, 0, st>>>(wf32, ncols, nb, S.patches,
+                                                                           bw + 2LL * nb * kK, 0.03f);
     SOLWEIG_CHECK_LAUNCH("split_bf16_kernel");
     day_tables_kernel<<<nhours, kK, 0, st>>>(layout, hours, tables);
     SOLWEIG_CHECK_LAUNCH("day_tables_kernel");
     if (ev) cudaEventRecord(ev[3], st);
-    int rc = launch_gemm(S.masks, px, S.patches, bw, ncols, nb, sums, err, st, cfg.gemm_ctas_per_sm);
+    int rc = launch_gemm(S.masks, px, S.patches, bw, ncols, nb, sums, err, st, cfg.gemm_ctas_per_sm, true);
     if (rc) return rc;
     if (ev) cudaEventRecord(ev[4], st);
 

@@ -844,14 +844,14 @@ __global__ void day_weights_kernel(const SolweigSkyLayout* __restrict__ L, const
     w[idx] = v;
 }
 
-// BF16 hi/lo split of w [ncols][kK] into the canonical operand layout
+// BF16 hi/lo split of scale * w [ncols][kK] into the canonical operand layout
 // b[0][nb rows] (hi) and b[1][nb rows] (lo); rows >= ncols are zero.
 __global__ void split_bf16_kernel(const float* __restrict__ w, int ncols, int nb, int patches,
-                                  __nv_bfloat16* __restrict__ b) {
+                                  __nv_bfloat16* __restrict__ b, float scale = 1.f) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= nb * kK) return;
     const int n = idx / kK, k = idx - n * kK;
-    const float v = (n < ncols && k < patches) ? w[n * kK + k] : 0.f;
+    const float v = (n < ncols && k < patches) ? scale * w[n * kK + k] : 0.f;
     const __nv_bfloat16 hi = __float2bfloat16_rn(v);
     const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
     const int o = canon_off(n, k);
@@ -950,13 +950,19 @@ struct GemmArgs {
     const uint32_t* masks;  // S/V bit planes [10][px]
     long long px;
     int patches;
-    const __nv_bfloat16* b;  // [2][nb * kK] canonical hi, lo
+    const __nv_bfloat16* b;  // [2][nb * kK] canonical hi, lo (combined: [4][nb * kK], then c * w hi, lo)
     int ncols, nb;
-    float* out;  // [2 * ncols][px]: sky columns, then vegetation columns
+    float* out;  // [2 * ncols][px]: sky columns, then vegetation columns (combined: [ncols][px])
     int* error;
+    // 1: one set of columns, sky sums plus the vegetation sums of weights
+    // prescaled by c (the diffuse transmissivity of vegetation): both MMA
+    // pairs accumulate into the same tensor-memory columns
+    int combined;
 };
 
-size_t gemm_smem_bytes(int nb) { return (size_t)2 * kABytes + (size_t)2 * nb * kK * 2 + 16; }
+size_t gemm_smem_bytes(int nb, bool combined) {
+    return (size_t)2 * kABytes + (size_t)(combined ? 4 : 2) * nb * kK * 2 + 16;
+}
 
 // Expand 8 mask bits to 8 BF16 values (1.0 or 0.0) packed in a uint4.
 __device__ __forceinline__ uint4 expand8(uint32_t byte) {
@@ -978,18 +984,19 @@ __global__ void __launch_bounds__(kARows, 1) patch_gemm_kernel(GemmArgs g) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* a_sky = smem;
     unsigned char* a_veg = smem + kABytes;
-    unsigned char* b_ops = smem + 2 * kABytes;  // hi then lo
+    unsigned char* b_ops = smem + 2 * kABytes;  // hi then lo (combined: then c * w hi, lo)
     const int bbytes = g.nb * kK * 2;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(b_ops + 2 * bbytes);
+    const int nbops = g.combined ? 4 : 2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(b_ops + nbops * bbytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5;
     uint32_t ncols_tmem = 32;
-    while (ncols_tmem < (uint32_t)(2 * g.nb)) ncols_tmem <<= 1;
+    while (ncols_tmem < (uint32_t)((g.combined ? 1 : 2) * g.nb)) ncols_tmem <<= 1;
 
     {  // weights: global -> shared, 16 bytes per copy
         const uint4* src = reinterpret_cast<const uint4*>(g.b);
         uint4* dst = reinterpret_cast<uint4*>(b_ops);
-        for (int i = tid; i < 2 * bbytes / 16; i += blockDim.x) dst[i] = src[i];
+        for (int i = tid; i < nbops * bbytes / 16; i += blockDim.x) dst[i] = src[i];
     }
     if (tid == 0) {
         tc::mbar_init(bar, 1);
@@ -1046,8 +1053,15 @@ __global__ void __launch_bounds__(kARows, 1) patch_gemm_kernel(GemmArgs g) {
                 const uint64_t av = tc::smem_desc(a_veg_addr + s * 256, 128, kSBO);
                 tc::mma_bf16(tmem, as, bh, idesc, s > 0);
                 tc::mma_bf16(tmem, as, bl, idesc, true);
-                tc::mma_bf16(tmem + g.nb, av, bh, idesc, s > 0);
-                tc::mma_bf16(tmem + g.nb, av, bl, idesc, true);
+                if (g.combined) {
+                    const uint64_t ch = tc::smem_desc(b_hi_addr + 2 * bbytes + s * 256, 128, kSBO);
+                    const uint64_t cl = tc::smem_desc(b_hi_addr + 3 * bbytes + s * 256, 128, kSBO);
+                    tc::mma_bf16(tmem, av, ch, idesc, true);
+                    tc::mma_bf16(tmem, av, cl, idesc, true);
+                } else {
+                    tc::mma_bf16(tmem + g.nb, av, bh, idesc, s > 0);
+                    tc::mma_bf16(tmem + g.nb, av, bl, idesc, true);
+                }
             }
             tc::mma_commit(bar);
         }
@@ -1059,17 +1073,30 @@ __global__ void __launch_bounds__(kARows, 1) patch_gemm_kernel(GemmArgs g) {
         phase ^= 1u;
         tc::fence_after_sync();
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int c0 = 0; c0 < g.ncols; c0 += 8) {
-            float vs[8], vv[8];
-            tc::tmem_ld8(lane_base + c0, vs);
-            tc::tmem_ld8(lane_base + g.nb + c0, vv);
-            tc::tmem_wait_ld();
-            if (in) {
+        if (g.combined) {
+            for (int c0 = 0; c0 < g.ncols; c0 += 8) {
+                float vs[8];
+                tc::tmem_ld8(lane_base + c0, vs);
+                tc::tmem_wait_ld();
+                if (in) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    if (c0 + i < g.ncols) {
-                        g.out[(long long)(c0 + i) * g.px + p] = vs[i];
-                        g.out[(long long)(g.ncols + c0 + i) * g.px + p] = vv[i];
+                    for (int i = 0; i < 8; ++i)
+                        if (c0 + i < g.ncols) g.out[(long long)(c0 + i) * g.px + p] = vs[i];
+                }
+            }
+        } else {
+            for (int c0 = 0; c0 < g.ncols; c0 += 8) {
+                float vs[8], vv[8];
+                tc::tmem_ld8(lane_base + c0, vs);
+                tc::tmem_ld8(lane_base + g.nb + c0, vv);
+                tc::tmem_wait_ld();
+                if (in) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        if (c0 + i < g.ncols) {
+                            g.out[(long long)(c0 + i) * g.px + p] = vs[i];
+                            g.out[(long long)(g.ncols + c0 + i) * g.px + p] = vv[i];
+                        }
                     }
                 }
             }
@@ -1099,7 +1126,7 @@ struct DayRadArgs {
     const DayTable* tables;
     const float* gvf;   // [H][3][px]
     const float* nosh;  // [px]
-    const float* sums;  // [2 * ncols][px]
+    const float* sums;  // [ncols][px]: sky + 0.03 x vegetation sums (luminance, luminance*cos*omega)
     int ncols;
     SolweigState state;
     SolweigOutputs out;  // base pointers; hour h at + h * hour_stride
@@ -1255,13 +1282,14 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
                 tg_out = cur * (1.f - hs.wave_w) + prv * hs.wave_w;
                 st_tg = h.wave_update ? tg_out : prv;
             }
+            // the contraction already added the vegetation patches at their
+            // diffuse transmissivity (dsh_veg): sky + dsh_veg x vegetation sums
             const long long s0 = 2LL * hr;
-            const float lum_sky = a.sums[s0 * n + q], cw_sky = a.sums[(s0 + 1) * n + q];
-            const float lum_veg = a.sums[(a.ncols + s0) * n + q], cw_veg = a.sums[(a.ncols + s0 + 1) * n + q];
-            d_rad = hs.rad_d * (lum_sky + dsh_veg * lum_veg);
+            const float lum = a.sums[s0 * n + q], cw = a.sums[(s0 + 1) * n + q];
+            d_rad = hs.rad_d * lum;
             kdown = hs.rad_i_sin * shadow + d_rad + reflected;
             kside_i = shadow * hs.rad_i_cos;
-            kside_d = hs.rad_ratio * (cw_sky + dsh_veg * cw_veg);
+            kside_d = hs.rad_ratio * cw;
             kside = kside_i + kside_d + hs.sw_sun * band_weighted<OPT>(m_sun, wcos) +
                     hs.sw_shade * band_weighted<OPT>(m_shd, wcos) + hs.sw_shade * vc;
         } else {
@@ -1321,7 +1349,7 @@ DayWork day_work_layout(long long px, int nhours, bool water) {
     w.nosh = o; o = align256(o + 4LL * px);
     w.sums = o; o = align256(o + 4LL * px * 2 * ncols);
     w.wf32 = o; o = align256(o + 4LL * ncols * kK);
-    w.bw = o; o = align256(o + 2LL * 2 * nb * kK);
+    w.bw = o; o = align256(o + 2LL * 4 * nb * kK);
     w.tables = o; o = align256(o + (long long)sizeof(DayTable) * nhours);
     w.error = o; o = align256(o + 16);
     w.bounds = o; o = align256(o + 4LL * 3 * nhours);
@@ -1369,8 +1397,8 @@ void launch_day_gvf(int ty, const SolweigScene& S, const SolweigHour* hours, int
 }
 
 int launch_gemm(const uint32_t* masks, long long px, int patches, const __nv_bfloat16* b, int ncols, int nb,
-                float* out, int* error, cudaStream_t st, int ctas_per_sm = 0) {
-    const size_t smem = gemm_smem_bytes(nb);
+                float* out, int* error, cudaStream_t st, int ctas_per_sm = 0, bool combined = false) {
+    const size_t smem = gemm_smem_bytes(nb, combined);
     SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "patch contraction: %d weight columns need %zu bytes of shared memory",
                       ncols, smem);
     set_smem_attr((const void*)patch_gemm_kernel, smem);
@@ -1384,7 +1412,7 @@ int launch_gemm(const uint32_t* masks, long long px, int patches, const __nv_bfl
     long long grid = (long long)sms * per_sm;
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
-    GemmArgs g{masks, px, patches, b, ncols, nb, out, error};
+    GemmArgs g{masks, px, patches, b, ncols, nb, out, error, combined ? 1 : 0};
     patch_gemm_kernel<<<(unsigned)grid, kARows, smem, st>>>(g);
     SOLWEIG_CHECK_LAUNCH("patch_gemm_kernel");
     return SOLWEIG_OK;
