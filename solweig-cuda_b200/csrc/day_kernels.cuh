@@ -1171,6 +1171,10 @@ __device__ __forceinline__ float wedge_fsh_f(float ta, float tan_zen) {
 template <int OPT, int THREADS>
 __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(SolweigScene S, DayRadArgs a) {
     __shared__ float wcos[SOLWEIG_MAX_BANDS], wsin[SOLWEIG_MAX_BANDS];
+    // per-pixel statics of the day, one column per thread: read back every
+    // hour from shared memory instead of living in (spilled) registers
+    constexpr int kStat = 18;
+    __shared__ uint32_t stat[kStat][THREADS];
     const SolweigSkyLayout& L = *a.layout;
     if (threadIdx.x < SOLWEIG_MAX_BANDS) {
         const int b = threadIdx.x;
@@ -1178,7 +1182,6 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
         wcos[b] = b < L.nbands ? L.omega[k0] * L.cos_alt[k0] : 0.f;
         wsin[b] = b < L.nbands ? L.omega[k0] * L.sin_alt[k0] : 0.f;
     }
-    __syncthreads();  // wcos, wsin
     const long long n = (long long)S.rows * S.cols;
     const long long p = (long long)blockIdx.x * THREADS + threadIdx.x;
     const bool in = p < n;
@@ -1187,33 +1190,39 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
     const bool need_tg = o.tg || o.tg_out || a.state.tgout1;
 
     // --- per-pixel static data, loaded once for the day
-    uint32_t bld[SOLWEIG_MASK_WORDS];
+    {
+        uint32_t* my = &stat[0][threadIdx.x];
 #pragma unroll
-    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
-        const int nbits = S.patches - 32 * w;
-        const uint32_t valid = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
-        bld[w] = ~S.masks[(long long)w * n + q] & ~S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + q] & valid;
-    }
-    uint32_t cnt_lo = 0, cnt_hi = 0;  // sky patches per band, 8 bits each
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            const int nbits = S.patches - 32 * w;
+            const uint32_t valid = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
+            my[w * THREADS] =
+                ~S.masks[(long long)w * n + q] & ~S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + q] & valid;
+        }
+        uint32_t cnt_lo = 0, cnt_hi = 0;  // sky patches per band, 8 bits each
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        cnt_lo |= (uint32_t)S.sky_band_counts[(long long)b * n + q] << (8 * b);
-        cnt_hi |= (uint32_t)(b + 4 < S.nbands ? S.sky_band_counts[(long long)(b + 4) * n + q] : 0) << (8 * b);
+        for (int b = 0; b < 4; ++b) {
+            cnt_lo |= (uint32_t)S.sky_band_counts[(long long)b * n + q] << (8 * b);
+            cnt_hi |= (uint32_t)(b + 4 < S.nbands ? S.sky_band_counts[(long long)(b + 4) * n + q] : 0) << (8 * b);
+        }
+        const double tan_asvf = S.tan_asvf[q];
+        my[5 * THREADS] = cnt_lo;
+        my[6 * THREADS] = cnt_hi;
+        my[7 * THREADS] = (uint32_t)S.flags[q] | ((uint32_t)tan_bucket(tan_asvf) << 8);
+        my[8 * THREADS] = __float_as_uint(S.emis[q]);
+        my[9 * THREADS] = __float_as_uint(S.svfbuveg[q]);
+        my[10 * THREADS] = __float_as_uint((float)tan(S.svfalfa[q]));
+        my[11 * THREADS] = (uint32_t)__double2loint(tan_asvf);
+        my[12 * THREADS] = (uint32_t)__double2hiint(tan_asvf);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) my[(13 + i) * THREADS] = __float_as_uint(S.veg_sums[i * n + q]);
+        my[17 * THREADS] = __float_as_uint(a.nosh[q]);
     }
-    const uint8_t fl = S.flags[q];
-    const bool ground = fl & 1;
-    const bool water = S.has_water && (fl & 4);
-    const float emis = S.emis[q];
-    const float svfbuveg = S.svfbuveg[q];
-    const float tan_alfa = (float)tan(S.svfalfa[q]);
-    const double tan_asvf = S.tan_asvf[q];
-    const int tbucket = tan_bucket(tan_asvf);
-    const float vc = S.veg_sums[q], vs = S.veg_sums[n + q];
-    const float oc = S.veg_sums[2 * n + q], os = S.veg_sums[3 * n + q];
-    const float g_nosh = a.nosh[q];
+    __syncthreads();  // wcos, wsin (each thread reads only its own statics)
+    const volatile uint32_t* sv = &stat[0][threadIdx.x];
+    auto statf = [&](int f) { return __uint_as_float(sv[f * THREADS]); };
     constexpr float ewall = 0.9f, albedo_b = 0.2f;
     constexpr float absK = 0.7f, absL = 0.95f, Fside = 0.22f, Fup = 0.06f, Fcyl = 0.28f;
-    constexpr float dsh_veg = 0.03f;
     constexpr float sbc = (float)kSBC, inv_pi = (float)(1.0 / kPi);
 
     float st_lup = a.state.tgmap1 ? a.state.tgmap1[q] : 0.f;
@@ -1227,29 +1236,53 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
         const bool day = h.daytime != 0;
         const float ta = (float)h.ta;
 
-        // building patches: sunlit / shaded split of the hour
+        // building patches: sunlit / shaded split of the hour, weighted per
+        // altitude band (omega cos / omega sin), one mask word at a time
         const DayTable& T = hs;
         const int P = S.patches;
+        const uint32_t flw = sv[7 * THREADS];
+        const int tbucket = (int)(flw >> 8);
+        const double tan_asvf = __hiloint2double((int)sv[12 * THREADS], (int)sv[11 * THREADS]);
         const int isun = count_le_from(T.tsun, P, T.sun_start[tbucket], tan_asvf);
         const int ishd = count_le_from(T.vshade, P, T.shd_start[tbucket], tan_asvf);
-        uint32_t m_sun[SOLWEIG_MASK_WORDS], m_shd[SOLWEIG_MASK_WORDS], m_lsun[SOLWEIG_MASK_WORDS],
-            m_lshd[SOLWEIG_MASK_WORDS];
+        float lw_sun_c = 0.f, lw_sun_s = 0.f, lw_shd_c = 0.f, lw_shd_s = 0.f, sw_sun = 0.f, sw_shd = 0.f;
 #pragma unroll
         for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            const uint32_t bw = sv[w * THREADS];
             const uint32_t test = T.test[w];
-            m_sun[w] = bld[w] & T.suf[isun][w];
-            m_shd[w] = bld[w] & T.pre[ishd][w];
-            m_lsun[w] = m_sun[w] & test;
-            m_lshd[w] = bld[w] & (~test | m_shd[w]);
-        }
-        const float lw_sun_c = band_weighted<OPT>(m_lsun, wcos), lw_sun_s = band_weighted<OPT>(m_lsun, wsin);
-        const float lw_shd_c = band_weighted<OPT>(m_lshd, wcos), lw_shd_s = band_weighted<OPT>(m_lshd, wsin);
-        float ld_sky = 0.f, ls_sky = 0.f;
+            const uint32_t m_sun = bw & T.suf[isun][w];
+            const uint32_t m_shd = bw & T.pre[ishd][w];
+            const uint32_t m_lsun = m_sun & test;
+            const uint32_t m_lshd = bw & (~test | m_shd);
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const float cnt = (float)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
-            ld_sky = fmaf(hs.band_down[b], cnt, ld_sky);
-            ls_sky = fmaf(hs.band_side[b], cnt, ls_sky);
+            for (int b = 0; b < 8; ++b) {
+                const int lo = Bands<OPT>::off(b), hi = Bands<OPT>::off(b + 1);
+                const int a0 = lo > w * 32 ? lo : w * 32;
+                const int e0 = hi < w * 32 + 32 ? hi : w * 32 + 32;
+                if (a0 < e0) {
+                    const uint32_t mk = (e0 - a0 == 32) ? 0xffffffffu : (((1u << (e0 - a0)) - 1u) << (a0 - w * 32));
+                    const float c = wcos[b], sn = wsin[b];
+                    const float nls = (float)__popc(m_lsun & mk), nlh = (float)__popc(m_lshd & mk);
+                    lw_sun_c = fmaf(nls, c, lw_sun_c);
+                    lw_sun_s = fmaf(nls, sn, lw_sun_s);
+                    lw_shd_c = fmaf(nlh, c, lw_shd_c);
+                    lw_shd_s = fmaf(nlh, sn, lw_shd_s);
+                    if (day) {
+                        sw_sun = fmaf((float)__popc(m_sun & mk), c, sw_sun);
+                        sw_shd = fmaf((float)__popc(m_shd & mk), c, sw_shd);
+                    }
+                }
+            }
+        }
+        float ld_sky = 0.f, ls_sky = 0.f;
+        {
+            const uint32_t cnt_lo = sv[5 * THREADS], cnt_hi = sv[6 * THREADS];
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const float cnt = (float)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
+                ld_sky = fmaf(hs.band_down[b], cnt, ld_sky);
+                ls_sky = fmaf(hs.band_side[b], cnt, ls_sky);
+            }
         }
         const float lw_shade = hs.lw_shade, lw_sun = hs.lw_sun;
 
@@ -1261,10 +1294,11 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             const float g_lup = a.gvf[g0];
             const float g_alb = a.gvf[g0 + n];
             shadow = a.gvf[g0 + 2 * n];
-            const float fsh = wedge_fsh_f(tan_alfa, hs.tan_zen);
+            const float svfbuveg = statf(9);
+            const float fsh = wedge_fsh_f(statf(10), hs.tan_zen);
             const float reflected = albedo_b * (1.f - svfbuveg) * (hs.rad_g * (1.f - fsh) + hs.rad_d * fsh);
             const float base_up = hs.rad_d * svfbuveg + reflected;
-            kup_all = g_alb * hs.direct_up + base_up * g_nosh;
+            kup_all = g_alb * hs.direct_up + base_up * statf(17);
             const float prev = h.firstdaytime ? g_lup : st_lup;
             lup_all = g_lup * (1.f - hs.wave_w) + prev * hs.wave_w;
             st_lup = h.wave_update ? lup_all : prev;
@@ -1275,7 +1309,7 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
                                       ((double)S.tmaxlst[q] / 24.0 - h.snup / 24.0)) * kPi / 2.0;
                 double tgd = amp * sin(phase) * h.ci_tgg;
                 if (S.landcover == 1 && tgd < 0.0) tgd = 0.0;
-                if (water) tgd = h.twater - h.ta;
+                if (S.has_water && (flw & 4)) tgd = h.twater - h.ta;
                 tg = (float)tgd;
                 const float cur = tg * shadow + ta;
                 const float prv = h.firstdaytime ? cur : st_tg;
@@ -1290,16 +1324,17 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             kdown = hs.rad_i_sin * shadow + d_rad + reflected;
             kside_i = shadow * hs.rad_i_cos;
             kside_d = hs.rad_ratio * cw;
-            kside = kside_i + kside_d + hs.sw_sun * band_weighted<OPT>(m_sun, wcos) +
-                    hs.sw_shade * band_weighted<OPT>(m_shd, wcos) + hs.sw_shade * vc;
+            kside = kside_i + kside_d + hs.sw_sun * sw_sun + hs.sw_shade * sw_shd + hs.sw_shade * statf(13);
         } else {
-            float lup = emis * hs.night_lup;
-            if (S.landcover == 1 && (fl & 4)) lup = hs.night_lup_water;
+            float lup = statf(8) * hs.night_lup;
+            if (S.landcover == 1 && (flw & 4)) lup = hs.night_lup_water;
             lup_all = lup;
         }
         const float refl = (ld_sky + lup_all) * ((1.f - ewall) * 0.5f * inv_pi);
-        const float ldown = ld_sky + lw_shade * vs + lw_shade * lw_shd_s + lw_sun * lw_sun_s + refl * os;
-        const float lside = ls_sky + lw_shade * vc + lw_shade * lw_shd_c + lw_sun * lw_sun_c + refl * oc;
+        const float ldown =
+            ld_sky + lw_shade * statf(14) + lw_shade * lw_shd_s + lw_sun * lw_sun_s + refl * statf(16);
+        const float lside =
+            ls_sky + lw_shade * statf(13) + lw_shade * lw_shd_c + lw_sun * lw_sun_c + refl * statf(15);
         // E+S+W+N of Kup and Lup are 4x the all-direction values (see the file header).
         const float sstr = absK * (kside * Fcyl + (kdown + kup_all) * Fup + 2.f * kup_all * Fside) +
                            absL * ((ldown + lup_all) * Fup + lside * Fcyl + 2.f * lup_all * Fside);
@@ -1308,8 +1343,8 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             const long long hs_ = a.hour_stride;
             if (o.tmrt) o.tmrt[hr * hs_ + p] = tmrt;
             if (o.utci)
-                o.utci[hr * hs_ + p] = ground ? utci_eval(h.utci, (double)tmrt, h.ta, h.utci_valid)
-                                              : __int_as_float(0x7fc00000);
+                o.utci[hr * hs_ + p] = (flw & 1) ? utci_eval(h.utci, (double)tmrt, h.ta, h.utci_valid)
+                                                 : __int_as_float(0x7fc00000);
             if (o.kdown) o.kdown[hr * hs_ + p] = kdown;
             if (o.kup) o.kup[hr * hs_ + p] = kup_all;
             if (o.ldown) o.ldown[hr * hs_ + p] = ldown;

@@ -270,8 +270,10 @@ __device__ __forceinline__ float4 write_quad(const SolweigScene& S, const Solwei
 // grid (tiles along columns, tiles along rows, hours of the range); kSwThreads
 // threads; dynamic shared memory sweep_smem_bytes().  Scenes with water use
 // the raster sweep kernel (they also need the first direction's Lup).
-// `bounds` (optional): per-hour GVF input ranges of the day ([3][nhours]),
-// grid.z = hour h0 + blockIdx.z.
+// `hours`, `quads`, `ceiling` (planes [hour][px]) and `exits` ([hour][rows +
+// cols]) point at the range's first hour; grid.z indexes the hours of the
+// range.  `bounds` (optional): per-hour GVF input ranges of the day
+// ([3][nhours]) for hour h0 + blockIdx.z.
 __global__ void __launch_bounds__(kSwThreads, 6) day_sweep_tma_kernel(const __grid_constant__ CUtensorMap geo_map,
                                                                       SolweigScene S,
                                                                       const SolweigHour* __restrict__ hours,
@@ -322,8 +324,13 @@ __global__ void __launch_bounds__(kSwThreads, 6) day_sweep_tma_kernel(const __gr
     const double wall = in ? S.walls[p] : 0.0;
     const uint8_t fl = in ? S.flags[p] : 0;
     const double top_p = in ? S.vegdem[p] : 0.0;
+    // this hour's ray exits and ceiling plane (the pointers are those of the
+    // range's first hour)
+    const long long npx = (long long)S.rows * S.cols;
+    const int* ex = exits + (long long)blockIdx.z * (S.rows + S.cols);
+    const float* ceil_h = ceiling ? ceiling + (long long)blockIdx.z * npx : nullptr;
     int kend = 0;
-    if (in) kend = min(K, min(__ldg(&exits[r]), __ldg(&exits[S.rows + c])));
+    if (in) kend = min(K, min(__ldg(&ex[r]), __ldg(&ex[S.rows + c])));
     // wait for the window (bounded); on a timeout record the error, wait once
     // more for the copy in flight and walk from the raster only
     const bool got = sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
@@ -352,9 +359,9 @@ __global__ void __launch_bounds__(kSwThreads, 6) day_sweep_tma_kernel(const __gr
     const double wclear = a >= 0.0 ? nextafter((double)m - a, pinf) : pinf;
     const ShadowResult s = shadow_walk_window(in, sm.win, kSwWin, (r - wr0) * kSwWin + (c - wc0), kw, wclear,
                                               reinterpret_cast<const float4*>(S.geo32), S.cols, p, a, top_p,
-                                              (fl & 2) != 0, wall, ray, h.ray_dz, K, kend, S.hmax, ceiling);
+                                              (fl & 2) != 0, wall, ray, h.ray_dz, K, kend, S.hmax, ceil_h);
     float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (in) q = write_quad(S, h, p, a, wall, fl, s, quads + (long long)blockIdx.z * S.rows * S.cols);
+    if (in) q = write_quad(S, h, p, a, wall, fl, s, quads + (long long)blockIdx.z * npx);
     if (bounds) gvf_bounds_reduce(in && (fl & 1), q.y, q.z * q.x, bounds, nhours, h0 + blockIdx.z);
 }
 
