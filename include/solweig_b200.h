@@ -292,23 +292,23 @@ int solweig_day_batched(const SolweigScene* scene, const SolweigSkyLayout* layou
                         int first_steps, int second_steps, void* work, int64_t work_bytes,
                         void* stream);
 /* Launch shapes of the batched day (the autotuner's search space).
- * Defaults (config == NULL): {32, 8, 8, 256, 0, 2, 0, 1}. */
+ * Defaults (config == NULL): {16, 16, 8, 256, 0, 1, 0, 0}. */
 typedef struct SolweigDayConfig {
     int32_t shadow_bx, shadow_by;  /* shadow block: <= 256 threads, a multiple of 32 */
     int32_t gvf_rows;              /* GVF tile rows per block: 4, 8 or 16 (32 columns) */
     int32_t rad_threads;           /* radiation block: 128 or 256 pixels */
     int32_t gemm_ctas_per_sm;      /* contraction CTAs per SM: 0 = as many as fit, 1, 2 */
-    int32_t gvf_hours;             /* 32x32 tiles walk all daytime hours in one block (1 m
-                                      walk, no water): 2: 8 hours per pass, the hour values as
-                                      16-bit fixed point summed in integer lanes; 1: 4 hours
-                                      per pass in float32; 0: one launch slice per hour */
+    int32_t gvf_hours;             /* 1: 32x32 tiles walk all daytime hours in one block, 4
+                                      hours per pass (1 m walk, no water); 0: one launch slice
+                                      per hour everywhere */
     int32_t no_ceiling;            /* 0: the sweep stops on the per-hour ray ceilings
                                       (same results, fewer steps); 1: every ray walks
                                       to its global clearance */
-    int32_t sweep_window;          /* 1: the sweep reads its first steps from a 48x48 px
-                                      shared-memory window staged by TMA, with the warp-vote
-                                      exit on the window maximum (packed float32 geometry,
-                                      no water; same results); 0: every step from the raster */
+    int32_t sweep_window;          /* 1 (48x48 px) or 2 (40x40 px): the sweep reads its first
+                                      steps from a shared-memory window staged by TMA per 16x16
+                                      tile, with the warp-vote exit on the window maximum
+                                      (packed float32 geometry, no water; same results);
+                                      0: every step from the raster */
 } SolweigDayConfig;
 int solweig_day_batched_ex(const SolweigScene* scene, const SolweigSkyLayout* layout,
                            const SolweigHour* hours, int nhours, const SolweigState* state,
@@ -343,8 +343,7 @@ int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout*
  * writes [2H][px]: sky plus 0.03 x vegetation sums of luminance and
  * luminance*cos*omega per hour), weights f32 [2H][160], BF16 operands (hi/lo
  * of the weights and of 0.03 x the weights), per-hour tables, error flag,
- * per-hour GVF input ranges [3][H]
- * (ordered-int min Lup, max Lup, max albedo*shadow), total size:
+ * 16x16 tile maxima of the heights (window sweep), total size:
  * offsets[0..10]. */
 int solweig_day_batched_layout(int rows, int cols, int nhours, int has_water, int64_t* offsets);
 /* Copy the device error flag of the last batched day in `work` to out_device:

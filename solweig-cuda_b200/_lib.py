@@ -106,7 +106,7 @@ class SolweigDayConfig(ctypes.Structure):
 
     @classmethod
     def default(cls):
-        return cls(32, 8, 8, 256, 0, 2, 0, 1)
+        return cls(16, 16, 8, 256, 0, 1, 0, 0)
 
 
 EXPORTED_SYMBOLS = (

@@ -100,11 +100,13 @@ class BatchedDay:
 def day_launches(scene, config, sweep_parts=1):
     """Kernel launches of one batched day for this scene and launch shapes,
     with the sweep stage issued in ``sweep_parts`` hour ranges: per range the
-    ray exits, the ceilings and the sweep; once the height dilation; then the
-    GVF (the hour-vectorized kernel or the per-hour one), weights, two
-    splits (sky and vegetation weights), tables, contraction and radiation."""
+    ray exits, the ceilings and the sweep; once the height dilation (and the
+    tile maxima of the window sweep); then the GVF (the hour-vectorized
+    kernel or the per-hour one), weights, two splits (sky and vegetation
+    weights), tables, contraction and radiation."""
     c = int(not config.no_ceiling)
-    return sweep_parts * (2 + c) + c + 7
+    win = int(config.sweep_window != 0 and scene.geo32 is not None and not scene.struct.has_water)
+    return sweep_parts * (2 + c) + c + win + 7
 
 
 class ChosenDay(BatchedDay):
@@ -296,7 +298,7 @@ class ChosenDay(BatchedDay):
         self.buffers.mark()
         return dict(zip(self.STAGES, (float(x) for x in ms)))
 
-    WORK_FIELDS = ("quads", "lup_first", "gvf", "nosh", "sums", "wf32", "bw", "tables", "error", "bounds",
+    WORK_FIELDS = ("quads", "lup_first", "gvf", "nosh", "sums", "wf32", "bw", "tables", "error", "tilemax",
                    "total")
 
     def work_offsets(self):

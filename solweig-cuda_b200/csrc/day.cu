@@ -55,7 +55,7 @@ extern "C" int solweig_day_batched_layout(int rows, int cols, int nhours, int ha
     SOLWEIG_CHECK_ARG(offsets && rows > 0 && cols > 0 && nhours > 0, "solweig_day_batched_layout: bad arguments");
     const DayWork w = day_work_layout((long long)rows * cols, nhours, has_water != 0);
     const long long v[11] = {w.quads, w.lup_first, w.gvf, w.nosh, w.sums, w.wf32, w.bw, w.tables, w.error,
-                             w.bounds, w.total};
+                             w.tilemax, w.total};
     for (int i = 0; i < 11; ++i) offsets[i] = v[i];
     return SOLWEIG_OK;
 }
@@ -94,7 +94,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
                      const int32_t* gvf_dxdy, int first_steps, int second_steps, void* work,
                      int64_t work_bytes, void* stream, cudaEvent_t* ev, const SolweigDayConfig* cfg_in,
                      int part = kDayAll, int h0 = 0, int h1 = -1) {
-    SolweigDayConfig cfg{32, 8, 8, 256, 0, 2, 0, 1};
+    SolweigDayConfig cfg{16, 16, 8, 256, 0, 1, 0, 0};
     if (cfg_in) cfg = *cfg_in;
     SOLWEIG_CHECK_ARG(cfg.shadow_bx > 0 && cfg.shadow_by > 0 && cfg.shadow_bx * cfg.shadow_by <= 256 &&
                           (cfg.shadow_bx * cfg.shadow_by) % 32 == 0,
@@ -106,10 +106,10 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
                       "solweig_day_batched: rad_threads must be 128 or 256");
     SOLWEIG_CHECK_ARG(cfg.gemm_ctas_per_sm >= 0 && cfg.gemm_ctas_per_sm <= 2,
                       "solweig_day_batched: gemm_ctas_per_sm must be 0 (auto), 1 or 2");
-    SOLWEIG_CHECK_ARG(cfg.gvf_hours >= 0 && cfg.gvf_hours <= 2, "solweig_day_batched: gvf_hours must be 0, 1 or 2");
+    SOLWEIG_CHECK_ARG(cfg.gvf_hours == 0 || cfg.gvf_hours == 1, "solweig_day_batched: gvf_hours must be 0 or 1");
     SOLWEIG_CHECK_ARG(cfg.no_ceiling == 0 || cfg.no_ceiling == 1, "solweig_day_batched: no_ceiling must be 0 or 1");
-    SOLWEIG_CHECK_ARG(cfg.sweep_window == 0 || cfg.sweep_window == 1,
-                      "solweig_day_batched: sweep_window must be 0 or 1");
+    SOLWEIG_CHECK_ARG(cfg.sweep_window >= 0 && cfg.sweep_window <= 2,
+                      "solweig_day_batched: sweep_window must be 0, 1 or 2");
     SOLWEIG_CHECK_ARG(scene && layout && hours && base && work, "solweig_day_batched: null argument");
     const SolweigScene& S = *scene;
     SOLWEIG_CHECK_ARG(S.rows > 0 && S.cols > 0, "solweig_day_batched: bad scene shape %dx%d", S.rows, S.cols);
@@ -138,9 +138,9 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     __nv_bfloat16* bw = reinterpret_cast<__nv_bfloat16*>(wb + w.bw);
     DayTable* tables = reinterpret_cast<DayTable*>(wb + w.tables);
     int* err = reinterpret_cast<int*>(wb + w.error);
-    uint32_t* bounds = reinterpret_cast<uint32_t*>(wb + w.bounds);
-    // the fixed-point GVF (gvf_hours = 2) needs the per-hour ranges the sweep reduces
-    const bool hv8 = cfg.gvf_hours == 2 && !S.has_water && first_steps == 1 && second_steps == 22;
+    float* tmax = reinterpret_cast<float*>(wb + w.tilemax);
+    // the window sweep: packed geometry (16-byte aligned for the tensor map), no water
+    const bool window = cfg.sweep_window != 0 && S.geo32 && !S.has_water && ((uintptr_t)S.geo32 & 15) == 0;
     cudaStream_t st = as_stream(stream);
 
     DayGvfArgs ga{first_steps, second_steps, second_steps - 1};
@@ -177,9 +177,10 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
         float* dil = sums;
         if (h0 == 0) {
             cudaMemsetAsync(err, 0, sizeof(int), st);  // the day's error flag
-            if (hv8) {  // per-hour ranges: min <- all ones, max <- 0
-                cudaMemsetAsync(bounds, 0xff, 4LL * nhours, st);
-                cudaMemsetAsync(bounds + nhours, 0, 8LL * nhours, st);
+            if (window) {  // 16 x 16 tile maxima of the heights, for the warp vote
+                const long long ntiles = (long long)sweep_tiles_along(S.rows) * sweep_tiles_along(S.cols);
+                sweep_tile_max_kernel<<<blocks_for(ntiles, 8), 256, 0, st>>>(S, tmax);
+                SOLWEIG_CHECK_LAUNCH("sweep_tile_max_kernel");
             }
         }
         if (ceiling && h0 == 0) {
@@ -199,23 +200,29 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
         int* exits = reinterpret_cast<int*>(wb + w.gvf + 4LL * px * nhours) + (long long)h0 * (S.rows + S.cols);
         day_ray_exits_kernel<<<nh, 1024, 0, st>>>(S, hours + h0, exits);
         SOLWEIG_CHECK_LAUNCH("day_ray_exits_kernel");
-        if (cfg.sweep_window && S.geo32 && !S.has_water && ((uintptr_t)S.geo32 & 15) == 0) {
+        if (window) {
+            const int win = cfg.sweep_window == 2 ? 40 : 48;
             CUtensorMap map;
-            const int rc = sweep_geo_map(S, &map);
+            const int rc = sweep_geo_map(S, win, &map);
             if (rc) return rc;
-            const size_t smem = sweep_smem_bytes();
-            set_smem_attr((const void*)day_sweep_tma_kernel, smem);
             dim3 grid(blocks_for(S.cols, kSwTile), blocks_for(S.rows, kSwTile), nh);
-            day_sweep_tma_kernel<<<grid, kSwThreads, smem, st>>>(map, S, hours + h0, quads + h0 * px,
-                                                                 ceiling ? ceiling + h0 * px : nullptr, exits, err,
-                                                                 hv8 ? bounds : nullptr, nhours, h0);
+            const float* ceil0 = ceiling ? ceiling + h0 * px : nullptr;
+            if (win == 40) {
+                set_smem_attr((const void*)day_sweep_tma_kernel<40>, sweep_smem_bytes<40>());
+                day_sweep_tma_kernel<40><<<grid, kSwThreads, sweep_smem_bytes<40>(), st>>>(
+                    map, S, hours + h0, quads + h0 * px, ceil0, exits, tmax, err);
+            } else {
+                set_smem_attr((const void*)day_sweep_tma_kernel<48>, sweep_smem_bytes<48>());
+                day_sweep_tma_kernel<48><<<grid, kSwThreads, sweep_smem_bytes<48>(), st>>>(
+                    map, S, hours + h0, quads + h0 * px, ceil0, exits, tmax, err);
+            }
             SOLWEIG_CHECK_LAUNCH("day_sweep_tma_kernel");
             return SOLWEIG_OK;
         }
         dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nh);
         day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(
             S, hours + h0, quads + h0 * px, lup_first ? lup_first + h0 * px : nullptr,
-            ceiling ? ceiling + h0 * px : nullptr, exits, hv8 ? bounds : nullptr, nhours, h0);
+            ceiling ? ceiling + h0 * px : nullptr, exits);
         SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
         return SOLWEIG_OK;
     }
@@ -225,14 +232,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
         GvfTable<22> tab;
         fill_day_table(tab, gvf_dxdy, 22, pitch);
         const bool hv = cfg.gvf_hours == 1 && !S.has_water;
-        if (hv8) {
-            const size_t smem = hv_smem_bytes();
-            set_smem_attr((const void*)day_gvf_hv8_kernel, smem);
-            dim3 grid(blocks_for(S.cols, kHvTile), blocks_for(S.rows, kHvTile));
-            day_gvf_hv8_kernel<<<grid, dim3(kHvTile, kHvTile), smem, st>>>(S, hours, nhours, tab, quads, bounds, gvf,
-                                                                          nosh);
-            SOLWEIG_CHECK_LAUNCH("day_gvf_hv8_kernel");
-        } else if (!hv) {
+        if (!hv) {
             launch_day_gvf<1, 22, 22>(cfg.gvf_rows, S, hours, nhours, ga, tab, quads, lup_first, gvf, nosh, st);
         } else {
             const size_t smem = hv_smem_bytes();

@@ -180,8 +180,7 @@ __global__ void __launch_bounds__(256, 8) day_shadow_kernel(SolweigScene S,
                                                                    float4* __restrict__ quads,
                                                                    float* __restrict__ lup_first,
                                                                    const float* __restrict__ ceiling,
-                                                                   const int* __restrict__ exits,
-                                                                   uint32_t* __restrict__ bounds, int nhours, int h0) {
+                                                                   const int* __restrict__ exits) {
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
@@ -189,12 +188,10 @@ __global__ void __launch_bounds__(256, 8) day_shadow_kernel(SolweigScene S,
     warp_tile_pixel(blockDim.x, blockDim.y, r, c);
     const bool in = r < S.rows && c < S.cols;
     const long long n = (long long)S.rows * S.cols;
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (in)
-        q = shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
-                              ceiling ? ceiling + z * n : nullptr,
-                              exits ? exits + (long long)z * (S.rows + S.cols) : nullptr);
-    if (bounds) gvf_bounds_reduce(in && (__float_as_int(q.w) & kQuadGround), q.y, q.z * q.x, bounds, nhours, h0 + z);
+    if (!in) return;
+    shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
+                      ceiling ? ceiling + z * n : nullptr,
+                      exits ? exits + (long long)z * (S.rows + S.cols) : nullptr);
 }
 
 // Per daytime hour, the first-outside step of every row and column of the
@@ -559,277 +556,6 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
     }
 }
 
-// Hour-vectorized GVF with 8 daytime hours per shared-memory pass, the hour
-// values as 16-bit fixed point.  Per cell and hour one 32-bit word holds
-// (Lup - Lmin_h) * sL_h in its high half and albedo*shadow * sA_h in its low
-// half, both rounded to integers in [0, kGvfQMax]; the walk sums the words
-// with plain integer adds: 22 * kGvfQMax < 2^16, so the low half never
-// carries into the high one.  Lmin_h / Lmax_h and the largest
-// albedo*shadow of each hour come from the sweep (over ground pixels, the
-// only ones a walk sums), so the scales follow each hour's range:
-// quantisation error <= range / (2 kGvfQMax) per sample (~0.034 W/m2 for a
-// 200 W/m2 Lup range).  Per sample two 16-byte shared loads and 8 integer
-// adds serve 8 hours (the float kernel above: the same loads and 8 float
-// adds for 4 hours), and a 16-hour day takes 2 passes instead of 4.
-//
-// The own pixel is step 0 of every direction, so the first-ring terms
-// (lup1, alb1: FIRST = 1) are the same in all 18 directions and use the
-// pixel's exact float values; the second-ring sums are the dequantised
-// word sums.  Walk lengths, sunlit-wall first steps, the frozen tails of
-// border tiles and the albedo-without-shadow plane follow day_gvf_hv_kernel.
-constexpr int kHv8 = 8;
-constexpr uint32_t kGvfQMax = 2978;
-static_assert(22u * kGvfQMax < 65536u, "a 22-step sum of the low half must not carry");
-
-__global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv8_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
-                                                                   int nhours, GvfTable<22> tab,
-                                                                   const float4* __restrict__ quads,
-                                                                   const uint32_t* __restrict__ bounds,
-                                                                   float* __restrict__ gvf, float* __restrict__ nosh) {
-    constexpr int FIRST = 1, SECOND = 22;
-    static_assert(FIRST == 1, "the first ring is the own pixel only");
-    const int tr = blockIdx.y, tc = blockIdx.x;
-    const bool interior = hv_tile_interior(S.rows, S.cols, tr, tc);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint4* PA = reinterpret_cast<uint4*>(smem_raw);  // packed words of pass hours 0..3
-    uint4* PB = PA + kHvN;                          // pass hours 4..7
-    uint32_t* bits = reinterpret_cast<uint32_t*>(PB + kHvN);  // bit0 ground, bits 1..8 sunlit wall
-    float* albs = reinterpret_cast<float*>(bits + kHvN);      // albedo, then the walk lengths
-    int* dayh = reinterpret_cast<int*>(albs + kHvN);          // daytime hour indices
-    __shared__ int nday;
-    __shared__ float qs[4][kHv8];  // per pass hour: Lmin, 1/sL, 1/sA, wall Lup
-    const int tid = threadIdx.y * kHvTile + threadIdx.x;
-    const long long n = (long long)S.rows * S.cols;
-    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
-    if (tid == 0) {
-        int k = 0;
-        for (int h = 0; h < nhours && k < 64; ++h)
-            if (hours[h].daytime) dayh[k++] = h;
-        nday = k;
-    }
-    __syncthreads();
-    const int nd = nday;
-    if (nd == 0) return;
-    {
-        const float4* q0 = quads + (long long)dayh[0] * n;
-        for (int i = tid; i < kHvN; i += kHvThreads) {
-            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
-            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
-            const float4 q = in ? q0[(long long)rr * S.cols + cc] : make_float4(0.f, 0.f, 0.f, 0.f);
-            bits[i] = (uint32_t)__float_as_int(q.w) & kQuadGround;
-            albs[i] = q.z;
-        }
-    }
-    __syncthreads();
-    const int lw_ = tid >> 5, ll = tid & 31;
-    const int tx = (lw_ & 3) * 8 + (ll & 7), ty = (lw_ >> 2) * 4 + (ll >> 3);
-    const int r = tr * kHvTile + ty, c = tc * kHvTile + tx;
-    const bool valid = r < S.rows && c < S.cols;
-    const long long p = valid ? (long long)r * S.cols + c : 0;
-    const int own = (ty + kHvHalo) * kHvPitch + tx + kHvHalo;
-    const bool own_ground = valid && (bits[own] & 1u) != 0;
-    const float ob = own_ground ? 1.f : 0.f;
-    const uint32_t face = valid ? S.gvf_face[p] : 0u;
-    constexpr float albedo_b = 0.2f;
-    constexpr float inv_first = 1.f / FIRST, inv_first1 = 1.f / (FIRST + 1);
-    constexpr float inv_second = 1.f / SECOND, inv_second1 = 1.f / (SECOND + 1);
-    uint32_t hits[4] = {0u, 0u, 0u, 0u};
-    float nsh = 0.f;
-    for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
-        int hit = 0, lim = 0;
-        float s_alb = 0.f, n_alb = 0.f;
-        if (own_ground) {
-            hit = lim = SECOND;
-            for (int m = 0; m < SECOND; ++m) {
-                if (!interior) {
-                    const int2 o = tab.offs[j * SECOND + m];
-                    if (!in_raster(r + o.x, c + o.y, S.rows, S.cols)) {
-                        if (m == 0) {
-                            hit = lim = 0;
-                        } else {  // frozen tail: step m and the rest repeat step m - 1
-                            lim = m;
-                            const float al = albs[own + tab.delta[j * SECOND + m - 1]];
-                            s_alb += al;
-                            s_alb += (SECOND - 1 - m) * al;
-                        }
-                        break;
-                    }
-                }
-                const int off = own + tab.delta[j * SECOND + m];
-                if (!(bits[off] & 1u)) {
-                    hit = lim = m;
-                    break;
-                }
-                s_alb += albs[off];
-                if (m + 1 == FIRST) n_alb = s_alb;
-            }
-        }
-        hits[j / 5] |= ((uint32_t)lim | (hit > lim ? 32u : 0u)) << (6 * (j % 5));
-        const int n_wall = SECOND - hit;
-        const int n_wall_first = FIRST > hit ? FIRST - hit : 0;
-        const float nosh1 = n_wall_first > 0 ? ((float)n_wall_first * albedo_b + n_alb) * inv_first1 : n_alb * inv_first;
-        const float nosh2 = n_wall > 0 ? ((float)n_wall * albedo_b + s_alb) * inv_second : s_alb * inv_second;
-        nsh += (nosh1 * 0.5f + nosh2 * 0.4f) * (1.f / 0.9f);
-    }
-    nsh *= ob;
-    nsh += 18.f * (albs[own] * (1.f - ob));
-    if (valid) nosh[p] = nsh / 18.f;
-    // the albedo array is not read again: it holds each thread's walk lengths
-    // from here on (4 words per thread), which frees their registers
-    __syncthreads();
-    uint32_t* hits_sm = reinterpret_cast<uint32_t*>(albs) + 4 * tid;
-    static_assert(4 * kHvThreads <= kHvN, "walk lengths must fit in the albedo array");
-#pragma unroll
-    for (int i = 0; i < 4; ++i) hits_sm[i] = hits[i];
-
-    for (int g0 = 0; g0 < nd; g0 += kHv8) {
-        const int nc = nd - g0 < kHv8 ? nd - g0 : kHv8;
-        __syncthreads();  // the previous pass no longer reads the tile or qs
-        if (tid < kHv8) {
-            float lmin = 0.f, il = 0.f, ia = 0.f, lw = 0.f;
-            if (tid < nc) {
-                const int h = dayh[g0 + tid];
-                if (bounds[nhours + h] != 0u) {  // the hour has ground pixels
-                    const float lo = ord2f(bounds[h]), hi = ord2f(bounds[nhours + h]);
-                    const float am = ord2f(bounds[2 * nhours + h]);
-                    lmin = lo;
-                    il = hi > lo ? (hi - lo) / (float)kGvfQMax : 0.f;
-                    ia = am > 0.f ? am / (float)kGvfQMax : 0.f;
-                }
-                const SolweigHour& hh = hours[h];
-                lw = (float)(kSBC * 0.9 * pow4(hh.tgwall + hh.ta + 273.15) - kSBC * 0.9 * pow4(hh.ta + 273.15));
-            }
-            qs[0][tid] = lmin;
-            qs[1][tid] = il;
-            qs[2][tid] = ia;
-            qs[3][tid] = lw;
-        }
-        __syncthreads();
-        for (int i = tid; i < kHvN; i += kHvThreads) {
-            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
-            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
-            const long long pix = in ? (long long)rr * S.cols + cc : 0;
-            uint32_t b = bits[i] & 1u;
-#pragma unroll
-            for (int half = 0; half < 2; ++half) {  // 4 hours at a time: fewer live registers
-                uint32_t wv[4];
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const int k = 4 * half + kk;
-                    wv[kk] = 0u;
-                    if (k < nc && in) {
-                        const float4 q = quads[(long long)dayh[g0 + k] * n + pix];
-                        const float sl = qs[1][k] > 0.f ? 1.f / qs[1][k] : 0.f;
-                        const float sa = qs[2][k] > 0.f ? 1.f / qs[2][k] : 0.f;
-                        const float lq = fminf(fmaxf(rintf((q.y - qs[0][k]) * sl), 0.f), (float)kGvfQMax);
-                        const float aq = fminf(fmaxf(rintf(q.z * q.x * sa), 0.f), (float)kGvfQMax);
-                        wv[kk] = ((uint32_t)lq << 16) | (uint32_t)aq;
-                        b |= (((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u) << (1 + k);
-                    }
-                }
-                (half ? PB : PA)[i] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-            }
-            bits[i] = b;
-        }
-        __syncthreads();
-        float lup_t[kHv8], alb_t[kHv8];
-#pragma unroll
-        for (int k = 0; k < kHv8; ++k) lup_t[k] = alb_t[k] = 0.f;
-        if (own_ground) {
-#pragma unroll 1
-            for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
-                const uint32_t code = (hits_sm[j / 5] >> (6 * (j % 5))) & 63u;
-                const int lim = (int)(code & 31u);
-                const int hit = (code & 32u) ? SECOND : lim;
-                uint32_t acc[kHv8];
-#pragma unroll
-                for (int k = 0; k < kHv8; ++k) acc[k] = 0u;
-                uint32_t seen = 0u;
-#pragma unroll
-                for (int m = 0; m < SECOND; ++m) {
-                    if (m < lim) {
-                        const int off = own + tab.delta[j * SECOND + m];
-                        const uint4 A = PA[off], B = PB[off];
-                        seen |= bits[off];
-                        acc[0] += A.x; acc[1] += A.y; acc[2] += A.z; acc[3] += A.w;
-                        acc[4] += B.x; acc[5] += B.y; acc[6] += B.z; acc[7] += B.w;
-                    }
-                }
-                // first step of each hour's sunlit-wall bit (5 bits per hour, 31 =
-                // never); sunlit walls are rare, so they are located by a second,
-                // short scan only when the walk met one
-                unsigned long long first_pk = ~0ull;
-                seen = (seen >> 1) & 0xFFu;
-                if (seen) {
-                    uint32_t pending = seen;
-                    for (int m = 0; m < lim && pending; ++m) {
-                        const uint32_t nb = (bits[own + tab.delta[j * SECOND + m]] >> 1) & pending;
-                        for (uint32_t t = nb; t; t &= t - 1) {
-                            const int k = __ffs(t) - 1;
-                            first_pk = (first_pk & ~(31ull << (5 * k))) | ((unsigned long long)m << (5 * k));
-                        }
-                        pending &= ~nb;
-                    }
-                }
-                // frozen tail (border tiles): step lim and the rest repeat step lim - 1
-                const float rest = (float)(SECOND - lim);
-                const uint32_t* lastw = nullptr;
-                if (hit > lim) lastw = reinterpret_cast<const uint32_t*>(&PA[own + tab.delta[j * SECOND + lim - 1]]);
-                const bool fj = (face >> j) & 1u;
-#pragma unroll
-                for (int k = 0; k < kHv8; ++k) {
-                    float sl = (float)(acc[k] >> 16) * qs[1][k] + (float)lim * qs[0][k];
-                    float sa = (float)(acc[k] & 0xFFFFu) * qs[2][k];
-                    if (lastw != nullptr) {
-                        // PB[last] lies kHvN uint4 (4 kHvN words) past PA[last]
-                        const uint32_t wk = k < 4 ? lastw[k] : lastw[4 * kHvN + (k - 4)];
-                        sl = fmaf(rest, (float)(wk >> 16) * qs[1][k] + qs[0][k], sl);
-                        sa = fmaf(rest, (float)(wk & 0xFFFFu) * qs[2][k], sa);
-                    }
-                    const int f = (int)((first_pk >> (5 * k)) & 31ull);
-                    const int n_sun = f < hit ? SECOND - f : 0;
-                    const float s_wall = (float)n_sun;
-                    float s_lwall = s_wall * qs[3][k], s_albwall = s_wall * albedo_b;
-                    if (n_sun == SECOND && fj) {
-                        s_lwall = 0.f;
-                        s_albwall = 0.f;
-                    }
-                    const bool sun_far = n_sun > 0;
-                    const float lup2 = sun_far ? (s_lwall + sl) * inv_second1 : sl * inv_second;
-                    const float alb2 = sun_far ? (s_albwall + sa) * inv_second1 : sa * inv_second;
-                    lup_t[k] += lup2 * (0.4f / 0.9f);
-                    alb_t[k] += alb2 * (0.4f / 0.9f);
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kHv8; ++k) {
-            if (k < nc && valid) {
-                const int h = dayh[g0 + k];
-                const SolweigHour& hh = hours[h];
-                const float4 oq = quads[(long long)h * n + p];
-                const float own_lup = oq.y, own_albsh = oq.z * oq.x;
-                // first ring (the own pixel, step 0 of all 18 directions): a sunlit
-                // wall is seen there iff the own pixel carries the bit
-                const bool own_sun = ((uint32_t)__float_as_int(oq.w) & kQuadSunwall) != 0;
-                float lt = lup_t[k], at = alb_t[k];
-                if (own_ground) {
-                    const float lup1 = own_sun ? (qs[3][k] + own_lup) * inv_first1 : own_lup * inv_first;
-                    const float alb1 = own_sun ? (albedo_b + own_albsh) * inv_first1 : own_albsh * inv_first;
-                    lt += 18.f * (lup1 * (0.5f / 0.9f));
-                    at += 18.f * (alb1 * (0.5f / 0.9f));
-                }
-                lt += 18.f * (own_lup * (1.f - ob));
-                at += 18.f * (own_albsh * (1.f - ob));
-                const double ambient = kSBC * (double)S.emis[p] * pow4(hh.ta + 273.15);
-                gvf[(3LL * h) * n + p] = (float)((double)(lt / 18.f) + ambient);
-                gvf[(3LL * h + 1) * n + p] = at / 18.f;
-                gvf[(3LL * h + 2) * n + p] = oq.x;
-            }
-        }
-    }
-}
-
 // ------------------------------------------------------------- kernels 3, 4, 5
 
 // w[2h][k] = luminance, w[2h+1][k] = luminance * cos(alt) * omega (0 at night).
@@ -1171,10 +897,6 @@ __device__ __forceinline__ float wedge_fsh_f(float ta, float tan_zen) {
 template <int OPT, int THREADS>
 __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(SolweigScene S, DayRadArgs a) {
     __shared__ float wcos[SOLWEIG_MAX_BANDS], wsin[SOLWEIG_MAX_BANDS];
-    // per-pixel statics of the day, one column per thread: read back every
-    // hour from shared memory instead of living in (spilled) registers
-    constexpr int kStat = 18;
-    __shared__ uint32_t stat[kStat][THREADS];
     const SolweigSkyLayout& L = *a.layout;
     if (threadIdx.x < SOLWEIG_MAX_BANDS) {
         const int b = threadIdx.x;
@@ -1182,6 +904,7 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
         wcos[b] = b < L.nbands ? L.omega[k0] * L.cos_alt[k0] : 0.f;
         wsin[b] = b < L.nbands ? L.omega[k0] * L.sin_alt[k0] : 0.f;
     }
+    __syncthreads();  // wcos, wsin
     const long long n = (long long)S.rows * S.cols;
     const long long p = (long long)blockIdx.x * THREADS + threadIdx.x;
     const bool in = p < n;
@@ -1190,39 +913,33 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
     const bool need_tg = o.tg || o.tg_out || a.state.tgout1;
 
     // --- per-pixel static data, loaded once for the day
-    {
-        uint32_t* my = &stat[0][threadIdx.x];
+    uint32_t bld[SOLWEIG_MASK_WORDS];
 #pragma unroll
-        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
-            const int nbits = S.patches - 32 * w;
-            const uint32_t valid = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
-            my[w * THREADS] =
-                ~S.masks[(long long)w * n + q] & ~S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + q] & valid;
-        }
-        uint32_t cnt_lo = 0, cnt_hi = 0;  // sky patches per band, 8 bits each
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            cnt_lo |= (uint32_t)S.sky_band_counts[(long long)b * n + q] << (8 * b);
-            cnt_hi |= (uint32_t)(b + 4 < S.nbands ? S.sky_band_counts[(long long)(b + 4) * n + q] : 0) << (8 * b);
-        }
-        const double tan_asvf = S.tan_asvf[q];
-        my[5 * THREADS] = cnt_lo;
-        my[6 * THREADS] = cnt_hi;
-        my[7 * THREADS] = (uint32_t)S.flags[q] | ((uint32_t)tan_bucket(tan_asvf) << 8);
-        my[8 * THREADS] = __float_as_uint(S.emis[q]);
-        my[9 * THREADS] = __float_as_uint(S.svfbuveg[q]);
-        my[10 * THREADS] = __float_as_uint((float)tan(S.svfalfa[q]));
-        my[11 * THREADS] = (uint32_t)__double2loint(tan_asvf);
-        my[12 * THREADS] = (uint32_t)__double2hiint(tan_asvf);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) my[(13 + i) * THREADS] = __float_as_uint(S.veg_sums[i * n + q]);
-        my[17 * THREADS] = __float_as_uint(a.nosh[q]);
+    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+        const int nbits = S.patches - 32 * w;
+        const uint32_t valid = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
+        bld[w] = ~S.masks[(long long)w * n + q] & ~S.masks[(long long)(SOLWEIG_MASK_WORDS + w) * n + q] & valid;
     }
-    __syncthreads();  // wcos, wsin (each thread reads only its own statics)
-    const volatile uint32_t* sv = &stat[0][threadIdx.x];
-    auto statf = [&](int f) { return __uint_as_float(sv[f * THREADS]); };
+    uint32_t cnt_lo = 0, cnt_hi = 0;  // sky patches per band, 8 bits each
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        cnt_lo |= (uint32_t)S.sky_band_counts[(long long)b * n + q] << (8 * b);
+        cnt_hi |= (uint32_t)(b + 4 < S.nbands ? S.sky_band_counts[(long long)(b + 4) * n + q] : 0) << (8 * b);
+    }
+    const uint8_t fl = S.flags[q];
+    const bool ground = fl & 1;
+    const bool water = S.has_water && (fl & 4);
+    const float emis = S.emis[q];
+    const float svfbuveg = S.svfbuveg[q];
+    const float tan_alfa = (float)tan(S.svfalfa[q]);
+    const double tan_asvf = S.tan_asvf[q];
+    const int tbucket = tan_bucket(tan_asvf);
+    const float vc = S.veg_sums[q], vs = S.veg_sums[n + q];
+    const float oc = S.veg_sums[2 * n + q], os = S.veg_sums[3 * n + q];
+    const float g_nosh = a.nosh[q];
     constexpr float ewall = 0.9f, albedo_b = 0.2f;
     constexpr float absK = 0.7f, absL = 0.95f, Fside = 0.22f, Fup = 0.06f, Fcyl = 0.28f;
+    constexpr float dsh_veg = 0.03f;
     constexpr float sbc = (float)kSBC, inv_pi = (float)(1.0 / kPi);
 
     float st_lup = a.state.tgmap1 ? a.state.tgmap1[q] : 0.f;
@@ -1236,53 +953,29 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
         const bool day = h.daytime != 0;
         const float ta = (float)h.ta;
 
-        // building patches: sunlit / shaded split of the hour, weighted per
-        // altitude band (omega cos / omega sin), one mask word at a time
+        // building patches: sunlit / shaded split of the hour
         const DayTable& T = hs;
         const int P = S.patches;
-        const uint32_t flw = sv[7 * THREADS];
-        const int tbucket = (int)(flw >> 8);
-        const double tan_asvf = __hiloint2double((int)sv[12 * THREADS], (int)sv[11 * THREADS]);
         const int isun = count_le_from(T.tsun, P, T.sun_start[tbucket], tan_asvf);
         const int ishd = count_le_from(T.vshade, P, T.shd_start[tbucket], tan_asvf);
-        float lw_sun_c = 0.f, lw_sun_s = 0.f, lw_shd_c = 0.f, lw_shd_s = 0.f, sw_sun = 0.f, sw_shd = 0.f;
+        uint32_t m_sun[SOLWEIG_MASK_WORDS], m_shd[SOLWEIG_MASK_WORDS], m_lsun[SOLWEIG_MASK_WORDS],
+            m_lshd[SOLWEIG_MASK_WORDS];
 #pragma unroll
         for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
-            const uint32_t bw = sv[w * THREADS];
             const uint32_t test = T.test[w];
-            const uint32_t m_sun = bw & T.suf[isun][w];
-            const uint32_t m_shd = bw & T.pre[ishd][w];
-            const uint32_t m_lsun = m_sun & test;
-            const uint32_t m_lshd = bw & (~test | m_shd);
-#pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const int lo = Bands<OPT>::off(b), hi = Bands<OPT>::off(b + 1);
-                const int a0 = lo > w * 32 ? lo : w * 32;
-                const int e0 = hi < w * 32 + 32 ? hi : w * 32 + 32;
-                if (a0 < e0) {
-                    const uint32_t mk = (e0 - a0 == 32) ? 0xffffffffu : (((1u << (e0 - a0)) - 1u) << (a0 - w * 32));
-                    const float c = wcos[b], sn = wsin[b];
-                    const float nls = (float)__popc(m_lsun & mk), nlh = (float)__popc(m_lshd & mk);
-                    lw_sun_c = fmaf(nls, c, lw_sun_c);
-                    lw_sun_s = fmaf(nls, sn, lw_sun_s);
-                    lw_shd_c = fmaf(nlh, c, lw_shd_c);
-                    lw_shd_s = fmaf(nlh, sn, lw_shd_s);
-                    if (day) {
-                        sw_sun = fmaf((float)__popc(m_sun & mk), c, sw_sun);
-                        sw_shd = fmaf((float)__popc(m_shd & mk), c, sw_shd);
-                    }
-                }
-            }
+            m_sun[w] = bld[w] & T.suf[isun][w];
+            m_shd[w] = bld[w] & T.pre[ishd][w];
+            m_lsun[w] = m_sun[w] & test;
+            m_lshd[w] = bld[w] & (~test | m_shd[w]);
         }
+        const float lw_sun_c = band_weighted<OPT>(m_lsun, wcos), lw_sun_s = band_weighted<OPT>(m_lsun, wsin);
+        const float lw_shd_c = band_weighted<OPT>(m_lshd, wcos), lw_shd_s = band_weighted<OPT>(m_lshd, wsin);
         float ld_sky = 0.f, ls_sky = 0.f;
-        {
-            const uint32_t cnt_lo = sv[5 * THREADS], cnt_hi = sv[6 * THREADS];
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const float cnt = (float)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
-                ld_sky = fmaf(hs.band_down[b], cnt, ld_sky);
-                ls_sky = fmaf(hs.band_side[b], cnt, ls_sky);
-            }
+        for (int b = 0; b < 8; ++b) {
+            const float cnt = (float)(((b < 4 ? cnt_lo : cnt_hi) >> (8 * (b & 3))) & 0xFFu);
+            ld_sky = fmaf(hs.band_down[b], cnt, ld_sky);
+            ls_sky = fmaf(hs.band_side[b], cnt, ls_sky);
         }
         const float lw_shade = hs.lw_shade, lw_sun = hs.lw_sun;
 
@@ -1294,11 +987,10 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             const float g_lup = a.gvf[g0];
             const float g_alb = a.gvf[g0 + n];
             shadow = a.gvf[g0 + 2 * n];
-            const float svfbuveg = statf(9);
-            const float fsh = wedge_fsh_f(statf(10), hs.tan_zen);
+            const float fsh = wedge_fsh_f(tan_alfa, hs.tan_zen);
             const float reflected = albedo_b * (1.f - svfbuveg) * (hs.rad_g * (1.f - fsh) + hs.rad_d * fsh);
             const float base_up = hs.rad_d * svfbuveg + reflected;
-            kup_all = g_alb * hs.direct_up + base_up * statf(17);
+            kup_all = g_alb * hs.direct_up + base_up * g_nosh;
             const float prev = h.firstdaytime ? g_lup : st_lup;
             lup_all = g_lup * (1.f - hs.wave_w) + prev * hs.wave_w;
             st_lup = h.wave_update ? lup_all : prev;
@@ -1309,7 +1001,7 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
                                       ((double)S.tmaxlst[q] / 24.0 - h.snup / 24.0)) * kPi / 2.0;
                 double tgd = amp * sin(phase) * h.ci_tgg;
                 if (S.landcover == 1 && tgd < 0.0) tgd = 0.0;
-                if (S.has_water && (flw & 4)) tgd = h.twater - h.ta;
+                if (water) tgd = h.twater - h.ta;
                 tg = (float)tgd;
                 const float cur = tg * shadow + ta;
                 const float prv = h.firstdaytime ? cur : st_tg;
@@ -1324,17 +1016,16 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             kdown = hs.rad_i_sin * shadow + d_rad + reflected;
             kside_i = shadow * hs.rad_i_cos;
             kside_d = hs.rad_ratio * cw;
-            kside = kside_i + kside_d + hs.sw_sun * sw_sun + hs.sw_shade * sw_shd + hs.sw_shade * statf(13);
+            kside = kside_i + kside_d + hs.sw_sun * band_weighted<OPT>(m_sun, wcos) +
+                    hs.sw_shade * band_weighted<OPT>(m_shd, wcos) + hs.sw_shade * vc;
         } else {
-            float lup = statf(8) * hs.night_lup;
-            if (S.landcover == 1 && (flw & 4)) lup = hs.night_lup_water;
+            float lup = emis * hs.night_lup;
+            if (S.landcover == 1 && (fl & 4)) lup = hs.night_lup_water;
             lup_all = lup;
         }
         const float refl = (ld_sky + lup_all) * ((1.f - ewall) * 0.5f * inv_pi);
-        const float ldown =
-            ld_sky + lw_shade * statf(14) + lw_shade * lw_shd_s + lw_sun * lw_sun_s + refl * statf(16);
-        const float lside =
-            ls_sky + lw_shade * statf(13) + lw_shade * lw_shd_c + lw_sun * lw_sun_c + refl * statf(15);
+        const float ldown = ld_sky + lw_shade * vs + lw_shade * lw_shd_s + lw_sun * lw_sun_s + refl * os;
+        const float lside = ls_sky + lw_shade * vc + lw_shade * lw_shd_c + lw_sun * lw_sun_c + refl * oc;
         // E+S+W+N of Kup and Lup are 4x the all-direction values (see the file header).
         const float sstr = absK * (kside * Fcyl + (kdown + kup_all) * Fup + 2.f * kup_all * Fside) +
                            absL * ((ldown + lup_all) * Fup + lside * Fcyl + 2.f * lup_all * Fside);
@@ -1343,8 +1034,8 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             const long long hs_ = a.hour_stride;
             if (o.tmrt) o.tmrt[hr * hs_ + p] = tmrt;
             if (o.utci)
-                o.utci[hr * hs_ + p] = (flw & 1) ? utci_eval(h.utci, (double)tmrt, h.ta, h.utci_valid)
-                                                 : __int_as_float(0x7fc00000);
+                o.utci[hr * hs_ + p] = ground ? utci_eval(h.utci, (double)tmrt, h.ta, h.utci_valid)
+                                              : __int_as_float(0x7fc00000);
             if (o.kdown) o.kdown[hr * hs_ + p] = kdown;
             if (o.kup) o.kup[hr * hs_ + p] = kup_all;
             if (o.ldown) o.ldown[hr * hs_ + p] = ldown;
@@ -1370,7 +1061,7 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
 inline long long align256(long long x) { return (x + 255) & ~255LL; }
 
 struct DayWork {
-    long long quads, lup_first, gvf, nosh, sums, wf32, bw, tables, error, bounds, total;
+    long long quads, lup_first, gvf, nosh, sums, wf32, bw, tables, error, tilemax, total;
 };
 
 DayWork day_work_layout(long long px, int nhours, bool water) {
@@ -1387,7 +1078,9 @@ DayWork day_work_layout(long long px, int nhours, bool water) {
     w.bw = o; o = align256(o + 2LL * 4 * nb * kK);
     w.tables = o; o = align256(o + (long long)sizeof(DayTable) * nhours);
     w.error = o; o = align256(o + 16);
-    w.bounds = o; o = align256(o + 4LL * 3 * nhours);
+    // per 16 x 16 tile maxima of the heights (ceil(rows/16) * ceil(cols/16)
+    // floats, bounded here from the pixel count alone: <= px/256 + (rows + cols)/16 + 1)
+    w.tilemax = o; o = align256(o + 4LL * (px / 256 + (px + 1) / 16 + 4));
     w.total = o;
     return w;
 }

@@ -2,18 +2,21 @@
 //
 // A block sweeps a 16 x 16 pixel tile for one daytime hour.  All rays of the
 // hour leave the tile towards the sun, and their offsets grow monotonically,
-// so the first steps of every walk stay inside a 48 x 48 pixel window that
-// holds the tile in the corner away from the sun.  Thread 0 stages that
-// window of the packed (dsm, canopy, trunk, 0) geometry from HBM into shared
-// memory with one cp.async.bulk.tensor load (a 2-D tensor map over the
-// raster viewed as rows x (4 * cols) float32) completing on an mbarrier,
-// while the block computes the tile's per-pixel statics and the step at
-// which each tile row / column leaves the window.  A walk then takes its
-// samples from shared memory up to that step and from the raster (L1/L2)
-// after it.
+// so the first steps of every walk stay inside a WIN x WIN pixel window that
+// holds the tile in the corner away from the sun (WIN = 48: 32 steps of
+// room, 6 blocks per SM; WIN = 40: 24 steps, 8 blocks per SM).  Thread 0
+// stages that window of the packed (dsm, canopy, trunk, 0) geometry from HBM
+// into shared memory with one cp.async.bulk.tensor load (a 2-D tensor map
+// over the raster viewed as rows x (4 * cols) float32) completing on an
+// mbarrier.  A walk takes its samples from shared memory up to the step at
+// which it leaves the window and from the raster (L1/L2) after it.
 //
-// Warp-vote exit: after the stage, the block reduces the window's maximum
-// height M.  Every 4 steps the lanes of a warp vote (__all_sync) on
+// No block-wide barrier after the start: while the copy is in flight every
+// warp loads its pixels' statics, finds the window exits of its own 8 x 4
+// piece (lane-parallel scans) and the window's maximum height M (from the
+// day's 16 x 16 tile maxima), then waits on the mbarrier itself and walks.
+//
+// Warp-vote exit: every 4 steps the lanes of a warp vote (__all_sync) on
 // M - dz_{k-1} < dsm_p; once it holds for the whole warp, no sample left in
 // the window can change any lane's outputs and the warp jumps to the first
 // step outside the window together.
@@ -21,9 +24,6 @@
 // The per-step recurrences are those of shadow_walk_packed (shadow.cuh), in
 // the same float64 operations: every output is bit-identical.  The raster
 // must carry the packed float32 geometry (SolweigScene::geo32).
-//
-// The kernel also reduces, per hour, the range of the GVF inputs over ground
-// pixels (gvf_bounds_reduce) for the fixed-point GVF of the batched day.
 #pragma once
 #include <cuda.h>
 
@@ -35,61 +35,40 @@ namespace solweig {
 // includes this header instantiates its own copy.
 namespace {
 
-constexpr int kSwTile = 16;              // tile side (pixels)
-constexpr int kSwWin = 48;               // window side (pixels)
+constexpr int kSwTile = 16;  // tile side (pixels); also the tile of the height maxima
 constexpr int kSwThreads = kSwTile * kSwTile;
-constexpr int kSwWinBytes = kSwWin * kSwWin * 16;
-constexpr int kSwScanLimit = 4 * kSwWin;  // window exits are found by a linear scan up to here
+constexpr int kSwScanLimit = 256;  // window exits are found by a linear scan up to here
 constexpr uint32_t kSwWaitPolls = 1u << 22;
 
+template <int WIN>
 struct SweepSmem {
-    float4 win[kSwWin * kSwWin];  // 128-byte aligned at the start of dynamic shared memory
+    float4 win[WIN * WIN];  // 128-byte aligned at the start of dynamic shared memory
     unsigned long long bar;
-    int row_exit[kSwTile], col_exit[kSwTile];
-    float wmax[kSwThreads / 32];
 };
 
-// Order-preserving map of floats to unsigned ints (for atomicMin / atomicMax).
-__device__ __forceinline__ uint32_t f2ord(float f) {
-    const uint32_t u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float ord2f(uint32_t u) {
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
+// Number of 16 x 16 tiles of the height maxima along each axis.
+__host__ __device__ __forceinline__ int sweep_tiles_along(int n) { return (n + kSwTile - 1) / kSwTile; }
 
-// Per-hour ranges of the GVF inputs over ground pixels, reduced by the sweep:
-// b[h] = ordered min Lup, b[H + h] = ordered max Lup, b[2H + h] = ordered max
-// albedo*shadow (0 = no ground pixel yet).  Every thread of the block calls
-// it (valid = it has a daytime ground pixel).
-__device__ __forceinline__ void gvf_bounds_reduce(bool valid, float lup, float albsh, uint32_t* b, int H, int h) {
-    __shared__ uint32_t red[3][32];
-    uint32_t lo = valid ? f2ord(lup) : 0xffffffffu;
-    uint32_t hi = valid ? f2ord(lup) : 0u;
-    uint32_t ah = valid ? f2ord(albsh) : 0u;
-    lo = __reduce_min_sync(0xffffffffu, lo);
-    hi = __reduce_max_sync(0xffffffffu, hi);
-    ah = __reduce_max_sync(0xffffffffu, ah);
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
-    const int w = tid >> 5, nw = (nt + 31) >> 5;
-    if ((tid & 31) == 0) {
-        red[0][w] = lo;
-        red[1][w] = hi;
-        red[2][w] = ah;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int i = 1; i < nw; ++i) {
-            lo = min(lo, red[0][i]);
-            hi = max(hi, red[1][i]);
-            ah = max(ah, red[2][i]);
-        }
-        if (hi != 0u) {  // the block had a ground pixel
-            atomicMin(&b[h], lo);
-            atomicMax(&b[H + h], hi);
-            atomicMax(&b[2 * H + h], ah);
+// Per 16 x 16 tile, the maximum of the three packed heights (dsm, canopy,
+// trunk); one warp per tile row segment, once per day.
+__global__ void __launch_bounds__(256) sweep_tile_max_kernel(SolweigScene S, float* __restrict__ tmax) {
+    const int ntx = sweep_tiles_along(S.cols), nty = sweep_tiles_along(S.rows);
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= ntx * nty) return;
+    const int ty = t / ntx, tx = t - ty * ntx;
+    const float4* geo = reinterpret_cast<const float4*>(S.geo32);
+    float m = 0.f;  // samples outside the raster read as zero
+    for (int i = lane; i < kSwTile * kSwTile; i += 32) {
+        const int r = ty * kSwTile + i / kSwTile, c = tx * kSwTile + i % kSwTile;
+        if (r < S.rows && c < S.cols) {
+            const float4 v = __ldg(&geo[(long long)r * S.cols + c]);
+            m = fmaxf(m, fmaxf(v.x, fmaxf(v.y, v.z)));
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) tmax[t] = m;
 }
 
 __device__ __forceinline__ void sw_mbar_init(unsigned long long* bar) {
@@ -239,10 +218,10 @@ __device__ __forceinline__ ShadowResult shadow_walk_window(
     return s;
 }
 
-// Quad epilogue of shadow_quad_pixel for a walk result (returns the quad).
-__device__ __forceinline__ float4 write_quad(const SolweigScene& S, const SolweigHour& h, long long p, double a,
-                                             double wall, uint8_t fl, const ShadowResult& s,
-                                             float4* __restrict__ quad) {
+// Quad epilogue of shadow_quad_pixel for a walk result.
+__device__ __forceinline__ void write_quad(const SolweigScene& S, const SolweigHour& h, long long p, double a,
+                                           double wall, uint8_t fl, const ShadowResult& s,
+                                           float4* __restrict__ quad) {
     const double wallbol = wall > 0.0 ? 1.0 : 0.0;
     const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);
     double wallsun = wall - (s.f - a);
@@ -261,32 +240,27 @@ __device__ __forceinline__ float4 write_quad(const SolweigScene& S, const Solwei
     const double shadow = (double)(float)(sh - (1.0 - vegsh) * (1.0 - h.psi));
     const double tg = ground_tg(S, h, p);
     const float lup = (float)lup_excess((double)S.emis[p], tg, shadow, h.ta);
-    const float4 q = make_float4((float)shadow, lup, S.alb[p],
-                                 __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
-    quad[p] = q;
-    return q;
+    quad[p] = make_float4((float)shadow, lup, S.alb[p],
+                          __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
 }
 
 // grid (tiles along columns, tiles along rows, hours of the range); kSwThreads
-// threads; dynamic shared memory sweep_smem_bytes().  Scenes with water use
-// the raster sweep kernel (they also need the first direction's Lup).
+// threads; dynamic shared memory sweep_smem_bytes<WIN>().  Scenes with water
+// use the raster sweep kernel (they also need the first direction's Lup).
 // `hours`, `quads`, `ceiling` (planes [hour][px]) and `exits` ([hour][rows +
 // cols]) point at the range's first hour; grid.z indexes the hours of the
-// range.  `bounds` (optional): per-hour GVF input ranges of the day
-// ([3][nhours]) for hour h0 + blockIdx.z.
-__global__ void __launch_bounds__(kSwThreads, 6) day_sweep_tma_kernel(const __grid_constant__ CUtensorMap geo_map,
-                                                                      SolweigScene S,
-                                                                      const SolweigHour* __restrict__ hours,
-                                                                      float4* __restrict__ quads,
-                                                                      const float* __restrict__ ceiling,
-                                                                      const int* __restrict__ exits,
-                                                                      int* __restrict__ error,
-                                                                      uint32_t* __restrict__ bounds, int nhours,
-                                                                      int h0) {
+// range.  `tmax`: the day's 16 x 16 tile maxima (sweep_tile_max_kernel).
+template <int WIN>
+__global__ void __launch_bounds__(kSwThreads, WIN <= 40 ? 8 : 6)
+    day_sweep_tma_kernel(const __grid_constant__ CUtensorMap geo_map, SolweigScene S,
+                         const SolweigHour* __restrict__ hours, float4* __restrict__ quads,
+                         const float* __restrict__ ceiling, const int* __restrict__ exits,
+                         const float* __restrict__ tmax, int* __restrict__ error) {
+    static_assert(WIN >= kSwTile && WIN <= 64, "window side");
     const SolweigHour& h = hours[blockIdx.z];
     if (!h.daytime) return;
     extern __shared__ unsigned char sw_raw[];
-    SweepSmem& sm = *reinterpret_cast<SweepSmem*>(
+    SweepSmem<WIN>& sm = *reinterpret_cast<SweepSmem<WIN>*>(
         (reinterpret_cast<uintptr_t>(sw_raw) + 127) & ~static_cast<uintptr_t>(127));
     const int tid = threadIdx.x;
     const int2* ray = reinterpret_cast<const int2*>(h.ray_dxdy);
@@ -294,84 +268,81 @@ __global__ void __launch_bounds__(kSwThreads, 6) day_sweep_tma_kernel(const __gr
     const int r0 = blockIdx.y * kSwTile, c0 = blockIdx.x * kSwTile;
     // the window holds the tile in its corner away from the sun
     const int2 last = K > 0 ? __ldg(&ray[K - 1]) : make_int2(0, 0);
-    const int wr0 = last.x < 0 ? r0 + kSwTile - kSwWin : r0;
-    const int wc0 = last.y < 0 ? c0 + kSwTile - kSwWin : c0;
+    const int wr0 = last.x < 0 ? r0 + kSwTile - WIN : r0;
+    const int wc0 = last.y < 0 ? c0 + kSwTile - WIN : c0;
     if (tid == 0) sw_mbar_init(&sm.bar);
     __syncthreads();  // the barrier is initialised before anyone polls it
-    if (tid == 0) sw_tma_load(sm.win, &geo_map, 4 * wc0, wr0, &sm.bar, kSwWinBytes);
-    // first step at which each tile row / column leaves the window (linear
-    // scan, capped: a smaller value only moves samples to the raster path)
-    if (tid < 2 * kSwTile) {
-        const bool row = tid < kSwTile;
-        const int i = row ? tid : tid - kSwTile;
-        const int pos = row ? r0 + i - wr0 : c0 + i - wc0;
-        const int lim = K < kSwScanLimit ? K : kSwScanLimit;
-        int k = 0;
-        for (; k < lim; ++k) {
-            const int2 o = __ldg(&ray[k]);
-            const int v = pos + (row ? o.x : o.y);
-            if (v < 0 || v >= kSwWin) break;
-        }
-        (row ? sm.row_exit : sm.col_exit)[i] = k;
-    }
+    if (tid == 0) sw_tma_load(sm.win, &geo_map, 4 * wc0, wr0, &sm.bar, (uint32_t)(WIN * WIN * 16));
+
     // this thread's pixel: warps take 8 x 4 (columns x rows) pieces
     const int w = tid >> 5, l = tid & 31;
-    const int tx = (w & 1) * 8 + (l & 7), ty = (w >> 1) * 4 + (l >> 3);
+    const int tx0 = (w & 1) * 8, ty0 = (w >> 1) * 4;
+    const int tx = tx0 + (l & 7), ty = ty0 + (l >> 3);
     const int r = r0 + ty, c = c0 + tx;
     const bool in = r < S.rows && c < S.cols;
+    const long long npx = (long long)S.rows * S.cols;
     const long long p = in ? (long long)r * S.cols + c : 0;
     const double a = in ? S.dsm[p] : 0.0;
     const double wall = in ? S.walls[p] : 0.0;
     const uint8_t fl = in ? S.flags[p] : 0;
     const double top_p = in ? S.vegdem[p] : 0.0;
-    // this hour's ray exits and ceiling plane (the pointers are those of the
-    // range's first hour)
-    const long long npx = (long long)S.rows * S.cols;
+    // this hour's ray exits and ceiling plane
     const int* ex = exits + (long long)blockIdx.z * (S.rows + S.cols);
     const float* ceil_h = ceiling ? ceiling + (long long)blockIdx.z * npx : nullptr;
     int kend = 0;
     if (in) kend = min(K, min(__ldg(&ex[r]), __ldg(&ex[S.rows + c])));
-    // wait for the window (bounded); on a timeout record the error, wait once
-    // more for the copy in flight and walk from the raster only
-    const bool got = sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
-    if (!got) {
-        if (tid == 0) atomicExch(error, 2);
-        sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
-    }
-    const bool staged = __syncthreads_and(got) != 0;
-    // window maximum of the three heights
-    float m = -__int_as_float(0x7f800000);
-    if (staged) {
-        for (int i = tid; i < kSwWin * kSwWin; i += kSwThreads) {
-            const float4 v = sm.win[i];
-            m = fmaxf(m, fmaxf(v.x, fmaxf(v.y, v.z)));
+
+    // window exits of the piece: lanes 0-3 scan its rows, lanes 4-11 its
+    // columns (linear scans, capped: a smaller value only moves samples to
+    // the raster path)
+    int scan = 0;
+    if (l < 12) {
+        const bool row = l < 4;
+        const int pos = row ? r0 + ty0 + l - wr0 : c0 + tx0 + (l - 4) - wc0;
+        const int lim = K < kSwScanLimit ? K : kSwScanLimit;
+        for (; scan < lim; ++scan) {
+            const int2 o = __ldg(&ray[scan]);
+            const int v = pos + (row ? o.x : o.y);
+            if (v < 0 || v >= WIN) break;
         }
     }
+    const int row_exit = __shfl_sync(0xffffffffu, scan, l >> 3);
+    const int col_exit = __shfl_sync(0xffffffffu, scan, 4 + (l & 7));
+    // the window's maximum height, from the tile maxima it overlaps (tiles
+    // outside the raster count as zero, as the copy fills them)
+    float m = 0.f;
+    {
+        const int ntx = sweep_tiles_along(S.cols), nty = sweep_tiles_along(S.rows);
+        const int ya = wr0 >> 4, yb = (wr0 + WIN - 1) >> 4;  // arithmetic shifts: floor
+        const int xa = wc0 >> 4, xb = (wc0 + WIN - 1) >> 4;
+        const int tyi = ya + (l >> 2), txi = xa + (l & 3);
+        if (l < 16 && tyi <= yb && txi <= xb && tyi >= 0 && tyi < nty && txi >= 0 && txi < ntx)
+            m = __ldg(&tmax[tyi * ntx + txi]);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (l == 0) sm.wmax[w] = m;
-    __syncthreads();
-    m = sm.wmax[0];
-#pragma unroll
-    for (int i = 1; i < kSwThreads / 32; ++i) m = fmaxf(m, sm.wmax[i]);
-    const int kw = staged && in ? min(kend, min(sm.row_exit[ty], sm.col_exit[tx])) : 0;
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    // wait for the window (bounded, every thread); on a timeout record the
+    // error, wait once more for the copy in flight and walk from the raster
+    const bool got = sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
+    if (!got) sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
+    const bool staged = __all_sync(0xffffffffu, got);
+    if (!staged && l == 0) atomicExch(error, 2);
+    const int kw = staged && in ? min(kend, min(row_exit, col_exit)) : 0;
     const double pinf = __longlong_as_double(0x7ff0000000000000ll);
     const double wclear = a >= 0.0 ? nextafter((double)m - a, pinf) : pinf;
-    const ShadowResult s = shadow_walk_window(in, sm.win, kSwWin, (r - wr0) * kSwWin + (c - wc0), kw, wclear,
+    const ShadowResult s = shadow_walk_window(in, sm.win, WIN, (r - wr0) * WIN + (c - wc0), kw, wclear,
                                               reinterpret_cast<const float4*>(S.geo32), S.cols, p, a, top_p,
                                               (fl & 2) != 0, wall, ray, h.ray_dz, K, kend, S.hmax, ceil_h);
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (in) q = write_quad(S, h, p, a, wall, fl, s, quads + (long long)blockIdx.z * npx);
-    if (bounds) gvf_bounds_reduce(in && (fl & 1), q.y, q.z * q.x, bounds, nhours, h0 + blockIdx.z);
+    if (in) write_quad(S, h, p, a, wall, fl, s, quads + (long long)blockIdx.z * npx);
 }
 
 // Tensor map of the packed geometry viewed as a rows x (4 * cols) float32
-// array, box kSwWin rows x 4 * kSwWin floats (one window); elements outside
-// the raster read as zero (the walks never use them: they stop at the raster
+// array, box WIN rows x 4 * WIN floats (one window); elements outside the
+// raster read as zero (the walks never use them: they stop at the raster
 // edge).  The x coordinate of a window is 4 * its first column, so every
 // copy starts on a 16-byte boundary.  The driver's encoder is looked up once
 // through the runtime.
-inline int sweep_geo_map(const SolweigScene& S, CUtensorMap* map) {
+inline int sweep_geo_map(const SolweigScene& S, int win, CUtensorMap* map) {
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -389,7 +360,7 @@ inline int sweep_geo_map(const SolweigScene& S, CUtensorMap* map) {
     SOLWEIG_CHECK_ARG(S.geo32 && ((uintptr_t)S.geo32 & 15) == 0, "day sweep: packed geometry missing or unaligned");
     const cuuint64_t dims[2] = {4ull * (cuuint64_t)S.cols, (cuuint64_t)S.rows};
     const cuuint64_t strides[1] = {16ull * (cuuint64_t)S.cols};
-    const cuuint32_t box[2] = {4u * kSwWin, (cuuint32_t)kSwWin};
+    const cuuint32_t box[2] = {4u * (cuuint32_t)win, (cuuint32_t)win};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(S.geo32), dims, strides,
                               box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -401,7 +372,10 @@ inline int sweep_geo_map(const SolweigScene& S, CUtensorMap* map) {
     return SOLWEIG_OK;
 }
 
-inline size_t sweep_smem_bytes() { return sizeof(SweepSmem) + 128; }
+template <int WIN>
+inline size_t sweep_smem_bytes() {
+    return sizeof(SweepSmem<WIN>) + 128;
+}
 
 }  // namespace
 

@@ -2,18 +2,17 @@
 
 The search space is :class:`_lib.SolweigDayConfig`:
 
-* sweep: the shared-memory window sweep (TMA-staged 48 x 48 windows, fixed
-  16 x 16 tiles), or the raster sweep with a shadow block (columns x rows)
-  of 32x8, 64x4, 16x16, 32x4, 128x2
+* sweep: the shared-memory window sweep (TMA-staged 48 x 48 or 40 x 40
+  windows, fixed 16 x 16 tiles), or the raster sweep with a shadow block
+  (columns x rows) of 32x8, 64x4, 16x16, 32x4, 128x2
 * GVF: tile rows per block of the per-hour kernel: 4, 8, 16 (32 columns,
-  halo of ``second`` - 1), or the hour-vectorized kernels on 32 x 32 tiles
-  (float32 4-hour passes, 16-bit fixed-point 8-hour passes)
+  halo of ``second`` - 1), or the hour-vectorized kernel on 32 x 32 tiles
 * radiation block: 128 or 256 pixels
 * patch-contraction CTAs per SM: 1 or 2
 
 ``solweig_day_batched_timed`` times every stage with CUDA events on the
 launching stream, and each stage's time depends only on its own parameter,
-so the search is one pass per parameter with the others held (6 + 5 + 2 + 2
+so the search is one pass per parameter with the others held (7 + 4 + 2 + 2
 timed days, each repeated and the minimum taken).  Results are cached per
 (device, tile-size bucket, hours, patches) in a JSON file
 (``$SOLWEIG_TUNE_CACHE`` or ``~/.cache/solweig_cuda_b200/autotune.json``),
@@ -35,7 +34,7 @@ __all__ = ["SHADOW_BLOCKS", "GVF_ROWS", "GVF_HOURS", "RAD_THREADS", "GEMM_CTAS",
 
 SHADOW_BLOCKS = ((32, 8), (64, 4), (16, 16), (32, 4), (128, 2))
 GVF_ROWS = (4, 8, 16)
-GVF_HOURS = (0, 1, 2)
+GVF_HOURS = (0, 1)
 RAD_THREADS = (128, 256)
 GEMM_CTAS = (1, 2)
 
@@ -57,7 +56,7 @@ def _bucket(n):
 def tune_key(runner):
     sc = runner.scene
     name = torch.cuda.get_device_name(sc.device)
-    return f"v4|{name}|{_bucket(sc.rows)}x{_bucket(sc.cols)}|h{runner.hours}|p{sc.struct.patches}"
+    return f"v5|{name}|{_bucket(sc.rows)}x{_bucket(sc.cols)}|h{runner.hours}|p{sc.struct.patches}"
 
 
 def _load():
@@ -136,7 +135,8 @@ def tune(runner, met, repeats=2, use_cache=True):
     def set_gemm(c, v):
         c[4] = v
 
-    pick("day_shadow_kernel", [(cfg[0], cfg[1], 1)] + [(bx, by, 0) for bx, by in SHADOW_BLOCKS], set_shadow)
+    pick("day_shadow_kernel", [(cfg[0], cfg[1], w) for w in (1, 2)] + [(bx, by, 0) for bx, by in SHADOW_BLOCKS],
+         set_shadow)
     pick("day_gvf_kernel", [(cfg[2], h) for h in GVF_HOURS if h] + [(r, 0) for r in GVF_ROWS], set_gvf)
     pick("day_radiation_kernel", RAD_THREADS, set_rad)
     pick("patch_gemm_kernel", GEMM_CTAS, set_gemm)
