@@ -310,9 +310,7 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
 // once; then per pass of kHvCh daytime hours the tile is staged as
 // (Lup, albedo*shadow) pairs plus the sunlit-wall bits of those hours, and
 // every walked sample is one pair of 16-byte shared loads serving all kHvCh
-// hours; each hour's sunlit-wall bit rides in the lowest mantissa bit of its
-// albedo*shadow value, so the walk ORs four words and looks for the first
-// step of each bit in a second, short scan only when it met a sunlit wall.  The sunlit-wall statistics need only the first step at which each
+// hours.  The sunlit-wall statistics need only the first step at which each
 // hour's bit appears: seen at step f < hit means n_sun = second - f (the
 // steps after a building hit keep counting, as in gvf_direction_fixed).
 // Same recurrences and the same float32 operation order as
@@ -437,21 +435,21 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
             const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
             const long long pix = in ? (long long)rr * S.cols + cc : 0;
             float v[2 * kHvCh];
+            uint32_t b = bits[i] & 1u;
 #pragma unroll
             for (int k = 0; k < kHvCh; ++k) {
                 if (k < nc && in) {
                     const float4 q = quads[(long long)dayh[g0 + k] * n + pix];
                     v[2 * k] = q.y;
-                    // the hour's sunlit-wall bit rides in the lowest mantissa bit of
-                    // albedo*shadow (>= 0, changed by at most one ulp)
-                    const uint32_t sw = ((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u;
-                    v[2 * k + 1] = __uint_as_float((__float_as_uint(q.z * q.x) & ~1u) | sw);
+                    v[2 * k + 1] = q.z * q.x;
+                    b |= (((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u) << (1 + k);
                 } else {
                     v[2 * k] = v[2 * k + 1] = 0.f;
                 }
             }
             LA[i] = make_float4(v[0], v[1], v[2], v[3]);
             LB[i] = make_float4(v[4], v[5], v[6], v[7]);
+            bits[i] = b;
         }
         __syncthreads();
         float lw[kHvCh];
@@ -476,16 +474,22 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                 float sl[kHvCh], sa[kHvCh], l0[kHvCh], a0[kHvCh];
 #pragma unroll
                 for (int k = 0; k < kHvCh; ++k) sl[k] = sa[k] = l0[k] = a0[k] = 0.f;
-                uint32_t any = 0u, first_pk = 0xFFFFFu;  // 5 bits per hour, 31 = never
+                uint32_t seen = 0u, first_pk = 0xFFFFFu;  // 5 bits per hour, 31 = never
 #pragma unroll
                 for (int m = 0; m < SECOND; ++m) {
                     if (m < lim) {
                         const int off = own + tab.delta[j * SECOND + m];
                         const float4 A = LA[off], B = LB[off];
+                        const uint32_t b = (bits[off] >> 1) & 15u;
                         sl[0] += A.x; sa[0] += A.y; sl[1] += A.z; sa[1] += A.w;
                         sl[2] += B.x; sa[2] += B.y; sl[3] += B.z; sa[3] += B.w;
-                        any |= __float_as_uint(A.y) | __float_as_uint(A.w) | __float_as_uint(B.y) |
-                               __float_as_uint(B.w);
+                        const uint32_t nb = b & ~seen;
+                        if (nb) {
+#pragma unroll
+                            for (int k = 0; k < kHvCh; ++k)
+                                if ((nb >> k) & 1u) first_pk = (first_pk & ~(31u << (5 * k))) | ((uint32_t)m << (5 * k));
+                            seen |= b;
+                        }
                         if (m + 1 == FIRST) {
 #pragma unroll
                             for (int k = 0; k < kHvCh; ++k) {
@@ -493,21 +497,6 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                                 a0[k] = sa[k];
                             }
                         }
-                    }
-                }
-                if (any & 1u) {
-                    // the walk met a sunlit wall (rare): the first step of each hour's bit
-                    uint32_t pending = 15u;
-                    for (int m = 0; m < lim && pending; ++m) {
-                        const int off = own + tab.delta[j * SECOND + m];
-                        const float4 A = LA[off], B = LB[off];
-                        const uint32_t b = (__float_as_uint(A.y) & 1u) | ((__float_as_uint(A.w) & 1u) << 1) |
-                                           ((__float_as_uint(B.y) & 1u) << 2) | ((__float_as_uint(B.w) & 1u) << 3);
-                        const uint32_t nb = b & pending;
-#pragma unroll
-                        for (int k = 0; k < kHvCh; ++k)
-                            if ((nb >> k) & 1u) first_pk = (first_pk & ~(31u << (5 * k))) | ((uint32_t)m << (5 * k));
-                        pending &= ~nb;
                     }
                 }
                 if (hit > lim) {
