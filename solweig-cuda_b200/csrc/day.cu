@@ -10,6 +10,9 @@
 //                           day_ray_exits_kernel: first step outside the
 //                           raster of every row and column
 //  1 day_shadow_kernel      grid.z = hour: shadow sweep + GVF field quads
+//                           (day_sweep_tma_kernel with sweep_window = 1 / 2:
+//                           the same sweep on TMA-staged shared-memory windows
+//                           with the warp-vote exit, sweep_tma.cuh)
 //  2 day_gvf_hv_kernel      32 x 32 tiles, every daytime hour per block (4 per
 //                           shared-memory pass): all-direction GVF (Lup,
 //                           albedo) + the pixel's shadow, the hour-independent
@@ -17,14 +20,16 @@
 //                           (day_gvf_kernel, grid.z = hour, for other walk
 //                           lengths and water scenes)
 //  3 day_weights_kernel     per-hour patch weights (luminance, luminance*cos*omega)
-//  4 split_bf16_kernel      weights -> BF16 hi/lo pair in the canonical
-//                           K-major shared-memory layout of the contraction
+//  4 split_bf16_kernel      weights (and 0.03 x the weights) -> BF16 hi/lo
+//                           pairs in the canonical K-major shared-memory
+//                           layout of the contraction
 //  5 day_tables_kernel      per hour: exact thresholds on tan(asvf) for the
 //                           sunlit / shaded split of building patches, sorted,
 //                           with the prefix/suffix patch masks, bucket start
 //                           tables and the hour's flux scalars
-//  6 patch_gemm_kernel      tcgen05: [128 px x 160 patches] 0/1 sky (vegetation)
-//                           masks x [160 x 2H] weights, FP32 in tensor memory
+//  6 patch_gemm_kernel      tcgen05: [128 px x 160 patches] 0/1 sky masks x
+//                           [160 x 2H] weights + vegetation masks x 0.03 x
+//                           weights into one set of FP32 columns in tensor memory
 //  7 day_radiation_kernel   one thread per pixel loops over the hours: wave
 //                           delay state in registers, fluxes, Tmrt, UTCI
 //
