@@ -313,9 +313,10 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
 // hours.  The sunlit-wall statistics need only the first step at which each
 // hour's bit appears: seen at step f < hit means n_sun = second - f (the
 // steps after a building hit keep counting, as in gvf_direction_fixed).
-// Same recurrences and the same float32 operation order as
-// gvf_direction_fixed except albedo*shadow, which is rounded once per sample
-// here instead of fused into the sum.
+// Same recurrences as gvf_direction_fixed and the same float32 sums along
+// the walk, except albedo*shadow, which is rounded once per sample here
+// instead of fused into the sum; the per-direction weights are applied as
+// fused multiply-adds (a few ulp from the per-hour kernel's order).
 //
 // Border tiles (halo reaching outside the raster) stage zeros outside and
 // follow the per-hour walk's edge rule: a walk whose first step leaves the
@@ -323,11 +324,19 @@ __global__ void __launch_bounds__(32 * TY) day_gvf_kernel(SolweigScene S, const 
 // last sample (step L - 1) for the remaining second - L steps and never hits.
 // Per direction the kernel keeps `lim` (samples read) and a frozen-tail bit
 // (then hit = second, else hit = lim): 6 bits, 5 directions per word.
+//
+// Shared memory: the two (Lup, albedo*shadow) float4 planes, one byte per
+// pixel of bits (ground during the walk-length pass, then the pass hours'
+// sunlit-wall bits 0..3) and the daytime hour list; the albedo of the
+// walk-length pass lives in the second float4 plane before the first hour
+// pass overwrites it.  A warp's byte loads (8 x 4 pixels, rows 74 bytes
+// apart) touch distinct banks: one wavefront.
 constexpr int kHvN = kHvPitch * kHvPitch;
 constexpr int kHvCh = 4;
 constexpr int kHvThreads = kHvTile * kHvTile;
+constexpr int kHvBitsBytes = (kHvN + 15) & ~15;
 
-size_t hv_smem_bytes() { return (size_t)kHvN * (2 * sizeof(float4) + 2 * sizeof(uint32_t)) + 64 * sizeof(int); }
+size_t hv_smem_bytes() { return (size_t)kHvN * 2 * sizeof(float4) + kHvBitsBytes + 64 * sizeof(int); }
 
 __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
                                                                   int nhours, GvfTable<22> tab,
@@ -339,9 +348,9 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* LA = reinterpret_cast<float4*>(smem_raw);  // Lup, albsh of pass hours 0, 1
     float4* LB = LA + kHvN;                            // pass hours 2, 3
-    uint32_t* bits = reinterpret_cast<uint32_t*>(LB + kHvN);  // bit0 ground, bits 1..4 sunlit wall
-    float* albs = reinterpret_cast<float*>(bits + kHvN);      // albedo
-    int* dayh = reinterpret_cast<int*>(albs + kHvN);          // daytime hour indices
+    uint8_t* bits = reinterpret_cast<uint8_t*>(LB + kHvN);    // ground bit, then sunlit-wall bits
+    float* albs = reinterpret_cast<float*>(LB);                // albedo (walk-length pass only)
+    int* dayh = reinterpret_cast<int*>(bits + kHvBitsBytes);   // daytime hour indices
     __shared__ int nday;
     const int tid = threadIdx.y * kHvTile + threadIdx.x;
     const long long n = (long long)S.rows * S.cols;
@@ -361,7 +370,7 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
             const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
             const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
             const float4 q = in ? q0[(long long)rr * S.cols + cc] : make_float4(0.f, 0.f, 0.f, 0.f);
-            bits[i] = (uint32_t)__float_as_int(q.w) & kQuadGround;
+            bits[i] = (uint8_t)(__float_as_int(q.w) & kQuadGround);
             albs[i] = q.z;
         }
     }
@@ -435,21 +444,21 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
             const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
             const long long pix = in ? (long long)rr * S.cols + cc : 0;
             float v[2 * kHvCh];
-            uint32_t b = bits[i] & 1u;
+            uint32_t b = 0u;
 #pragma unroll
             for (int k = 0; k < kHvCh; ++k) {
                 if (k < nc && in) {
                     const float4 q = quads[(long long)dayh[g0 + k] * n + pix];
                     v[2 * k] = q.y;
                     v[2 * k + 1] = q.z * q.x;
-                    b |= (((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u) << (1 + k);
+                    b |= (((uint32_t)__float_as_int(q.w) & kQuadSunwall) ? 1u : 0u) << k;
                 } else {
                     v[2 * k] = v[2 * k + 1] = 0.f;
                 }
             }
             LA[i] = make_float4(v[0], v[1], v[2], v[3]);
             LB[i] = make_float4(v[4], v[5], v[6], v[7]);
-            bits[i] = b;
+            bits[i] = (uint8_t)b;
         }
         __syncthreads();
         float lw[kHvCh];
@@ -480,7 +489,7 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                     if (m < lim) {
                         const int off = own + tab.delta[j * SECOND + m];
                         const float4 A = LA[off], B = LB[off];
-                        const uint32_t b = (bits[off] >> 1) & 15u;
+                        const uint32_t b = bits[off];
                         sl[0] += A.x; sa[0] += A.y; sl[1] += A.z; sa[1] += A.w;
                         sl[2] += B.x; sa[2] += B.y; sl[3] += B.z; sa[3] += B.w;
                         const uint32_t nb = b & ~seen;
@@ -515,25 +524,25 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                     }
                 }
                 const bool fj = (face >> j) & 1u;
+                // Per hour, with f the first step showing a sunlit wall (FIRST = 1):
+                //   near = (f == 0 < hit): lup1 = (lw + l0) / 2, else l0;
+                //   far  = (f < hit):      lup2 = ((SECOND - f) lw + sl) / (SECOND + 1), else sl / SECOND,
+                //          the wall term dropped when f == 0 on a self-shadowed face (fj);
+                //   lup_t += (0.5 lup1 + 0.4 lup2) / 0.9  (the same for the albedos with albedo_b),
+                // as two fused multiply-adds with the selected weights.
 #pragma unroll
                 for (int k = 0; k < kHvCh; ++k) {
                     const int f = (int)((first_pk >> (5 * k)) & 31u);
-                    const int n_sun = f < hit ? SECOND - f : 0;
-                    const int n_sun_first = (f < FIRST && f < hit) ? FIRST - f : 0;
-                    const bool sun_near = n_sun_first > 0, sun_far = n_sun > 0;
-                    const float s_wall = (float)n_sun;
-                    float s_lwall = s_wall * lw[k], s_albwall = s_wall * albedo_b;
-                    if (n_sun == SECOND && fj) {
-                        s_lwall = 0.f;
-                        s_albwall = 0.f;
-                    }
-                    const float nn = (float)n_sun_first;
-                    const float lup1 = sun_near ? (nn * lw[k] + l0[k]) * inv_first1 : l0[k] * inv_first;
-                    const float lup2 = sun_far ? (s_lwall + sl[k]) * inv_second1 : sl[k] * inv_second;
-                    const float alb1 = sun_near ? (nn * albedo_b + a0[k]) * inv_first1 : a0[k] * inv_first;
-                    const float alb2 = sun_far ? (s_albwall + sa[k]) * inv_second1 : sa[k] * inv_second;
-                    lup_t[k] += (lup1 * 0.5f + lup2 * 0.4f) * (1.f / 0.9f);
-                    alb_t[k] += (alb1 * 0.5f + alb2 * 0.4f) * (1.f / 0.9f);
+                    const bool sun_far = f < hit;
+                    const bool sun_near = sun_far && f == 0;
+                    const float wn = (sun_far && !(sun_near && fj)) ? (float)(SECOND - f) : 0.f;
+                    const float en = sun_near ? 1.f : 0.f;
+                    const float c1 = sun_near ? (inv_first1 * 0.5f / 0.9f) : (inv_first * 0.5f / 0.9f);
+                    const float c2 = sun_far ? (inv_second1 * 0.4f / 0.9f) : (inv_second * 0.4f / 0.9f);
+                    lup_t[k] = fmaf(c1, fmaf(en, lw[k], l0[k]), lup_t[k]);
+                    lup_t[k] = fmaf(c2, fmaf(wn, lw[k], sl[k]), lup_t[k]);
+                    alb_t[k] = fmaf(c1, fmaf(en, albedo_b, a0[k]), alb_t[k]);
+                    alb_t[k] = fmaf(c2, fmaf(wn, albedo_b, sa[k]), alb_t[k]);
                 }
             }
         }
