@@ -222,8 +222,9 @@ def _peaks():
 # What bounds each stage of the batched day (from the ncu summaries in
 # profiles/): the HBM fraction of the gather-bound stages is small by nature.
 STAGE_LIMITER = {
-    "day_shadow_kernel": "latency of the ray-step gathers (shared-memory window, then L1/L2)",
-    "day_gvf_kernel": "shared-memory wavefronts of the 18 x 22 walks",
+    "day_shadow_kernel": "latency of the ray-step gathers through L1/L2 and lane divergence of the walk lengths",
+    "day_gvf_kernel": "instruction issue of the 18 x 22 walks and the block barriers of the 4-hour passes "
+                      "(shared-memory wavefronts about half of their peak)",
     "day_tables_kernel": "negligible (one block per hour)",
     "patch_gemm_kernel": "tensor pipe and the FP32 sum stores",
     "day_radiation_kernel": "latency of the per-pixel hour loop",

@@ -342,14 +342,19 @@ int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout*
  * albedo-without-shadow GVF [px], patch sums (room for [2][2H][px]; the day
  * writes [2H][px]: sky plus 0.03 x vegetation sums of luminance and
  * luminance*cos*omega per hour), weights f32 [2H][160], BF16 operands (hi/lo
- * of the weights and of 0.03 x the weights), per-hour tables, error flag,
- * 16x16 tile maxima of the heights (window sweep), total size:
- * offsets[0..10]. */
+ * of the weights and of 0.03 x the weights), per-hour tables, error flag pair
+ * (placed first, at offset 0 for every raster size), 16x16 tile maxima of the
+ * heights (window sweep), total size: offsets[0..10]. */
 int solweig_day_batched_layout(int rows, int cols, int nhours, int has_water, int64_t* offsets);
 /* Copy the device error flag of the last batched day in `work` to out_device:
  * 0 = none, 1 = a tensor-core wait of the contraction timed out (results
  * invalid), 2 = a sweep window's TMA wait timed out (that tile walked from the
- * raster instead; results still exact). */
+ * raster instead; results still exact), 3 = a sun ray table stayed inside the
+ * raster for more than max(rows, cols) + 2 steps (that hour's results
+ * invalid; rays built as the reference builds them never do).  The int after
+ * the flag in `work` has bit v set for every flag v raised by any day run in
+ * that buffer since the caller last zeroed it (the days never clear it), so
+ * one read after a graph of many days or tiles covers all of them. */
 int solweig_day_batched_error(const void* work, int rows, int cols, int nhours, int has_water,
                               int* out_device, void* stream);
 /* The patch contraction alone: out[c][p] = sum_k sky(p,k) * weights[c][k] for

@@ -71,6 +71,8 @@ def simulate_day(dsm, trees, dem, met, latitude, longitude, landcover=None, pixe
         out[k] = host
         d2h += host.numel() * 4
     torch.cuda.current_stream().synchronize()
+    if hasattr(runner, "check_errors"):
+        runner.check_errors()
     out = {k: v.numpy() for k, v in out.items()}
     out["h2d_bytes"] = h2d
     out["d2h_bytes"] = d2h

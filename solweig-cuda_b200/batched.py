@@ -17,7 +17,41 @@ import torch
 from . import _lib
 from .engine import HourBuffers, device_ptr, outputs_struct, plan_day, plan_hours, stream_handle
 
-__all__ = ["BatchedDay", "ChosenDay", "MultiDay", "TileBatch"]
+__all__ = ["BatchedDay", "ChosenDay", "MultiDay", "TileBatch", "DayError"]
+
+# Bits of the sticky error word (word 1 of the flag pair at the start of the
+# work buffer): bit v is set when a day raised flag v.  Flags 1 (a tensor-core
+# wait of the contraction timed out) and 3 (a sun ray stayed inside the raster
+# for more than max(rows, cols) + 2 steps) leave invalid results; flag 2 (a
+# window sweep's TMA wait timed out) does not (that tile walked from the raster).
+_INVALID_BITS = (1 << 1) | (1 << 3)
+_FLAG_TEXT = {1: "a tensor-core wait of the patch contraction timed out",
+              2: "a sweep window's TMA wait timed out (results exact)",
+              3: "a sun ray table stayed inside the raster longer than max(rows, cols) + 2 steps"}
+
+
+class DayError(RuntimeError):
+    """A batched day raised a device error flag that invalidates its results."""
+
+
+def _error_words(work):
+    """The flag pair at the start of a batched-day work buffer (int32 view)."""
+    return work[:8].view(torch.int32)
+
+
+def clear_day_errors(work):
+    """Zero both words of the flag pair (the days never clear the sticky word)."""
+    _error_words(work).zero_()
+
+
+def check_day_errors(work, what="batched day"):
+    """Raise DayError when a day run in `work` since the last clear raised a
+    flag that invalidates results; returns the sticky bit set (synchronises)."""
+    bits = int(_error_words(work)[1].item())
+    if bits & _INVALID_BITS:
+        raised = [v for v in _FLAG_TEXT if bits & (1 << v)]
+        raise DayError(f"{what}: " + "; ".join(_FLAG_TEXT[v] for v in raised) + " - results invalid")
+    return bits
 
 
 class BatchedDay:
@@ -145,6 +179,7 @@ class ChosenDay(BatchedDay):
         if self.work_bytes <= 0:
             raise ValueError("bad batched-day shape")
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=scene.device)
+        clear_day_errors(self.work)
         self.config = _lib.SolweigDayConfig.default()
 
     @staticmethod
@@ -328,9 +363,14 @@ class ChosenDay(BatchedDay):
         n = 2 * self.hours * self.scene.pixels
         return self.work[o["sums"]:o["sums"] + 4 * n].view(torch.float32).view(2 * self.hours, self.scene.pixels)
 
+    def check_errors(self):
+        """Raise DayError if any day run by this object left invalid results."""
+        return check_day_errors(self.work, "batched day")
+
     def error_flag(self):
         """Device error flag of the last day (0 = ok, 1 = a tensor-core wait timed
-        out, 2 = a sweep window's TMA wait timed out: that tile walked from the raster)."""
+        out, 2 = a sweep window's TMA wait timed out: that tile walked from the raster,
+        3 = a sun ray stayed inside the raster for more than max(rows, cols) + 2 steps)."""
         flag = torch.zeros(1, dtype=torch.int32, device=self.scene.device)
         sc = self.scene
         _lib.check(_lib.lib().solweig_day_batched_error(
@@ -361,6 +401,7 @@ class MultiDay:
         self.work_bytes = int(_lib.lib().solweig_day_batched_work_bytes(scene.rows, scene.cols, hours,
                                                                         int(scene.struct.has_water)))
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=dev)
+        clear_day_errors(self.work)
         self.config = config if config is not None else _lib.SolweigDayConfig.default()
         self.graph = None
         self.launches = day_launches(scene, self.config) * days
@@ -411,6 +452,10 @@ class MultiDay:
             self.capture()
         return self.replay()
 
+    def check_errors(self):
+        """Raise DayError if any day of any replay so far left invalid results."""
+        return check_day_errors(self.work, "multi-day batch")
+
 
 class TileBatch:
     """Independent tiles (own scene, latitude and forcing) for one day each,
@@ -431,6 +476,7 @@ class TileBatch:
                                                                    int(s.struct.has_water)))
                               for s in self.scenes)
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=dev)
+        clear_day_errors(self.work)
         self.buffers = [HourBuffers(s, hours) for s in self.scenes]
         self.layouts = [s.layout.device(dev) for s in self.scenes]
         self.state = [{k: torch.zeros(s.shape, dtype=torch.float32, device=dev) for k in ("tgmap1", "tgout1")}
@@ -487,3 +533,7 @@ class TileBatch:
         if self.graph is None:
             self.capture()
         return self.replay()
+
+    def check_errors(self):
+        """Raise DayError if any tile-day of any replay so far left invalid results."""
+        return check_day_errors(self.work, "tile batch")

@@ -740,7 +740,8 @@ static int grad_prepare(const SolweigScene* scene, const SolweigSkyLayout* layou
     cudaMemsetAsync(nosh, 0, 4 * px, st);
     {
         dim3 grid(blocks_for(S.cols, 16), blocks_for(S.rows, 16), nhours);
-        day_shadow_kernel<<<grid, dim3(16, 16), 0, st>>>(S, hours, quads0, nullptr, nullptr, nullptr);
+        day_shadow_kernel<false><<<grid, dim3(16, 16), 0, st>>>(S, hours, quads0, nullptr, nullptr, nullptr,
+                                                                nullptr, 0);
         SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
     }
     param_quads_kernel<<<blocks_for(px * nhours, 256), 256, 0, st>>>(S, hours, nhours, quads0, quads1, sv,

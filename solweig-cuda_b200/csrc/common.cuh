@@ -48,4 +48,12 @@ __host__ __device__ __forceinline__ double pow4(double x) {
     return x2 * x2;
 }
 
+// Error flag pair of a batched day's work buffer: word 0 = the last flag of
+// the current day (cleared when the day starts), word 1 = bit v set for every
+// flag v raised since the host last zeroed it (never cleared by the kernels).
+__device__ __forceinline__ void raise_day_flag(int* error, int value) {
+    atomicExch(error, value);
+    atomicOr(error + 1, 1 << value);
+}
+
 }  // namespace solweig

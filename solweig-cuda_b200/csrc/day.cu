@@ -203,7 +203,14 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
         // first-outside steps of every row and column per hour (4 B each), in
         // the GVF region after the ceiling planes (8 B per pixel-hour left)
         int* exits = reinterpret_cast<int*>(wb + w.gvf + 4LL * px * nhours) + (long long)h0 * (S.rows + S.cols);
-        day_ray_exits_kernel<<<nh, 1024, 0, st>>>(S, hours + h0, exits);
+        // then the hours' step records (16 B per step, at most max(rows, cols) + 2
+        // steps per hour), when they fit before the end of the GVF region
+        const long long rec_at = (w.gvf + 4LL * px * nhours + 4LL * (S.rows + S.cols) * nhours + 15) & ~15LL;
+        const int kmax = (S.rows > S.cols ? S.rows : S.cols) + 2;
+        longlong2* rec = nullptr;
+        if (rec_at + 16LL * kmax * nhours <= w.gvf + 12LL * px * nhours)
+            rec = reinterpret_cast<longlong2*>(wb + rec_at) + (long long)h0 * kmax;
+        day_ray_exits_kernel<<<nh, 1024, 0, st>>>(S, hours + h0, exits, rec, kmax, err);
         SOLWEIG_CHECK_LAUNCH("day_ray_exits_kernel");
         if (window) {
             const int win = cfg.sweep_window == 2 ? 40 : 48;
@@ -225,9 +232,14 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
             return SOLWEIG_OK;
         }
         dim3 grid(blocks_for(S.cols, cfg.shadow_bx), blocks_for(S.rows, cfg.shadow_by), nh);
-        day_shadow_kernel<<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(
-            S, hours + h0, quads + h0 * px, lup_first ? lup_first + h0 * px : nullptr,
-            ceiling ? ceiling + h0 * px : nullptr, exits);
+        if (rec && S.geo32)
+            day_shadow_kernel<true><<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(
+                S, hours + h0, quads + h0 * px, lup_first ? lup_first + h0 * px : nullptr,
+                ceiling ? ceiling + h0 * px : nullptr, exits, rec, kmax);
+        else
+            day_shadow_kernel<false><<<grid, dim3(cfg.shadow_bx, cfg.shadow_by), 0, st>>>(
+                S, hours + h0, quads + h0 * px, lup_first ? lup_first + h0 * px : nullptr,
+                ceiling ? ceiling + h0 * px : nullptr, exits, nullptr, 0);
         SOLWEIG_CHECK_LAUNCH("day_shadow_kernel");
         return SOLWEIG_OK;
     }

@@ -173,14 +173,18 @@ __device__ __forceinline__ void warp_tile_pixel(int bx, int by, int& r, int& c) 
     }
 }
 
-// 32 registers (8 blocks of 256 per SM): the sweep is latency-bound and the
-// full occupancy outweighs a few spills (8.12 -> 7.74 ms per 2000^2 day).
-__global__ void __launch_bounds__(256, 8) day_shadow_kernel(SolweigScene S,
+// REC: the walks read the hour's step records (rec + z * kmax, written by
+// day_ray_exits_kernel) instead of the (dx, dy) and dz tables.  40 registers
+// (6 blocks of 256 per SM): the walk's float64 state no longer spills (per
+// 2000^2 day 5.77 ms against 5.97 ms at 32 registers and 8 blocks).
+template <bool REC>
+__global__ void __launch_bounds__(256, 6) day_shadow_kernel(SolweigScene S,
                                                                    const SolweigHour* __restrict__ hours,
                                                                    float4* __restrict__ quads,
                                                                    float* __restrict__ lup_first,
                                                                    const float* __restrict__ ceiling,
-                                                                   const int* __restrict__ exits) {
+                                                                   const int* __restrict__ exits,
+                                                                   const longlong2* __restrict__ rec, int kmax) {
     const int z = blockIdx.z;
     const SolweigHour& h = hours[z];
     if (!h.daytime) return;
@@ -189,19 +193,39 @@ __global__ void __launch_bounds__(256, 8) day_shadow_kernel(SolweigScene S,
     const bool in = r < S.rows && c < S.cols;
     const long long n = (long long)S.rows * S.cols;
     if (!in) return;
-    shadow_quad_pixel(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
-                      ceiling ? ceiling + z * n : nullptr,
-                      exits ? exits + (long long)z * (S.rows + S.cols) : nullptr);
+    shadow_quad_pixel<REC>(S, h, r, c, quads + z * n, lup_first ? lup_first + z * n : nullptr,
+                           ceiling ? ceiling + z * n : nullptr,
+                           exits ? exits + (long long)z * (S.rows + S.cols) : nullptr,
+                           REC ? rec + (long long)z * kmax : nullptr);
 }
 
 // Per daytime hour, the first-outside step of every row and column of the
-// raster (first_outside), for the bounds-check-free sweep.
+// raster (first_outside), for the bounds-check-free sweep, and with rec the
+// hour's step records for the steps [0, min(steps, kmax)).  A monotone ray
+// leaves the raster within max(rows, cols) steps, so kmax = max(rows, cols)
+// + 2 covers every walk; a ray table that stays inside longer has its exits
+// cut to kmax and sets the error flag to 3 (that hour's results invalid).
 __global__ void __launch_bounds__(1024) day_ray_exits_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
-                                                             int* __restrict__ exits) {
+                                                             int* __restrict__ exits, longlong2* __restrict__ rec,
+                                                             int kmax, int* __restrict__ error) {
     const SolweigHour& h = hours[blockIdx.x];
     if (!h.daytime) return;
-    ray_exits_block(reinterpret_cast<const int2*>(h.ray_dxdy), h.steps, S.rows, S.cols,
-                    exits + (long long)blockIdx.x * (S.rows + S.cols));
+    int* ex = exits + (long long)blockIdx.x * (S.rows + S.cols);
+    ray_exits_block(reinterpret_cast<const int2*>(h.ray_dxdy), h.steps, S.rows, S.cols, ex);
+    if (rec == nullptr) return;
+    const int K = min(h.steps, kmax);
+    ray_records_block(reinterpret_cast<const int2*>(h.ray_dxdy), h.ray_dz, K, S.cols,
+                      rec + (long long)blockIdx.x * kmax);
+    if (h.steps <= kmax) return;
+    __syncthreads();  // ex[] written by the whole block
+    int cut = 0;
+    for (int i = threadIdx.x; i < S.rows + S.cols; i += blockDim.x) {
+        if (ex[i] > kmax) {
+            ex[i] = kmax;
+            cut = 1;
+        }
+    }
+    if (cut) raise_day_flag(error, 3);
 }
 
 struct DayGvfArgs {
@@ -483,7 +507,10 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                 float sl[kHvCh], sa[kHvCh], l0[kHvCh], a0[kHvCh];
 #pragma unroll
                 for (int k = 0; k < kHvCh; ++k) sl[k] = sa[k] = l0[k] = a0[k] = 0.f;
-                uint32_t seen = 0u, first_pk = 0xFFFFFu;  // 5 bits per hour, 31 = never
+                // Per hour k (byte k of both words): seen = a sunlit wall met so far,
+                // cnt = steps before the first one (branch-free: each step adds
+                // the not-yet-seen bytes), so f = cnt_k when seen_k.
+                uint32_t seen = 0u, cnt = 0u;
 #pragma unroll
                 for (int m = 0; m < SECOND; ++m) {
                     if (m < lim) {
@@ -492,13 +519,8 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                         const uint32_t b = bits[off];
                         sl[0] += A.x; sa[0] += A.y; sl[1] += A.z; sa[1] += A.w;
                         sl[2] += B.x; sa[2] += B.y; sl[3] += B.z; sa[3] += B.w;
-                        const uint32_t nb = b & ~seen;
-                        if (nb) {
-#pragma unroll
-                            for (int k = 0; k < kHvCh; ++k)
-                                if ((nb >> k) & 1u) first_pk = (first_pk & ~(31u << (5 * k))) | ((uint32_t)m << (5 * k));
-                            seen |= b;
-                        }
+                        seen |= (b * 0x00204081u) & 0x01010101u;  // bit k -> byte k
+                        cnt += ~seen & 0x01010101u;
                         if (m + 1 == FIRST) {
 #pragma unroll
                             for (int k = 0; k < kHvCh; ++k) {
@@ -532,7 +554,7 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
                 // as two fused multiply-adds with the selected weights.
 #pragma unroll
                 for (int k = 0; k < kHvCh; ++k) {
-                    const int f = (int)((first_pk >> (5 * k)) & 31u);
+                    const int f = (seen >> (8 * k)) & 1u ? (int)((cnt >> (8 * k)) & 0xFFu) : 31;
                     const bool sun_far = f < hit;
                     const bool sun_near = sun_far && f == 0;
                     const float wn = (sun_far && !(sun_near && fj)) ? (float)(SECOND - f) : 0.f;
@@ -840,7 +862,7 @@ __global__ void __launch_bounds__(kARows, 1) patch_gemm_kernel(GemmArgs g) {
         __syncthreads();
     }
     if (failed) {
-        if (tid == 0) atomicExch(g.error, 1);
+        if (tid == 0) raise_day_flag(g.error, 1);
         // let the MMAs of the abandoned tile finish before freeing their columns
         tc::mbar_wait(bar, phase, kWaitPolls);
     }
@@ -1078,6 +1100,9 @@ DayWork day_work_layout(long long px, int nhours, bool water) {
     const int ncols = 2 * nhours;
     const int nb = (ncols + 15) / 16 * 16;
     long long o = 0;
+    // the error flag pair first: the same place for every raster size, so the
+    // days of differently sized tiles sharing one buffer share its sticky word
+    w.error = o; o = align256(o + 16);
     w.quads = o; o = align256(o + 16LL * px * nhours);
     w.lup_first = o; o = align256(o + (water ? 4LL * px * nhours : 0));
     w.gvf = o; o = align256(o + 12LL * px * nhours);
@@ -1086,7 +1111,6 @@ DayWork day_work_layout(long long px, int nhours, bool water) {
     w.wf32 = o; o = align256(o + 4LL * ncols * kK);
     w.bw = o; o = align256(o + 2LL * 4 * nb * kK);
     w.tables = o; o = align256(o + (long long)sizeof(DayTable) * nhours);
-    w.error = o; o = align256(o + 16);
     // per 16 x 16 tile maxima of the heights (ceil(rows/16) * ceil(cols/16)
     // floats, bounded here from the pixel count alone: <= px/256 + (rows + cols)/16 + 1)
     w.tilemax = o; o = align256(o + 4LL * (px / 256 + (px + 1) / 16 + 4));

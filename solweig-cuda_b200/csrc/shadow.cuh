@@ -151,10 +151,17 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
 // per-step bounds checks, linear sample offsets, and only the DSM height is
 // widened to float64 at a sample without canopy (tq, bq <= 0 compare the
 // same in float32).  Results are identical to shadow_walk_geo.
+//
+// The steps run in unrolled groups of four aligned at step 0, so the
+// ray-ceiling test (steps 4, 8, ...) is the first step of a group and costs
+// no per-step test.  With REC the hour's steps come as 16-byte records
+// {linear offset o.x * cols + o.y, dz bit pattern} (one uniform load per
+// step, ray_records_block); otherwise from the (dx, dy) and dz tables.
+template <bool REC>
 __device__ __forceinline__ ShadowResult shadow_walk_packed(
     const float4* __restrict__ geo, int cols, long long p, double a, double top_p, bool bush, double wall,
-    const int2* __restrict__ ray, const double* __restrict__ dz, int steps, int kend, double hmax,
-    const float* __restrict__ ceiling) {
+    const int2* __restrict__ ray, const double* __restrict__ dz, const longlong2* __restrict__ rec, int steps,
+    int kend, double hmax, const float* __restrict__ ceiling) {
     ShadowResult s;
     s.f = a;
     s.topmax = top_p;
@@ -165,47 +172,63 @@ __device__ __forceinline__ ShadowResult shadow_walk_packed(
     const bool nonneg = a >= 0.0;
     const double clear = nonneg ? nextafter(hmax - a, __longlong_as_double(0x7ff0000000000000ll))
                                 : __longlong_as_double(0x7ff0000000000000ll);
+    const float4* __restrict__ gp = geo + p;
+    const float* __restrict__ cp = ceiling != nullptr ? ceiling + p : nullptr;
     double dz_prev = 0.0;
     bool final = false;
     int k = 0;
-    for (; k < kend; ++k) {
-        const int2 o = __ldg(&ray[k]);
-        const double dzk = __ldg(&dz[k]);
-        const long long q = p + (long long)o.x * cols + o.y;
-        if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
-            final = true;
-            break;
-        }
-        if (ceiling != nullptr && k >= 4 && (k & 3) == 0) {
-            const double e = __dsub_ru((double)__ldg(&ceiling[q]), dz_prev);
-            if (nonneg && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) {
+    while (k < kend) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {  // u == k % 4
+            if (k >= kend) break;
+            long long off;
+            double dzk;
+            if (REC) {
+                const longlong2 r = __ldg(rec + k);
+                off = r.x;
+                dzk = __longlong_as_double(r.y);
+            } else {
+                const int2 o = __ldg(&ray[k]);
+                dzk = __ldg(&dz[k]);
+                off = (long long)o.x * cols + o.y;
+            }
+            if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) {
                 final = true;
                 break;
             }
-        }
-        const float4 v = __ldg(&geo[q]);
-        s.f = fmax(s.f, (double)v.x - dzk);
-        s.shadowed = s.f > a;
-        if (v.y <= 0.f && v.z <= 0.f && nonneg && s.topmax >= 0.0) {
-            if (s.shadowed) s.veg = false;
-            else s.ever = s.ever || s.veg;
-        } else {
-            const double tq = v.y, bq = v.z;
-            s.topmax = fmax(s.topmax, tq - dzk);
-            if (s.shadowed) {
-                s.veg = false;
-            } else {
-                const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
-                              (int)(bq - dz_prev > a);
-                s.veg = s.veg || (n > 0 && n < 4);
-                s.ever = s.ever || s.veg;
+            if (u == 0 && cp != nullptr && k >= 4) {
+                const double e = __dsub_ru((double)__ldg(cp + off), dz_prev);
+                if (nonneg && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) {
+                    final = true;
+                    break;
+                }
             }
+            const float4 v = __ldg(gp + off);
+            s.f = fmax(s.f, (double)v.x - dzk);
+            s.shadowed = s.f > a;
+            if (v.y <= 0.f && v.z <= 0.f && nonneg && s.topmax >= 0.0) {
+                if (s.shadowed) s.veg = false;
+                else s.ever = s.ever || s.veg;
+            } else {
+                const double tq = v.y, bq = v.z;
+                s.topmax = fmax(s.topmax, tq - dzk);
+                if (s.shadowed) {
+                    s.veg = false;
+                } else {
+                    const int n = (int)(tq - dzk > a) + (int)(bq - dzk > a) + (int)(tq - dz_prev > a) +
+                                  (int)(bq - dz_prev > a);
+                    s.veg = s.veg || (n > 0 && n < 4);
+                    s.ever = s.ever || s.veg;
+                }
+            }
+            if (s.shadowed && (!is_wall || s.f - a >= wall)) {
+                final = true;
+                break;
+            }
+            dz_prev = dzk;
+            ++k;
         }
-        if (s.shadowed && (!is_wall || s.f - a >= wall)) {
-            final = true;
-            break;
-        }
-        dz_prev = dzk;
+        if (final) break;
     }
     if (!final && k < steps) {
         // First step whose sample is outside the raster: all shifted values are 0.
@@ -216,6 +239,16 @@ __device__ __forceinline__ ShadowResult shadow_walk_packed(
         s.ever = s.ever || s.veg;
     }
     return s;
+}
+
+// Step records of one hour's ray for shadow_walk_packed<true>: rec[k] =
+// {o_k.x * cols + o_k.y, dz_k as a 64-bit pattern} for k < K, by one block.
+__device__ __forceinline__ void ray_records_block(const int2* __restrict__ ray, const double* __restrict__ dz,
+                                                  int K, int cols, longlong2* __restrict__ rec) {
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int2 o = __ldg(&ray[k]);
+        rec[k] = make_longlong2((long long)o.x * cols + o.y, __double_as_longlong(__ldg(&dz[k])));
+    }
 }
 
 // Per hour, the first step at which the ray from row r (column c) leaves the

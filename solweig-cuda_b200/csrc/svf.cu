@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
             if (WALK == 2) {
                 const int* e = exits + (long long)j * (prm.rows + prm.cols);
                 const int kend = min(K, min(__ldg(&e[r]), __ldg(&e[prm.rows + c])));
-                s = shadow_walk_packed(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base, K, kend,
-                                       prm.hmax, ceil_j);
+                s = shadow_walk_packed<false>(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base,
+                                              nullptr, K, kend, prm.hmax, ceil_j);
             } else if (WALK == 1) {
                 s = shadow_walk_geo(GeoF32x4{geo32}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
                                     dz + base, K, prm.hmax, true, ceil_j);

@@ -218,30 +218,11 @@ __device__ __forceinline__ ShadowResult shadow_walk_window(
     return s;
 }
 
-// Quad epilogue of shadow_quad_pixel for a walk result.
+// Quad epilogue of shadow_quad_pixel for a walk result (no water here).
 __device__ __forceinline__ void write_quad(const SolweigScene& S, const SolweigHour& h, long long p, double a,
                                            double wall, uint8_t fl, const ShadowResult& s,
                                            float4* __restrict__ quad) {
-    const double wallbol = wall > 0.0 ? 1.0 : 0.0;
-    const double facesh = self_shadow_face(S.aspect[p], wallbol, h.ray_low, h.ray_high, h.ray_middle);
-    double wallsun = wall - (s.f - a);
-    if (wallsun < 0.0) wallsun = 0.0;
-    if (facesh == 1.0) wallsun = 0.0;
-    const double wallsh = wall - wallsun;
-    double wallshve = (s.topmax - a) * (s.veg ? 1.0 : 0.0) * wallbol - wallsh;
-    if (wallshve < 0.0) wallshve = 0.0;
-    if (wallshve > wall) wallshve = wall;
-    wallsun = wallsun - wallshve;
-    if (wallsun < 0.0) wallsun = 0.0;
-    const double ground = (fl & 1) ? 1.0 : 0.0;
-    const bool sunwall = (wallsun / wall * ground) == 1.0;
-    const double sh = s.shadowed ? 0.0 : 1.0;
-    const double vegsh = s.veg ? 0.0 : 1.0;
-    const double shadow = (double)(float)(sh - (1.0 - vegsh) * (1.0 - h.psi));
-    const double tg = ground_tg(S, h, p);
-    const float lup = (float)lup_excess((double)S.emis[p], tg, shadow, h.ta);
-    quad[p] = make_float4((float)shadow, lup, S.alb[p],
-                          __int_as_float((fl & 1 ? kQuadGround : 0) | (sunwall ? kQuadSunwall : 0)));
+    quad[p] = quad_from_walk(S, h, p, a, wall, fl, s, nullptr);
 }
 
 // grid (tiles along columns, tiles along rows, hours of the range); kSwThreads
@@ -326,7 +307,7 @@ __global__ void __launch_bounds__(kSwThreads, WIN <= 40 ? 8 : 6)
     const bool got = sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
     if (!got) sw_mbar_wait(&sm.bar, 0, kSwWaitPolls);
     const bool staged = __all_sync(0xffffffffu, got);
-    if (!staged && l == 0) atomicExch(error, 2);
+    if (!staged && l == 0) raise_day_flag(error, 2);
     const int kw = staged && in ? min(kend, min(row_exit, col_exit)) : 0;
     const double pinf = __longlong_as_double(0x7ff0000000000000ll);
     const double wclear = a >= 0.0 ? nextafter((double)m - a, pinf) : pinf;

@@ -347,6 +347,9 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
         writer.finish()
         if on_gpu:
             torch.cuda.synchronize(scene.device)
+        for runner in runners.values():  # device error flags of every day run
+            if hasattr(runner, "check_errors"):
+                runner.check_errors()
         return files
     except BaseException:
         writer.abort()
@@ -456,6 +459,8 @@ def run_tiles(tiles, met_file, output_path, longitude, latitude, *, utc_offset_h
                                                              for v in variables}
                 stamp(f"Daily calculation completed: {day.date} ({len(group)} tiles)")
             torch.cuda.synchronize(torch.device(device))
+            for batch in batches.values():  # device error flags of every tile-day
+                batch.check_errors()
             del batches, scenes
         writer.finish()
         return files

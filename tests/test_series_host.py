@@ -142,3 +142,39 @@ def test_run_timeseries_rank_shares_cover_all_days(tmp_path):
     for date, rec in whole["days"].items():
         for var, paths in rec.items():
             assert np.array_equal(np.load(paths[0]), np.load(got[date][var][0]))
+
+
+def test_day_error_bits_raise_only_for_invalid_results():
+    """The sticky word of the flag pair: bits 1 and 3 (contraction wait timed
+    out, overlong ray) raise DayError; bit 2 (window sweep walked from the
+    raster, results exact) does not; a cleared pair passes."""
+    import torch
+    from solweig_cuda_b200 import batched
+    work = torch.zeros(64, dtype=torch.uint8)
+    batched.clear_day_errors(work)
+    assert batched.check_day_errors(work) == 0
+    words = work[:8].view(torch.int32)
+    words[1] = 1 << 2
+    assert batched.check_day_errors(work) == 4
+    for bit in (1, 3):
+        words[1] = (1 << bit) | (1 << 2)
+        with pytest.raises(batched.DayError):
+            batched.check_day_errors(work)
+    batched.clear_day_errors(work)
+    assert int(words[0]) == 0 and int(words[1]) == 0
+
+
+class FlaggedRunner(StubRunner):
+    """A runner whose days left invalid results (as a device flag would say)."""
+
+    def check_errors(self):
+        from solweig_cuda_b200 import batched
+        raise batched.DayError("batched day: test flag - results invalid")
+
+
+def test_run_timeseries_raises_when_a_day_left_invalid_results(tmp_path):
+    from solweig_cuda_b200 import batched, series
+    z = np.zeros((12, 10))
+    with pytest.raises(batched.DayError):
+        series.run_timeseries(z, z, z, _forcing(2), tmp_path, 0.0, 53.0, scene_factory=StubScene,
+                              runner_factory=FlaggedRunner, device="cpu")
