@@ -722,13 +722,14 @@ size_t gemm_smem_bytes(int nb, bool combined) {
 }
 
 // Expand 8 mask bits to 8 BF16 values (1.0 or 0.0) packed in a uint4.
+// t = byte + (byte << 15) holds bit 2i at position 2i and bit 2i + 1 at
+// position 16 + 2i, so (t >> 2i) & 0x10001 has the pair's two bits at 0 and
+// 16, and times 0x3F80 (BF16 1.0) gives the two packed values.
 __device__ __forceinline__ uint4 expand8(uint32_t byte) {
+    const uint32_t t = byte * 0x8001u;
     uint32_t v[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const uint32_t two = (byte >> (2 * i)) & 3u;
-        v[i] = ((two & 1u) | ((two & 2u) << 15)) * 0x3F80u;
-    }
+    for (int i = 0; i < 4; ++i) v[i] = ((t >> (2 * i)) & 0x10001u) * 0x3F80u;
     return make_uint4(v[0], v[1], v[2], v[3]);
 }
 
@@ -865,6 +866,165 @@ __global__ void __launch_bounds__(kARows, 1) patch_gemm_kernel(GemmArgs g) {
         if (tid == 0) raise_day_flag(g.error, 1);
         // let the MMAs of the abandoned tile finish before freeing their columns
         tc::mbar_wait(bar, phase, kWaitPolls);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, ncols_tmem);
+    }
+}
+
+// Pipelined form of the combined contraction (the batched day's): two A
+// stages in shared memory and two accumulators in tensor memory, 256
+// threads.  While the tensor cores multiply tile i, the threads expand tile
+// i + 1 into the other stage (threads 0-127 the sky masks, 128-255 the
+// vegetation masks of the same 128 pixels; the mask words of tile i + 2 are
+// already loading), then wait for tile i and store its sums from tensor
+// memory (warp w: lanes 32 (w % 4) .. + 31, every other 8-column group from
+// 8 (w / 4)).  Thread 0 issues each tile's MMAs once both of its operands
+// are in shared memory and the stage's accumulator has been read out.
+constexpr int kPipeThreads = 2 * kARows;
+
+size_t gemm_pipe_smem_bytes(int nb) { return (size_t)4 * kABytes + (size_t)4 * nb * kK * 2 + 32; }
+
+__global__ void __launch_bounds__(kPipeThreads, 1) patch_gemm_pipe_kernel(GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* b_ops = smem + 4 * kABytes;  // hi, lo, c * w hi, c * w lo
+    const int bbytes = g.nb * kK * 2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(b_ops + 4 * bbytes);  // one per stage
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row = tid & (kARows - 1);
+    const bool veg_half = tid >= kARows;
+    uint32_t ncols_tmem = 32;
+    while (ncols_tmem < (uint32_t)(2 * g.nb)) ncols_tmem <<= 1;
+    {  // weights: global -> shared, 16 bytes per copy
+        const uint4* src = reinterpret_cast<const uint4*>(g.b);
+        uint4* dst = reinterpret_cast<uint4*>(b_ops);
+        for (int i = tid; i < 4 * bbytes / 16; i += blockDim.x) dst[i] = src[i];
+    }
+    if (tid == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(tmem_slot, ncols_tmem);
+        tc::tmem_relinquish();
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = tc::idesc_bf16_f32(kARows, g.nb);
+    const uint32_t b_hi_addr = tc::smem_addr(b_ops);
+    uint32_t valid[SOLWEIG_MASK_WORDS];
+#pragma unroll
+    for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+        const int nbits = g.patches - 32 * w;
+        valid[w] = nbits >= 32 ? 0xffffffffu : (nbits <= 0 ? 0u : ((1u << nbits) - 1u));
+    }
+    const long long ntiles = (g.px + kARows - 1) / kARows;
+    const long long first = blockIdx.x, stride = gridDim.x;
+    const long long my = first < ntiles ? (ntiles - 1 - first) / stride + 1 : 0;  // tiles of this CTA
+
+    uint32_t sw[SOLWEIG_MASK_WORDS], vw[SOLWEIG_MASK_WORDS];
+    auto load = [&](long long t) {
+        const long long p = t * kARows + row;
+        const bool in = p < g.px;
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            sw[w] = in ? __ldg(&g.masks[(long long)w * g.px + p]) : 0u;
+            vw[w] = in ? __ldg(&g.masks[(long long)(SOLWEIG_MASK_WORDS + w) * g.px + p]) : 0u;
+        }
+    };
+    auto expand = [&](int st) {
+        unsigned char* a = smem + (2 * st + (veg_half ? 1 : 0)) * kABytes;
+        unsigned char* rowp = a + (row >> 3) * kSBO + (row & 7) * 16;
+#pragma unroll
+        for (int w = 0; w < SOLWEIG_MASK_WORDS; ++w) {
+            const uint32_t m = (veg_half ? (sw[w] & vw[w]) : (sw[w] & ~vw[w])) & valid[w];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                *reinterpret_cast<uint4*>(rowp + (w * 4 + j) * 128) = expand8((m >> (8 * j)) & 0xFFu);
+        }
+    };
+    auto issue = [&](int st) {  // thread 0: sky x (hi, lo) and vegetation x (c hi, c lo) into stage st
+        tc::fence_after_sync();
+        const uint32_t acc = tmem + (uint32_t)(st * g.nb);
+        const uint32_t as0 = tc::smem_addr(smem + 2 * st * kABytes), av0 = as0 + kABytes;
+#pragma unroll 1
+        for (int k = 0; k < kK / 16; ++k) {
+            const uint64_t bh = tc::smem_desc(b_hi_addr + k * 256, 128, kSBO);
+            const uint64_t bl = tc::smem_desc(b_hi_addr + bbytes + k * 256, 128, kSBO);
+            const uint64_t ch = tc::smem_desc(b_hi_addr + 2 * bbytes + k * 256, 128, kSBO);
+            const uint64_t cl = tc::smem_desc(b_hi_addr + 3 * bbytes + k * 256, 128, kSBO);
+            const uint64_t as = tc::smem_desc(as0 + k * 256, 128, kSBO);
+            const uint64_t av = tc::smem_desc(av0 + k * 256, 128, kSBO);
+            tc::mma_bf16(acc, as, bh, idesc, k > 0);
+            tc::mma_bf16(acc, as, bl, idesc, true);
+            tc::mma_bf16(acc, av, ch, idesc, true);
+            tc::mma_bf16(acc, av, cl, idesc, true);
+        }
+        tc::mma_commit(&bar[st]);
+    };
+
+    uint32_t parity[2] = {0u, 0u};
+    int pending = 0;  // stages with committed MMAs not yet waited for
+    bool failed = false;
+    if (my > 0) {
+        load(first);
+        expand(0);
+        if (my > 1) load(first + stride);
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) issue(0);
+        pending = 1;
+    }
+    for (long long i = 0; i < my; ++i) {
+        const int st = (int)(i & 1);
+        const long long t = first + i * stride;
+        if (i + 1 < my) {
+            expand(st ^ 1);  // its masks were loaded one iteration ago
+            if (i + 2 < my) load(t + 2 * stride);
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();  // stage st ^ 1 expanded; its accumulator read out last iteration
+        if (i + 1 < my) {
+            if (tid == 0) issue(st ^ 1);
+            pending |= 1 << (st ^ 1);
+        }
+        const bool ok = tc::mbar_wait(&bar[st], parity[st], kWaitPolls);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        parity[st] ^= 1u;
+        pending &= ~(1 << st);
+        tc::fence_after_sync();
+        const int q = warp & 3;
+        const uint32_t lane_base = tmem + (uint32_t)(st * g.nb) + ((uint32_t)(q * 32) << 16);
+        const long long p = t * kARows + q * 32 + lane;
+        const bool in = p < g.px;
+        for (int c0 = 8 * (warp >> 2); c0 < g.ncols; c0 += 16) {
+            float v[8];
+            tc::tmem_ld8(lane_base + c0, v);
+            tc::tmem_wait_ld();
+            if (in) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (c0 + k < g.ncols) g.out[(long long)(c0 + k) * g.px + p] = v[k];
+            }
+        }
+    }
+    if (failed) {
+        if (tid == 0) raise_day_flag(g.error, 1);
+        // let committed MMAs finish before their columns are freed
+        for (int st = 0; st < 2; ++st)
+            if (pending & (1 << st)) tc::mbar_wait(&bar[st], parity[st], kWaitPolls);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -1159,6 +1319,21 @@ void launch_day_gvf(int ty, const SolweigScene& S, const SolweigHour* hours, int
 
 int launch_gemm(const uint32_t* masks, long long px, int patches, const __nv_bfloat16* b, int ncols, int nb,
                 float* out, int* error, cudaStream_t st, int ctas_per_sm = 0, bool combined = false) {
+    if (combined && gemm_pipe_smem_bytes(nb) <= 227 * 1024) {
+        // the pipelined kernel: one CTA per SM (its shared memory)
+        const size_t smem = gemm_pipe_smem_bytes(nb);
+        set_smem_attr((const void*)patch_gemm_pipe_kernel, smem);
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long long ntiles = (px + kARows - 1) / kARows;
+        long long grid = sms > 0 ? sms : 1;
+        if (grid > ntiles) grid = ntiles;
+        GemmArgs g{masks, px, patches, b, ncols, nb, out, error, 1};
+        patch_gemm_pipe_kernel<<<(unsigned)grid, kPipeThreads, smem, st>>>(g);
+        SOLWEIG_CHECK_LAUNCH("patch_gemm_pipe_kernel");
+        return SOLWEIG_OK;
+    }
     const size_t smem = gemm_smem_bytes(nb, combined);
     SOLWEIG_CHECK_ARG(smem <= 227 * 1024, "patch contraction: %d weight columns need %zu bytes of shared memory",
                       ncols, smem);

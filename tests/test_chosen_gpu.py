@@ -61,6 +61,42 @@ def test_patch_sums_match_fp64(cuda, px, ncols):
     assert np.max(np.abs(got[ncols:].T - veg) / scale) < SUM_RTOL
 
 
+def test_day_patch_sums_match_fp64(cuda):
+    """The batched day's contraction (pipelined tcgen05 kernel: two operand
+    stages, two tensor-memory accumulators, several tiles per CTA and a
+    partial last tile) against FP64 sums of the same masks and the day's
+    FP64 weights: sky + 0.03 x vegetation, every pixel and hour."""
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic
+    sc = synthetic.make_scene(300, 260, seed=9)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, seed=1)
+    day = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0)
+    day.run_day(met)
+    torch.cuda.synchronize()
+    assert day.error_flag() == 0
+    sums = day.patch_sums().to(torch.float64)
+    L = scene.layout.host
+    P = L.count
+    words = scene.masks.view(torch.int32).view(10, -1).to(torch.int64) & 0xFFFFFFFF
+    bit = torch.arange(P, device=words.device)
+    Sb = (words[bit // 32] >> (bit % 32)[:, None]) & 1
+    Vb = (words[5 + bit // 32] >> (bit % 32)[:, None]) & 1
+    sky = (Sb * (1 - Vb)).to(torch.float64).T
+    veg = (Sb * Vb).to(torch.float64).T
+    W = np.zeros((2 * 24, P))
+    for h, s_ in enumerate(day.last_scalars):
+        if s_.lv is not None:
+            lum = s_.lv[:, 2]
+            W[2 * h] = lum
+            W[2 * h + 1] = lum * L.cos_alt * L.steradian
+    Wt = torch.from_numpy(W).to(words.device)
+    want = sky @ Wt.T + 0.03 * (veg @ Wt.T)
+    scale = Wt.abs().sum(dim=1).clamp_min(1e-30)
+    assert torch.isfinite(sums).all()
+    assert ((sums.T - want).abs() / scale).max().item() < SUM_RTOL
+
+
 @pytest.fixture(scope="module")
 def scene64():
     from solweig_cuda_b200 import engine, synthetic
