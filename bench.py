@@ -226,7 +226,7 @@ STAGE_LIMITER = {
     "day_gvf_kernel": "instruction issue of the 18 x 22 walks and the block barriers of the 4-hour passes "
                       "(shared-memory wavefronts about half of their peak)",
     "day_tables_kernel": "negligible (one block per hour)",
-    "patch_gemm_kernel": "tensor pipe and the FP32 sum stores",
+    "patch_gemm_kernel": "expansion of the mask bits into the BF16 operand stages (the MMAs overlap it)",
     "day_radiation_kernel": "latency of the per-pixel hour loop",
 }
 
@@ -235,9 +235,9 @@ def _stage_kernels(cfg):
     """The kernel that does the work of each timed stage for a launch config."""
     return {
         "day_shadow_kernel": "day_sweep_tma_kernel" if cfg.sweep_window else "day_shadow_kernel",
-        "day_gvf_kernel": {2: "day_gvf_hv8_kernel", 1: "day_gvf_hv_kernel"}.get(cfg.gvf_hours, "day_gvf_kernel"),
+        "day_gvf_kernel": "day_gvf_hv_kernel" if cfg.gvf_hours == 1 else "day_gvf_kernel",
         "day_tables_kernel": "day_tables_kernel",
-        "patch_gemm_kernel": "patch_gemm_kernel",
+        "patch_gemm_kernel": "patch_gemm_pipe_kernel",  # the combined sums of <= 24 hours
         "day_radiation_kernel": "day_radiation_kernel",
     }
 
