@@ -210,8 +210,10 @@ int solweig_svf_ex(const double* dsm, const double* vegdem, const double* vegdem
 /* solweig_svf_ex with a 256-byte aligned device work buffer of
  * solweig_svf_work_bytes(rows, cols) bytes (no counterpart in the reference):
  * per word of 32 patches, upper bounds of the heights ahead along each patch
- * ray let the visibility walks stop early, and per-row / per-column exit steps
- * drop their bounds checks; the masks and planes are identical. */
+ * ray let the visibility walks stop early, per-row / per-column exit steps
+ * drop their bounds checks, and 16-byte step records (linear offset, dz)
+ * replace the offset and dz tables in the walks when capacity <= max(rows,
+ * cols) + 2; the masks and planes are identical. */
 int64_t solweig_svf_work_bytes(int rows, int cols);
 int solweig_svf_ex2(const double* dsm, const double* vegdem, const double* vegdem2,
                     const void* geo32, const uint8_t* flags, int rows, int cols, int patches,

@@ -30,7 +30,8 @@ struct SvfRayParams {
 // cols]; the walk then stops on the ceilings and, with geo32, needs no
 // bounds checks.
 // WALK: 0 float64 rasters, 1 packed geometry, 2 packed geometry without
-// bounds checks (`exits` given).
+// bounds checks (`exits` given), 3 as 2 with the word's step records (`rec`,
+// kmax per patch, ray_records_block) instead of the offset and dz tables.
 // 32 registers (8 blocks per SM): the walks are latency-bound and full
 // occupancy outweighs the few spills (SVF 5.7 ms faster at 2000^2 than at
 // 40 registers).
@@ -39,7 +40,8 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
     const int2* __restrict__ ray, const double* __restrict__ dz, const int32_t* __restrict__ lengths,
-    uint32_t* __restrict__ masks, int word0, const float* __restrict__ ceiling, const int* __restrict__ exits) {
+    uint32_t* __restrict__ masks, int word0, const float* __restrict__ ceiling, const int* __restrict__ exits,
+    const longlong2* __restrict__ rec = nullptr, int kmax = 0) {
     __shared__ uint8_t state[kSvfPatchGroup][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long pixels = (long long)prm.rows * prm.cols;
@@ -62,11 +64,12 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
             const int K = lengths[patch];
             const float* ceil_j = ceiling ? ceiling + (long long)j * pixels : nullptr;
             ShadowResult s;
-            if (WALK == 2) {
+            if (WALK >= 2) {
                 const int* e = exits + (long long)j * (prm.rows + prm.cols);
                 const int kend = min(K, min(__ldg(&e[r]), __ldg(&e[prm.rows + c])));
-                s = shadow_walk_packed<false>(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base,
-                                              nullptr, K, kend, prm.hmax, ceil_j);
+                s = shadow_walk_packed<WALK == 3>(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base,
+                                                  WALK == 3 ? rec + (long long)j * kmax : nullptr, K, kend,
+                                                  prm.hmax, ceil_j);
             } else if (WALK == 1) {
                 s = shadow_walk_geo(GeoF32x4{geo32}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
                                     dz + base, K, prm.hmax, true, ceil_j);
@@ -275,30 +278,40 @@ extern "C" int solweig_svf_pack(const float* shmat, const float* vegmat, const f
 // Blocks of the visibility kernel: 8 x 4 pixel tiles.
 unsigned svf_tiles(int rows, int cols) { return (unsigned)(((cols + 7) / 8) * ((rows + 3) / 4)); }
 
-// first_outside tables of a group of patches: block j = patch0 + j.
+// first_outside tables of a group of patches: block j = patch0 + j; with
+// rec also the patches' step records (kmax >= every length).
 __global__ void __launch_bounds__(1024) patch_ray_exits_kernel(int rows, int cols, const int2* __restrict__ rays,
+                                                               const double* __restrict__ dz,
                                                                const int32_t* __restrict__ lengths, int capacity,
-                                                               int patch0, int count, int* __restrict__ exits) {
+                                                               int patch0, int count, int* __restrict__ exits,
+                                                               longlong2* __restrict__ rec, int kmax) {
     const int j = blockIdx.x;
     if (j >= count) return;
     const int patch = patch0 + j;
     ray_exits_block(rays + (long long)patch * capacity, lengths[patch], rows, cols,
                     exits + (long long)j * (rows + cols));
+    if (rec != nullptr)
+        ray_records_block(rays + (long long)patch * capacity, dz + (long long)patch * capacity,
+                          min(lengths[patch], kmax), cols, rec + (long long)j * kmax);
 }
 
 // Work of solweig_svf_ex2: 4 dilated height planes, the 32 ray-ceiling
-// planes of one patch word and its 32 first-outside tables.
+// planes of one patch word, its 32 first-outside tables and its step
+// records (kmax = max(rows, cols) + 2 per patch, >= every ray's length).
 struct SvfWork {
-    long long dil, ceil, exits, total;
+    long long dil, ceil, exits, rec, total;
+    int kmax;
 };
 
 SvfWork svf_work_layout(int rows, int cols) {
     const long long px = (long long)rows * cols;
     SvfWork w{};
+    w.kmax = (rows > cols ? rows : cols) + 2;
     w.dil = 0;
     w.ceil = (4LL * 4 * px + 255) & ~255LL;
     w.exits = (w.ceil + 4LL * kSvfPatchGroup * px + 255) & ~255LL;
-    w.total = w.exits + 4LL * kSvfPatchGroup * (rows + cols);
+    w.rec = (w.exits + 4LL * kSvfPatchGroup * (rows + cols) + 255) & ~255LL;
+    w.total = w.rec + 16LL * kSvfPatchGroup * w.kmax;
     return w;
 }
 
@@ -384,6 +397,8 @@ int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, con
         float* dil = reinterpret_cast<float*>(wb + w.dil);
         float* ceil = reinterpret_cast<float*>(wb + w.ceil);
         int* exits = reinterpret_cast<int*>(wb + w.exits);
+        // step records when every ray fits kmax (the host's ray tables do)
+        longlong2* rec = (g4 && capacity <= w.kmax) ? reinterpret_cast<longlong2*>(wb + w.rec) : nullptr;
         SolweigScene S{};
         S.rows = rows;
         S.cols = cols;
@@ -401,12 +416,16 @@ int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, con
             patch_ray_ceiling_kernel<<<cgrid, dim3(kCeilLanes, kCeilWarps), 0, st>>>(S, rays, ray_dz, lengths,
                                                                                      capacity, p0, cnt, dil, ceil);
             SOLWEIG_CHECK_LAUNCH("patch_ray_ceiling_kernel");
-            patch_ray_exits_kernel<<<cnt, 1024, 0, st>>>(rows, cols, rays, lengths, capacity, p0, cnt, exits);
+            patch_ray_exits_kernel<<<cnt, 1024, 0, st>>>(rows, cols, rays, ray_dz, lengths, capacity, p0, cnt, exits,
+                                                          rec, w.kmax);
             SOLWEIG_CHECK_LAUNCH("patch_ray_exits_kernel");
             dim3 grid(svf_tiles(rows, cols), 1);
-            if (g4) svf_visibility_kernel<2><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
-                                                                              rays, ray_dz, lengths, masks, wd, ceil,
-                                                                              exits);
+            if (rec) svf_visibility_kernel<3><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
+                                                                               rays, ray_dz, lengths, masks, wd, ceil,
+                                                                               exits, rec, w.kmax);
+            else if (g4) svf_visibility_kernel<2><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags,
+                                                                                   rp, rays, ray_dz, lengths, masks,
+                                                                                   wd, ceil, exits);
             else svf_visibility_kernel<0><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
                                                                            rays, ray_dz, lengths, masks, wd, ceil,
                                                                            nullptr);
