@@ -41,6 +41,13 @@
 // oriented minor index, so a warp's 32 lanes (consecutive Y) read 32
 // consecutive floats.
 //
+// Window maxima: with the ceiling the scan also writes, per pixel,
+// M(X, N) = max over X' in [X, X + kCeilSkip) of Hd(X', N) (no discount).  A
+// ray through q_k at step k >= 1 meets q_{k..k+kCeilSkip-1} within +-W lines,
+// so H(q_j) - dz_{j-1} <= M(q_k) - dz_{k-1} for those steps: when that is
+// <= dsm_p none of their compares is above the pixel and a walk (not of a
+// wall pixel) may skip them.  The planes hold (C, M) as float2 per pixel.
+//
 // Scan layout: a block owns 32 consecutive sheared lines (one per lane) and
 // splits the major axis into 16 segments (one per warp; 512 threads, so two
 // blocks fit per SM).  Phase 1 scans each
@@ -178,11 +185,32 @@ __device__ __forceinline__ float ceiling_sample(const float* __restrict__ plane,
 }
 
 // One backward scan of [x0, x1) from g over the lane's sheared line; with OUT,
-// writes every pixel of the line.  A batch of loads is issued before the
-// dependent chain consumes it.
+// writes every pixel of the line: (ceiling, window maximum).  A batch of loads
+// is issued before the dependent chain consumes it.  win[i] holds Hd at
+// x + 1 + i (the samples of the window after x), preloaded at the segment end.
 template <bool OUT>
 __device__ __forceinline__ float ceiling_run(const float* __restrict__ plane, const CeilingFrame& f, int cols,
-                                             int line, int x0, int x1, float g, float* __restrict__ out) {
+                                             int line, int x0, int x1, float g, float2* __restrict__ out) {
+    const float ninf = __int_as_float(0xff800000);
+    float win[kCeilSkip - 1];
+#pragma unroll
+    for (int i = 0; i < kCeilSkip - 1; ++i) {
+        win[i] = ninf;
+        if (OUT && x1 + i < f.nx) {
+            const int xx = x1 + i;
+            const int a = f.s_major > 0 ? xx : f.nx - 1 - xx;
+            win[i] = ceiling_sample(plane, f, a, line + (int)(((long long)xx * f.m) / f.d));
+        }
+    }
+    auto emit = [&](int x, int y, float v) {
+        float m = v;
+#pragma unroll
+        for (int i = 0; i < kCeilSkip - 1; ++i) m = fmaxf(m, win[i]);
+#pragma unroll
+        for (int i = kCeilSkip - 2; i > 0; --i) win[i] = win[i - 1];
+        win[0] = v;
+        if (OUT && y >= 0 && y < f.nb) out[ceiling_pixel(f, cols, x, y)] = make_float2(g, m);
+    };
     ShearCursor cur(max(x1 - 1, 0), f.m, f.d);
     int x = x1 - 1;
     for (; x - (kCeilBatch - 1) >= x0; x -= kCeilBatch) {
@@ -198,14 +226,15 @@ __device__ __forceinline__ float ceiling_run(const float* __restrict__ plane, co
 #pragma unroll
         for (int u = 0; u < kCeilBatch; ++u) {
             g = fmaxf(v[u], __fsub_ru(g, f.delta));
-            if (OUT && y[u] >= 0 && y[u] < f.nb) out[ceiling_pixel(f, cols, x - u, y[u])] = g;
+            if (OUT) emit(x - u, y[u], v[u]);
         }
     }
     for (; x >= x0; --x) {
         const int yy = line + cur.rx;
         const int a = f.s_major > 0 ? x : f.nx - 1 - x;
-        g = fmaxf(ceiling_sample(plane, f, a, yy), __fsub_ru(g, f.delta));
-        if (OUT && yy >= 0 && yy < f.nb) out[ceiling_pixel(f, cols, x, yy)] = g;
+        const float v = ceiling_sample(plane, f, a, yy);
+        g = fmaxf(v, __fsub_ru(g, f.delta));
+        if (OUT) emit(x, yy, v);
         cur.step_down(f.m, f.d);
     }
     return g;
@@ -213,7 +242,7 @@ __device__ __forceinline__ float ceiling_run(const float* __restrict__ plane, co
 
 // Both phases for one block of 32 sheared lines (see the file comment).
 __device__ __forceinline__ void ceiling_scan(const float* __restrict__ plane, const CeilingFrame& f, int cols,
-                                             int line0, float (*s_seg)[kCeilLanes], float* __restrict__ out) {
+                                             int line0, float (*s_seg)[kCeilLanes], float2* __restrict__ out) {
     const int seg = (f.nx + kCeilWarps - 1) / kCeilWarps;
     const int w = threadIdx.y;
     const int x0 = min(f.nx, w * seg), x1 = min(f.nx, x0 + seg);
@@ -279,7 +308,7 @@ __global__ void __launch_bounds__(256) ceiling_dilate_kernel(SolweigScene S, flo
 // block returns together.  Tables the frame does not fit give a +inf plane.
 __device__ __forceinline__ void ray_ceiling_block(const SolweigScene& S, const int2* __restrict__ ray,
                                                   const double* __restrict__ dz, int K,
-                                                  const float* __restrict__ dil, float* __restrict__ out,
+                                                  const float* __restrict__ dil, float2* __restrict__ out,
                                                   float (*s_seg)[kCeilLanes]) {
     if (K < kCeilMinSteps) return;
     const long long n = (long long)S.rows * S.cols;
@@ -288,7 +317,7 @@ __device__ __forceinline__ void ray_ceiling_block(const SolweigScene& S, const i
     if (!f.ok || f.band > 2) {
         for (long long p = (long long)blockIdx.x * blockDim.x * blockDim.y + tid; p < n;
              p += (long long)gridDim.x * blockDim.x * blockDim.y)
-            out[p] = __int_as_float(0x7f800000);
+            out[p] = make_float2(__int_as_float(0x7f800000), __int_as_float(0x7f800000));
         return;
     }
     const int line_first = blockIdx.x * kCeilLanes;
@@ -304,7 +333,7 @@ __device__ __forceinline__ void ray_ceiling_block(const SolweigScene& S, const i
 // dilated planes of ceiling_dilate_kernel.
 static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceiling_kernel(
     SolweigScene S, const SolweigHour* __restrict__ hours, const float* __restrict__ dil,
-    float* __restrict__ ceiling) {
+    float2* __restrict__ ceiling) {
     __shared__ float s_seg[kCeilWarps][kCeilLanes];
     const SolweigHour& h = hours[blockIdx.z];
     if (!h.daytime) return;
@@ -317,7 +346,7 @@ static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) day_ray_ceilin
 static __global__ void __launch_bounds__(kCeilLanes * kCeilWarps) patch_ray_ceiling_kernel(
     SolweigScene S, const int2* __restrict__ rays, const double* __restrict__ dz,
     const int32_t* __restrict__ lengths, int capacity, int patch0, int count, const float* __restrict__ dil,
-    float* __restrict__ ceiling) {
+    float2* __restrict__ ceiling) {
     __shared__ float s_seg[kCeilWarps][kCeilLanes];
     const int j = blockIdx.z, patch = patch0 + j;
     if (j >= count) return;

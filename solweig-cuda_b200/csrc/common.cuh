@@ -39,6 +39,10 @@ inline unsigned blocks_for(long long n, int threads) {
     return static_cast<unsigned>((n + threads - 1) / threads);
 }
 
+// Steps covered by the window maximum of the ray-ceiling planes (ceiling.cuh):
+// a walk may skip that many steps at once on it (shadow.cuh).
+constexpr int kCeilSkip = 8;
+
 __device__ __forceinline__ bool in_raster(int r, int c, int rows, int cols) {
     return (unsigned)r < (unsigned)rows && (unsigned)c < (unsigned)cols;
 }

@@ -173,12 +173,13 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
     }
     if (part == kDaySweep) {
         const int nh = h1 - h0;
-        // The ceiling planes (4 B per pixel-hour) live in the GVF region (12 B
+        // The ceiling planes (8 B per pixel-hour: ceiling and window maximum)
+        // live in the GVF region (12 B
         // per pixel-hour) and the four dilated height planes (16 B per pixel)
         // in the patch-sum region (at least 16 B per pixel): both are consumed
         // by the sweep before the GVF kernels and the contraction write those
         // regions.
-        float* ceiling = cfg.no_ceiling ? nullptr : gvf;
+        float2* ceiling = cfg.no_ceiling ? nullptr : reinterpret_cast<float2*>(gvf);
         float* dil = sums;
         if (h0 == 0) {
             cudaMemsetAsync(err, 0, sizeof(int), st);  // the day's error flag
@@ -201,11 +202,13 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
             SOLWEIG_CHECK_LAUNCH("day_ray_ceiling_kernel");
         }
         // first-outside steps of every row and column per hour (4 B each), in
-        // the GVF region after the ceiling planes (8 B per pixel-hour left)
-        int* exits = reinterpret_cast<int*>(wb + w.gvf + 4LL * px * nhours) + (long long)h0 * (S.rows + S.cols);
+        // the GVF region after the ceiling planes (4 B per pixel-hour left; a
+        // raster one pixel wide spills a few bytes into the next region, free
+        // until the GVF stage)
+        int* exits = reinterpret_cast<int*>(wb + w.gvf + 8LL * px * nhours) + (long long)h0 * (S.rows + S.cols);
         // then the hours' step records (16 B per step, at most max(rows, cols) + 2
         // steps per hour), when they fit before the end of the GVF region
-        const long long rec_at = (w.gvf + 4LL * px * nhours + 4LL * (S.rows + S.cols) * nhours + 15) & ~15LL;
+        const long long rec_at = (w.gvf + 8LL * px * nhours + 4LL * (S.rows + S.cols) * nhours + 15) & ~15LL;
         const int kmax = (S.rows > S.cols ? S.rows : S.cols) + 2;
         longlong2* rec = nullptr;
         if (rec_at + 16LL * kmax * nhours <= w.gvf + 12LL * px * nhours)
@@ -218,7 +221,7 @@ int day_batched_impl(const SolweigScene* scene, const SolweigSkyLayout* layout, 
             const int rc = sweep_geo_map(S, win, &map);
             if (rc) return rc;
             dim3 grid(blocks_for(S.cols, kSwTile), blocks_for(S.rows, kSwTile), nh);
-            const float* ceil0 = ceiling ? ceiling + h0 * px : nullptr;
+            const float2* ceil0 = ceiling ? ceiling + h0 * px : nullptr;
             if (win == 40) {
                 set_smem_attr((const void*)day_sweep_tma_kernel<40>, sweep_smem_bytes<40>());
                 day_sweep_tma_kernel<40><<<grid, kSwThreads, sweep_smem_bytes<40>(), st>>>(

@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256, 6) day_shadow_kernel(SolweigScene S,
                                                                    const SolweigHour* __restrict__ hours,
                                                                    float4* __restrict__ quads,
                                                                    float* __restrict__ lup_first,
-                                                                   const float* __restrict__ ceiling,
+                                                                   const float2* __restrict__ ceiling,
                                                                    const int* __restrict__ exits,
                                                                    const longlong2* __restrict__ rec, int kmax) {
     const int z = blockIdx.z;

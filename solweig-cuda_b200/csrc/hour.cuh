@@ -65,7 +65,7 @@ __device__ __forceinline__ float4 quad_from_walk(const SolweigScene& S, const So
 template <bool REC = false>
 __device__ __forceinline__ float4 shadow_quad_pixel(const SolweigScene& S, const SolweigHour& h, int r, int c,
                                                   float4* __restrict__ quad, float* __restrict__ lup_first,
-                                                  const float* __restrict__ ceiling = nullptr,
+                                                  const float2* __restrict__ ceiling = nullptr,
                                                   const int* __restrict__ exits = nullptr,
                                                   const longlong2* __restrict__ rec = nullptr) {
     const long long p = (long long)r * S.cols + c;

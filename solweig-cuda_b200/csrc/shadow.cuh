@@ -25,7 +25,12 @@
 //   * with a ray-ceiling plane (ceiling.cuh), every 4th step from step 4 on:
 //     ceiling(q_k) - dz_{k-1} (rounded up) < dsm_p bounds every later
 //     sample's h - dz_{j-1} below the pixel (dsm_p >= 0; for wall pixels
-//     also <= topmax >= 0), so nothing further can change.
+//     also <= topmax >= 0), so nothing further can change;
+//   * (packed walk) at the same steps, window maximum(q_k) - dz_{k-1}
+//     (rounded up) <= dsm_p bounds the next kCeilSkip samples' h - dz_{j-1}
+//     by the pixel: none of their compares is above it, so a walk of a pixel
+//     that is no wall skips them (f, topmax unused off walls, the flags only
+//     carry: ever picks up veg, as each unshadowed step would).
 // Once a sample leaves the raster it never re-enters (the offsets grow
 // monotonically), so the first outside step is applied and the loop ends.
 #pragma once
@@ -71,7 +76,7 @@ template <typename Geo>
 __device__ __forceinline__ ShadowResult shadow_walk_geo(
     const Geo& geo, int rows, int cols, int r, int c, double a, double top_p, bool bush, double wall,
     const int2* __restrict__ ray, const double* __restrict__ dz, int steps, double hmax,
-    bool vegetation, const float* __restrict__ ceiling = nullptr) {
+    bool vegetation, const float2* __restrict__ ceiling = nullptr) {
     ShadowResult s;
     s.f = a;
     s.topmax = top_p;
@@ -98,7 +103,7 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
             break;
         }
         if (ceiling != nullptr && k >= 4 && (k & 3) == 0) {
-            const double e = __dsub_ru((double)__ldg(&ceiling[q]), dz_prev);
+            const double e = __dsub_ru((double)__ldg(&ceiling[q]).x, dz_prev);
             if (a >= 0.0 && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) {
                 k = steps;
                 break;
@@ -157,11 +162,11 @@ __device__ __forceinline__ ShadowResult shadow_walk_geo(
 // no per-step test.  With REC the hour's steps come as 16-byte records
 // {linear offset o.x * cols + o.y, dz bit pattern} (one uniform load per
 // step, ray_records_block); otherwise from the (dx, dy) and dz tables.
-template <bool REC>
+template <bool REC, bool SKIP = true>
 __device__ __forceinline__ ShadowResult shadow_walk_packed(
     const float4* __restrict__ geo, int cols, long long p, double a, double top_p, bool bush, double wall,
     const int2* __restrict__ ray, const double* __restrict__ dz, const longlong2* __restrict__ rec, int steps,
-    int kend, double hmax, const float* __restrict__ ceiling) {
+    int kend, double hmax, const float2* __restrict__ ceiling) {
     ShadowResult s;
     s.f = a;
     s.topmax = top_p;
@@ -173,7 +178,7 @@ __device__ __forceinline__ ShadowResult shadow_walk_packed(
     const double clear = nonneg ? nextafter(hmax - a, __longlong_as_double(0x7ff0000000000000ll))
                                 : __longlong_as_double(0x7ff0000000000000ll);
     const float4* __restrict__ gp = geo + p;
-    const float* __restrict__ cp = ceiling != nullptr ? ceiling + p : nullptr;
+    const float2* __restrict__ cp = ceiling != nullptr ? ceiling + p : nullptr;
     double dz_prev = 0.0;
     bool final = false;
     int k = 0;
@@ -197,10 +202,18 @@ __device__ __forceinline__ ShadowResult shadow_walk_packed(
                 break;
             }
             if (u == 0 && cp != nullptr && k >= 4) {
-                const double e = __dsub_ru((double)__ldg(cp + off), dz_prev);
+                const float2 cm = __ldg(cp + off);
+                const double e = __dsub_ru((double)cm.x, dz_prev);
                 if (nonneg && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) {
                     final = true;
                     break;
+                }
+                if (SKIP && !is_wall && nonneg && k + kCeilSkip <= kend && __dsub_ru((double)cm.y, dz_prev) <= a) {
+                    // steps k .. k + kCeilSkip - 1 change nothing but the carried flags
+                    s.ever = s.ever || s.veg;
+                    k += kCeilSkip;
+                    dz_prev = REC ? __longlong_as_double(__ldg(rec + k - 1).y) : __ldg(&dz[k - 1]);
+                    break;  // the next group starts at k (still a multiple of 4)
                 }
             }
             const float4 v = __ldg(gp + off);

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
     const int2* __restrict__ ray, const double* __restrict__ dz, const int32_t* __restrict__ lengths,
-    uint32_t* __restrict__ masks, int word0, const float* __restrict__ ceiling, const int* __restrict__ exits,
+    uint32_t* __restrict__ masks, int word0, const float2* __restrict__ ceiling, const int* __restrict__ exits,
     const longlong2* __restrict__ rec = nullptr, int kmax = 0) {
     __shared__ uint8_t state[kSvfPatchGroup][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
         if (valid && patch < prm.patches) {
             const long long base = (long long)patch * prm.capacity;
             const int K = lengths[patch];
-            const float* ceil_j = ceiling ? ceiling + (long long)j * pixels : nullptr;
+            const float2* ceil_j = ceiling ? ceiling + (long long)j * pixels : nullptr;
             ShadowResult s;
             if (WALK >= 2) {
                 const int* e = exits + (long long)j * (prm.rows + prm.cols);
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(1024) patch_ray_exits_kernel(int rows, int col
 }
 
 // Work of solweig_svf_ex2: 4 dilated height planes, the 32 ray-ceiling
-// planes of one patch word, its 32 first-outside tables and its step
+// planes (ceiling and window maximum per pixel) of one patch word, its 32 first-outside tables and its step
 // records (kmax = max(rows, cols) + 2 per patch, >= every ray's length).
 struct SvfWork {
     long long dil, ceil, exits, rec, total;
@@ -309,7 +309,7 @@ SvfWork svf_work_layout(int rows, int cols) {
     w.kmax = (rows > cols ? rows : cols) + 2;
     w.dil = 0;
     w.ceil = (4LL * 4 * px + 255) & ~255LL;
-    w.exits = (w.ceil + 4LL * kSvfPatchGroup * px + 255) & ~255LL;
+    w.exits = (w.ceil + 8LL * kSvfPatchGroup * px + 255) & ~255LL;
     w.rec = (w.exits + 4LL * kSvfPatchGroup * (rows + cols) + 255) & ~255LL;
     w.total = w.rec + 16LL * kSvfPatchGroup * w.kmax;
     return w;
@@ -395,7 +395,7 @@ int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, con
         SOLWEIG_CHECK_ARG(((uintptr_t)work & 255) == 0, "solweig_svf_ex2: work buffer not 256-byte aligned");
         char* wb = static_cast<char*>(work);
         float* dil = reinterpret_cast<float*>(wb + w.dil);
-        float* ceil = reinterpret_cast<float*>(wb + w.ceil);
+        float2* ceil = reinterpret_cast<float2*>(wb + w.ceil);
         int* exits = reinterpret_cast<int*>(wb + w.exits);
         // step records when every ray fits kmax (the host's ray tables do)
         longlong2* rec = (g4 && capacity <= w.kmax) ? reinterpret_cast<longlong2*>(wb + w.rec) : nullptr;

@@ -123,7 +123,7 @@ __device__ __forceinline__ ShadowResult shadow_walk_window(
     bool in, const float4* __restrict__ win, int wpitch, int wbase, int kw, double wclear,
     const float4* __restrict__ geo, int cols, long long p, double a, double top_p, bool bush, double wall,
     const int2* __restrict__ ray, const double* __restrict__ dz, int steps, int kend, double hmax,
-    const float* __restrict__ ceiling) {
+    const float2* __restrict__ ceiling) {
     ShadowResult s;
     s.f = a;
     s.topmax = top_p;
@@ -160,7 +160,7 @@ __device__ __forceinline__ ShadowResult shadow_walk_window(
     auto settled = [&](long long q, int k, double dzk) {
         if (dz_prev >= clear && (!is_wall || (s.topmax >= 0.0 && hmax - dzk <= s.topmax))) return true;
         if (ceiling != nullptr && k >= 4 && (k & 3) == 0) {
-            const double e = __dsub_ru((double)__ldg(&ceiling[q]), dz_prev);
+            const double e = __dsub_ru((double)__ldg(&ceiling[q]).x, dz_prev);
             if (nonneg && e < a && (!is_wall || (s.topmax >= 0.0 && e <= s.topmax))) return true;
         }
         return false;
@@ -235,7 +235,7 @@ template <int WIN>
 __global__ void __launch_bounds__(kSwThreads, WIN <= 40 ? 8 : 6)
     day_sweep_tma_kernel(const __grid_constant__ CUtensorMap geo_map, SolweigScene S,
                          const SolweigHour* __restrict__ hours, float4* __restrict__ quads,
-                         const float* __restrict__ ceiling, const int* __restrict__ exits,
+                         const float2* __restrict__ ceiling, const int* __restrict__ exits,
                          const float* __restrict__ tmax, int* __restrict__ error) {
     static_assert(WIN >= kSwTile && WIN <= 64, "window side");
     const SolweigHour& h = hours[blockIdx.z];
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kSwThreads, WIN <= 40 ? 8 : 6)
     const double top_p = in ? S.vegdem[p] : 0.0;
     // this hour's ray exits and ceiling plane
     const int* ex = exits + (long long)blockIdx.z * (S.rows + S.cols);
-    const float* ceil_h = ceiling ? ceiling + (long long)blockIdx.z * npx : nullptr;
+    const float2* ceil_h = ceiling ? ceiling + (long long)blockIdx.z * npx : nullptr;
     int kend = 0;
     if (in) kend = min(K, min(__ldg(&ex[r]), __ldg(&ex[S.rows + c])));
 

@@ -4,8 +4,12 @@ A numpy restatement of the construction (frame from the ray table, integer
 shear, dilation by the measured band, discounted backward maximum along each
 sheared line) checked against the property the sweep's early exit relies on:
 for every pixel p, every step k >= 1 of its ray inside the raster and every
-later step j,  H(q_j) - dz_{j-1} <= C(q_k) - dz_{k-1}.
+later step j,  H(q_j) - dz_{j-1} <= C(q_k) - dz_{k-1};  and the window
+maximum M (the largest sampled dilated height at X .. X + 7 of the line)
+against the property of the 8-step skip:  H(q_j) - dz_{j-1} <= M(q_k) -
+dz_{k-1}  for k <= j < k + 8.
 """
+SKIP = 8
 import numpy as np
 import pytest
 
@@ -56,17 +60,26 @@ def ceiling_planes(H, dxdy, dz):
     lines = nb + roff
     line = np.arange(lines) - roff               # sheared line N of each lane
     G = np.full(lines, -np.inf)
+    win = np.full((SKIP - 1, lines), -np.inf)    # samples at x + 1 .. x + SKIP - 1
     Co = np.empty_like(Hm)
+    Mo = np.empty_like(Hm)
     for x in range(nx - 1, -1, -1):
         a = x if f["s_major"] > 0 else nx - 1 - x
         y = line + R[x]
         near = (y >= -W) & (y < nb + W)
         yc = np.clip(y, 0, nb - 1)
         b = yc if f["s_minor"] > 0 else nb - 1 - yc
-        G = np.maximum(np.where(near, plane[a, b], -np.inf), G - f["delta"])
+        v = np.where(near, plane[a, b], -np.inf)
+        G = np.maximum(v, G - f["delta"])
+        M = np.maximum(v, win.max(axis=0))
+        win = np.vstack([v[None], win[:-1]])
         inside = (y >= 0) & (y < nb)
-        Co[a, np.where(f["s_minor"] > 0, y, nb - 1 - y)[inside]] = G[inside]
-    return (Co if f["rows_major"] else Co.T), f
+        col = np.where(f["s_minor"] > 0, y, nb - 1 - y)[inside]
+        Co[a, col] = G[inside]
+        Mo[a, col] = M[inside]
+    if not f["rows_major"]:
+        Co, Mo = Co.T, Mo.T
+    return Co, f, Mo
 
 
 def _check_bound(H, C, ray):
@@ -105,10 +118,37 @@ def test_ceiling_bounds_every_later_sample(seed):
         ray = rays.shadow_ray(float(az), alt, 1.0, float(H.max()), (rows, cols), True)
         if ray.steps < 5:
             continue
-        C, f = ceiling_planes(H, ray.dxdy, ray.dz)
+        C, f, M = ceiling_planes(H, ray.dxdy, ray.dz)
         assert f["band"] <= 2 and f["m"] <= f["d"]
         assert np.all(C >= H)            # the sample itself is in its own bound
         assert _check_bound(H, C, ray) >= 0.0, (az, alt)
+        assert _check_window(H, M, ray) >= 0.0, (az, alt)
+
+
+def _check_window(H, M, ray):
+    """Smallest slack of M(q_k) - dz_{k-1} - (H(q_j) - dz_{j-1}) over every
+    pixel, step k >= 1 inside the raster and k <= j < k + SKIP inside."""
+    rows, cols = H.shape
+    rr, cc = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+    K = ray.steps
+    hv, mv, inside = [], [], []
+    for j in range(K):
+        r2, c2 = rr + ray.dxdy[j][0], cc + ray.dxdy[j][1]
+        ok = (r2 >= 0) & (r2 < rows) & (c2 >= 0) & (c2 < cols)
+        if j:
+            ok &= inside[-1]
+        inside.append(ok)
+        R2, C2 = np.clip(r2, 0, rows - 1), np.clip(c2, 0, cols - 1)
+        hv.append(np.where(ok, H[R2, C2], -np.inf))
+        mv.append(np.where(ok, M[R2, C2], np.inf))
+    slack = np.inf
+    for k in range(1, K):
+        rhs = mv[k] - ray.dz[k - 1]
+        for j in range(k, min(K, k + SKIP)):
+            m = inside[j]
+            if m.any():
+                slack = min(slack, float(np.min(rhs[m] - (hv[j][m] - ray.dz[j - 1]))))
+    return slack
 
 
 def test_ceiling_cuts_the_walk_on_a_city():
@@ -119,7 +159,7 @@ def test_ceiling_cuts_the_walk_on_a_city():
     dsm = sc.dsm.astype(np.float64)
     H = np.maximum(dsm, np.where(sc.trees > 0, sc.trees + dsm, 0.0))
     ray = rays.shadow_ray(200.0, 35.0, 1.0, float(H.max()), H.shape, True)
-    C, _ = ceiling_planes(H, ray.dxdy, ray.dz)
+    C, _, _ = ceiling_planes(H, ray.dxdy, ray.dz)
     # steps needed by the global clearance vs by the ceiling at step 4, for ground pixels
     ground = dsm == 0
     clear_global = np.searchsorted(ray.dz, H.max())
