@@ -28,9 +28,10 @@
 //     also <= topmax >= 0), so nothing further can change;
 //   * (packed walk) at the same steps, window maximum(q_k) - dz_{k-1}
 //     (rounded up) <= dsm_p bounds the next kCeilSkip samples' h - dz_{j-1}
-//     by the pixel: none of their compares is above it, so a walk of a pixel
-//     that is no wall skips them (f, topmax unused off walls, the flags only
-//     carry: ever picks up veg, as each unshadowed step would).
+//     by the pixel: none of their compares is above it and f cannot grow, so
+//     the walk skips them when, for a wall pixel, the bound is also <= topmax
+//     (the canopy top seen stays final); only the carried flags move: ever
+//     picks up veg when unshadowed, as each step would.
 // Once a sample leaves the raster it never re-enters (the offsets grow
 // monotonically), so the first outside step is applied and the loop ends.
 #pragma once
@@ -208,7 +209,8 @@ __device__ __forceinline__ ShadowResult shadow_walk_packed(
                     final = true;
                     break;
                 }
-                if (SKIP && !is_wall && nonneg && k + kCeilSkip <= kend && __dsub_ru((double)cm.y, dz_prev) <= a) {
+                const double em = __dsub_ru((double)cm.y, dz_prev);
+                if (SKIP && nonneg && k + kCeilSkip <= kend && em <= a && (!is_wall || em <= s.topmax)) {
                     // steps k .. k + kCeilSkip - 1 change nothing but the carried flags
                     s.ever = s.ever || s.veg;
                     k += kCeilSkip;
