@@ -111,6 +111,33 @@ __device__ __forceinline__ float band_weighted(const uint32_t (&m)[SOLWEIG_MASK_
     return s;
 }
 
+// Patches of m in each band (popcounts of the band's bit ranges), and the
+// weighted sum of such counts.
+template <int OPT>
+__device__ __forceinline__ void band_counts(const uint32_t (&m)[SOLWEIG_MASK_WORDS], float (&c)[8]) {
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const int lo = Bands<OPT>::off(b), hi = Bands<OPT>::off(b + 1);
+        int n = 0;
+#pragma unroll
+        for (int wd = 0; wd < SOLWEIG_MASK_WORDS; ++wd) {
+            const int a = lo > wd * 32 ? lo : wd * 32;
+            const int e = hi < wd * 32 + 32 ? hi : wd * 32 + 32;
+            if (a < e) {
+                const uint32_t mask = (e - a == 32) ? 0xffffffffu : (((1u << (e - a)) - 1u) << (a - wd * 32));
+                n += __popc(m[wd] & mask);
+            }
+        }
+        c[b] = (float)n;
+    }
+}
+__device__ __forceinline__ float band_dot(const float (&c)[8], const float* w) {
+    float s = 0.f;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) s = fmaf(c[b], w[b], s);
+    return s;
+}
+
 // Number of entries of the ascending array a[0..n) that are <= t.
 __device__ __forceinline__ int count_le(const double* a, int n, double t) {
     int lo = 0;
@@ -1063,11 +1090,14 @@ __device__ __forceinline__ float wedge_fsh_f(float ta, float tan_zen) {
     const float hkil = 2.f * ba * ha;
     float ukil = 0.f;
     if (xa < 0.f) {
+        // phi = atan(za / qa) in [0, pi/2): cos and sin from the same triangle,
+        // 1 / hypot(qa, za) with qa^2 + za^2 = ba^2 + 3 qa^2 / 4
         const float qa = tan_zen / 2.f;
         const float za = sqrtf(ba * ba - qa * qa / 4.f);
         const float phi = atanf(za / qa);
-        const float cphi = cosf(phi);
-        const float area = (sinf(phi) - phi * cphi) / (1.f - cphi);
+        const float ih = rsqrtf(fmaf(qa, qa, za * za));
+        const float cphi = qa * ih, sphi = za * ih;
+        const float area = (sphi - phi * cphi) / (1.f - cphi);
         ukil = 2.f * ba * xa * area;
     }
     const float pi2 = 2.f * (float)kPi;
@@ -1159,8 +1189,11 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) day_radiation_kernel(
             m_lsun[w] = m_sun[w] & test;
             m_lshd[w] = bld[w] & (~test | m_shd[w]);
         }
-        const float lw_sun_c = band_weighted<OPT>(m_lsun, wcos), lw_sun_s = band_weighted<OPT>(m_lsun, wsin);
-        const float lw_shd_c = band_weighted<OPT>(m_lshd, wcos), lw_shd_s = band_weighted<OPT>(m_lshd, wsin);
+        float cnt_lsun[8], cnt_lshd[8];
+        band_counts<OPT>(m_lsun, cnt_lsun);
+        band_counts<OPT>(m_lshd, cnt_lshd);
+        const float lw_sun_c = band_dot(cnt_lsun, wcos), lw_sun_s = band_dot(cnt_lsun, wsin);
+        const float lw_shd_c = band_dot(cnt_lshd, wcos), lw_shd_s = band_dot(cnt_lshd, wsin);
         float ld_sky = 0.f, ls_sky = 0.f;
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
