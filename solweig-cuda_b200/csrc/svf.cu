@@ -90,6 +90,45 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
     }
 }
 
+// The step-record form (WALK 3) with one warp per 8 x 4 pixel tile walking
+// all patches of the word in turn (grid.x: tiles / 8, one word per launch):
+// the warps of a block carry similar work -- each walks all 32 patches of
+// its own pixels, so the uneven lengths of single walks (window skips,
+// ceiling exits) even out -- and each pixel's two bits are assembled in
+// registers, so no warp waits at a barrier.  Same walks, same bits.
+__global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_warp_kernel(
+    const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
+    const int32_t* __restrict__ lengths, uint32_t* __restrict__ masks, int word, const float2* __restrict__ ceiling,
+    const int* __restrict__ exits, const longlong2* __restrict__ rec, int kmax) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long pixels = (long long)prm.rows * prm.cols;
+    const int tiles_x = (prm.cols + 7) / 8;
+    const long long ntiles = (long long)tiles_x * ((prm.rows + 3) / 4);
+    const long long tile = (long long)blockIdx.x * kSvfWarps + warp;
+    if (tile >= ntiles) return;  // the whole warp
+    const int rr = (int)(tile / tiles_x) * 4 + (lane >> 3), cc = (int)(tile % tiles_x) * 8 + (lane & 7);
+    if (rr >= prm.rows || cc >= prm.cols) return;
+    const long long p = (long long)rr * prm.cols + cc;
+    const float4 g = __ldg(&geo32[p]);  // the packed geometry holds the exact heights
+    const double a = g.x, top_p = g.y;
+    const bool bush = flags[p] & 2;
+    uint32_t sbits = 0u, vbits = 0u;
+    for (int j = 0; j < kSvfPatchGroup; ++j) {
+        const int patch = word * kSvfPatchGroup + j;
+        if (patch >= prm.patches) break;
+        const int K = lengths[patch];
+        const int* e = exits + (long long)j * (prm.rows + prm.cols);
+        const int kend = min(K, min(__ldg(&e[rr]), __ldg(&e[prm.rows + cc])));
+        const ShadowResult s = shadow_walk_packed<true>(geo32, prm.cols, p, a, top_p, bush, 0.0, nullptr, nullptr,
+                                                        rec + (long long)j * kmax, K, kend, prm.hmax,
+                                                        ceiling + (long long)j * pixels);
+        sbits |= (s.shadowed ? 0u : 1u) << j;
+        vbits |= (s.ever ? 1u : 0u) << j;
+    }
+    masks[(long long)word * pixels + p] = sbits;
+    masks[((long long)SOLWEIG_MASK_WORDS + word) * pixels + p] = vbits;
+}
+
 struct SvfReduceParams {
     long long pixels;
     int nbands;
@@ -420,9 +459,8 @@ int svf_impl(const double* dsm, const double* vegdem, const double* vegdem2, con
                                                           rec, w.kmax);
             SOLWEIG_CHECK_LAUNCH("patch_ray_exits_kernel");
             dim3 grid(svf_tiles(rows, cols), 1);
-            if (rec) svf_visibility_kernel<3><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags, rp,
-                                                                               rays, ray_dz, lengths, masks, wd, ceil,
-                                                                               exits, rec, w.kmax);
+            if (rec) svf_visibility_warp_kernel<<<blocks_for(svf_tiles(rows, cols), kSvfWarps), 32 * kSvfWarps, 0,
+                                                   st>>>(g4, flags, rp, lengths, masks, wd, ceil, exits, rec, w.kmax);
             else if (g4) svf_visibility_kernel<2><<<grid, 32 * kSvfWarps, 0, st>>>(dsm, vegdem, vegdem2, g4, flags,
                                                                                    rp, rays, ray_dz, lengths, masks,
                                                                                    wd, ceil, exits);

@@ -107,8 +107,53 @@ def svf_rays(patch_option, shape, amaxvalue, scale):
     """Per-patch visibility rays: ``(dxdy [P, cap, 2] int32, dz [P, cap], lengths [P], cap)``.
 
     ``lengths[p]`` is the index of the first step with dz > amaxvalue or an
-    offset leaving the raster, plus one (``src/svf.py:53-72``).
+    offset leaving the raster, plus one (``src/svf.py:53-72``).  The heights
+    grow linearly with the index, so only a prefix of the steps (up to two
+    past amaxvalue / slope) can hold that first step: each patch evaluates
+    ``_steps`` on that prefix alone, with the same float64 operations.
     """
+    rows, cols = shape
+    azimuth, altitude, _ = svf_patch_directions(patch_option)
+    P = azimuth.size
+    capacity = max(rows, cols) + 1
+    index_all = np.arange(capacity, dtype=np.float64)
+    lengths = np.zeros(P, dtype=np.int32)
+    if amaxvalue < 0:
+        return np.zeros((P, 1, 2), dtype=np.int32), np.zeros((P, 1)), lengths, 1
+    tables = []
+    for p in range(P):
+        az, el = azimuth[p] * (np.pi / 180.), altitude[p] * (np.pi / 180.)
+        tz = np.tan(el) / scale
+        s_, c_ = abs(np.sin(az)), abs(np.cos(az))
+        slope = (1 / s_ if _ymajor(az) else 1 / c_) * tz
+        m = capacity if not slope > 0 else int(min(capacity, np.ceil(amaxvalue / slope) + 2))
+        index = index_all[:max(m, 1)]
+        dx, dy, ds = _steps(az, index)
+        z = (ds * index) * tz
+        bad = np.flatnonzero((z > amaxvalue) | (np.abs(dx) >= rows) | (np.abs(dy) >= cols))
+        if len(bad):
+            n = int(bad[0]) + 1
+        elif m >= capacity:
+            n = capacity
+        else:  # cannot happen (z exceeds amaxvalue within the prefix); the full table
+            dx, dy, ds = _steps(az, index_all)
+            z = (ds * index_all) * tz
+            bad = np.flatnonzero((z > amaxvalue) | (np.abs(dx) >= rows) | (np.abs(dy) >= cols))
+            n = int(bad[0]) + 1 if len(bad) else capacity
+        lengths[p] = n
+        tables.append((dx[:n], dy[:n], z[:n]))
+    cap = max(1, int(lengths.max()))
+    dxdy = np.zeros((P, cap, 2), dtype=np.int32)
+    dz = np.zeros((P, cap), dtype=np.float64)
+    for p, (dx, dy, z) in enumerate(tables):
+        n = len(z)
+        dxdy[p, :n, 0], dxdy[p, :n, 1] = dx, dy
+        dz[p, :n] = z
+    return dxdy, dz, lengths, cap
+
+
+def _svf_rays_per_patch(patch_option, shape, amaxvalue, scale):
+    """The per-patch loop form of ``svf_rays`` (kept for the equality test)."""
     rows, cols = shape
     azimuth, altitude, _ = svf_patch_directions(patch_option)
     P = azimuth.size

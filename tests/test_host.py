@@ -135,3 +135,17 @@ def test_pipelined_sweep_ranges_cover_the_day():
                                                              (16, 24)]
     with pytest.raises(ValueError):
         ChosenDay._ranges(24, (2, 0))
+
+
+@pytest.mark.parametrize("shape,amax,scale", [((2000, 2000), 40.0, 1.0), ((150, 134), 25.3, 1.0),
+                                               ((64, 200), 12.0, 0.5), ((37, 41), 60.0, 2.0),
+                                               ((500, 480), 0.0, 1.0), ((30, 20), -1.0, 1.0)])
+def test_svf_rays_prefix_equals_full_tables(shape, amax, scale):
+    """The SVF ray tables evaluated on each patch's prefix of steps equal the
+    tables evaluated on every step (offsets, heights, lengths, capacity)."""
+    from solweig_cuda_b200 import rays
+    for po in (1, 2, 3):
+        a = rays.svf_rays(po, shape, amax, scale)
+        b = rays._svf_rays_per_patch(po, shape, amax, scale)
+        assert a[3] == b[3]
+        assert np.array_equal(a[2], b[2]) and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
