@@ -30,8 +30,8 @@ struct SvfRayParams {
 // cols]; the walk then stops on the ceilings and, with geo32, needs no
 // bounds checks.
 // WALK: 0 float64 rasters, 1 packed geometry, 2 packed geometry without
-// bounds checks (`exits` given), 3 as 2 with the word's step records (`rec`,
-// kmax per patch, ray_records_block) instead of the offset and dz tables.
+// bounds checks (`exits` given; used when the step records do not fit, else
+// svf_visibility_warp_kernel).
 // 32 registers (8 blocks per SM): the walks are latency-bound and full
 // occupancy outweighs the few spills (SVF 5.7 ms faster at 2000^2 than at
 // 40 registers).
@@ -40,8 +40,7 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
     const double* __restrict__ dsm, const double* __restrict__ top, const double* __restrict__ bot,
     const float4* __restrict__ geo32, const uint8_t* __restrict__ flags, SvfRayParams prm,
     const int2* __restrict__ ray, const double* __restrict__ dz, const int32_t* __restrict__ lengths,
-    uint32_t* __restrict__ masks, int word0, const float2* __restrict__ ceiling, const int* __restrict__ exits,
-    const longlong2* __restrict__ rec = nullptr, int kmax = 0) {
+    uint32_t* __restrict__ masks, int word0, const float2* __restrict__ ceiling, const int* __restrict__ exits) {
     __shared__ uint8_t state[kSvfPatchGroup][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long pixels = (long long)prm.rows * prm.cols;
@@ -64,12 +63,11 @@ __global__ void __launch_bounds__(32 * kSvfWarps, 8) svf_visibility_kernel(
             const int K = lengths[patch];
             const float2* ceil_j = ceiling ? ceiling + (long long)j * pixels : nullptr;
             ShadowResult s;
-            if (WALK >= 2) {
+            if (WALK == 2) {
                 const int* e = exits + (long long)j * (prm.rows + prm.cols);
                 const int kend = min(K, min(__ldg(&e[r]), __ldg(&e[prm.rows + c])));
-                s = shadow_walk_packed<WALK == 3>(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base,
-                                                  WALK == 3 ? rec + (long long)j * kmax : nullptr, K, kend,
-                                                  prm.hmax, ceil_j);
+                s = shadow_walk_packed<false>(geo32, prm.cols, p, a, top_p, bush, 0.0, ray + base, dz + base,
+                                              nullptr, K, kend, prm.hmax, ceil_j);
             } else if (WALK == 1) {
                 s = shadow_walk_geo(GeoF32x4{geo32}, prm.rows, prm.cols, r, c, a, top_p, bush, 0.0, ray + base,
                                     dz + base, K, prm.hmax, true, ceil_j);
