@@ -655,17 +655,26 @@ def main():
                              "reported with it) vs the plain per-hour form over the same days (its host "
                              "plan interleaved); L2 flushed before each"}
 
-    # End to end through the public API with host buffers.
+    # End to end through the public API with host buffers: the input rasters
+    # sit in page-locked host memory (as a caller streaming tiles keeps them),
+    # the results come back into the API's page-locked buffers.
     from solweig_cuda_b200 import api
+
+    def _pinned_host(x):
+        t = torch.empty(x.shape, dtype=torch.from_numpy(np.ascontiguousarray(x)).dtype, pin_memory=True)
+        t.copy_(torch.from_numpy(np.ascontiguousarray(x)))
+        return t
+
+    host_in = {k: _pinned_host(getattr(sc, k)) for k in ("dsm", "trees", "dem", "landcover")}
     e2e_times, h2d, d2h = [], 0, 0
     for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = api.simulate_day(sc.dsm, sc.trees, sc.dem, met, latitude=53.0, longitude=0.0,
-                               landcover=sc.landcover, pixel_size=1.0, device=dev,
-                               form=a.form)
+        res = api.simulate_day(host_in["dsm"].numpy(), host_in["trees"].numpy(), host_in["dem"].numpy(), met,
+                               latitude=53.0, longitude=0.0, landcover=host_in["landcover"].numpy(),
+                               pixel_size=1.0, device=dev, form=a.form)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if i > 0:
@@ -723,7 +732,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_s,
                     "seconds_each_step": [round(t, 4) for t in e2e_times],
-                    "includes": "H2D rasters, walls, 153-patch SVF, 24 h, D2H Tmrt+UTCI",
+                    "includes": "H2D rasters (page-locked), walls, 153-patch SVF, 24 h, D2H Tmrt+UTCI",
                     "run_timeseries_no_write": series_e2e},
             "gpu_launches": launches_per_day * a.steps,
             "clocks": clocks.summary(),
