@@ -29,8 +29,15 @@ __global__ void __launch_bounds__(256) wall_heights_kernel(const double* __restr
     walls[p] = h;
 }
 
-// One thread per pixel; non-wall pixels write 0.  Template offset lists are
-// small (<= 9 entries per angle for 1 m pixels) and read through L1.
+// A block covers 256 pixels of one row, one lane per pixel; non-wall pixels
+// write 0.  Wall pixels are few (a row segment of 32 holds a couple), so the
+// warp takes its wall pixels one after another and spreads the 180 template
+// angles over its lanes (angle = lane + 32 i); the best angle is the first
+// one with the highest score (scores compared strictly, as the per-pixel loop
+// does), found by a warp maximum of the scores and a minimum of the angles
+// that reach it.  The side sums of the chosen angle are added by the pixel's
+// own lane in the template's order.  Template offset lists are small (<= 9
+// entries per angle for 1 m pixels) and read through L1.
 __global__ void __launch_bounds__(256) wall_aspect_kernel(
     const double* __restrict__ dsm, const double* __restrict__ walls, double* __restrict__ aspect,
     int rows, int cols, int radius, const int32_t* __restrict__ line_off,
@@ -39,16 +46,20 @@ __global__ void __launch_bounds__(256) wall_aspect_kernel(
     const int32_t* __restrict__ s2_start) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
-    if (c >= cols) return;
-    const long long p = (long long)r * cols + c;
+    const int lane = threadIdx.x & 31;
+    const bool in = c < cols;
+    const long long p = (long long)r * cols + (in ? c : 0);
+    const bool cand = in && walls[p] > 0.0 && r >= radius && r < rows - radius - 2 && c >= radius &&
+                      c < cols - radius - 2;
     double out = 0.0;
-    if (walls[p] > 0.0 && r >= radius && r < rows - radius - 2 && c >= radius &&
-        c < cols - radius - 2) {
+    for (uint32_t m = __ballot_sync(0xffffffffu, cand); m; m &= m - 1) {
+        const int src = __ffs(m) - 1;
+        const int pc = __shfl_sync(0xffffffffu, c, src);
         int best = 0, best_angle = -1;
-        for (int angle = 0; angle < 180; ++angle) {
+        for (int angle = lane; angle < 180; angle += 32) {
             int score = 0;
             for (int j = line_start[angle]; j < line_start[angle + 1]; ++j) {
-                const int rr = r + line_off[2 * j], cc = c + line_off[2 * j + 1];
+                const int rr = r + line_off[2 * j], cc = pc + line_off[2 * j + 1];
                 score += walls[(long long)rr * cols + cc] > 0.0 ? 1 : 0;
             }
             if (score > best) {
@@ -56,19 +67,21 @@ __global__ void __launch_bounds__(256) wall_aspect_kernel(
                 best_angle = angle;
             }
         }
-        if (best_angle >= 0) {
-            double first = 0.0, second = 0.0;
-            for (int j = s1_start[best_angle]; j < s1_start[best_angle + 1]; ++j)
-                first += dsm[(long long)(r + s1_off[2 * j]) * cols + (c + s1_off[2 * j + 1])];
-            for (int j = s2_start[best_angle]; j < s2_start[best_angle + 1]; ++j)
-                second += dsm[(long long)(r + s2_off[2 * j]) * cols + (c + s2_off[2 * j + 1])];
-            double dir = 270.0 - best_angle;
-            if (first > second) dir -= 180.0;
+        const int top = __reduce_max_sync(0xffffffffu, best);
+        const int first = __reduce_min_sync(0xffffffffu, (best == top && best_angle >= 0) ? best_angle : 1 << 30);
+        if (lane == src && top > 0) {
+            double s1 = 0.0, s2 = 0.0;
+            for (int j = s1_start[first]; j < s1_start[first + 1]; ++j)
+                s1 += dsm[(long long)(r + s1_off[2 * j]) * cols + (pc + s1_off[2 * j + 1])];
+            for (int j = s2_start[first]; j < s2_start[first + 1]; ++j)
+                s2 += dsm[(long long)(r + s2_off[2 * j]) * cols + (pc + s2_off[2 * j + 1])];
+            double dir = 270.0 - first;
+            if (s1 > s2) dir -= 180.0;
             if (dir < 0.0) dir += 360.0;
             out = dir;
         }
     }
-    aspect[p] = out;
+    if (in) aspect[p] = out;
 }
 
 }  // namespace solweig
