@@ -89,6 +89,11 @@ typedef struct SolweigScene {
        value of the three rasters is exactly representable in float32 (the
        hourly shadow sweep then loads one 16-byte sample per step); NULL otherwise */
     const void* geo32;
+    /* optional statics of the batched day's hour-vectorized GVF (1 m walk, no
+       water), from solweig_gvf_statics: walk-length codes [4][pixels] and the
+       albedo-without-shadow GVF [pixels]; NULL: the day walks them itself */
+    const uint32_t* gvf_hits;
+    const float* gvf_nosh;
 } SolweigScene;
 
 /* Per-patch constants of the sky-vault layout (host arrays, copied per call). */
@@ -339,6 +344,16 @@ int solweig_day_batched_timed(const SolweigScene* scene, const SolweigSkyLayout*
                               const int32_t* gvf_dxdy, int first_steps, int second_steps,
                               void* work, int64_t work_bytes, const SolweigDayConfig* config,
                               void* stream, float* stage_ms);
+/* The scene statics of the batched day's hour-vectorized GVF (no
+ * counterpart in the reference): for the 1 m walk (first_steps 1,
+ * second_steps 22) of a scene without water, the walk length of every GVF
+ * direction (the first building step; device uint32 [4][pixels], 5
+ * directions of 6 bits per word) and the albedo-without-shadow GVF (device
+ * float32 [pixels]), which depend only on the ground bits and the albedo.
+ * Set scene->gvf_hits / gvf_nosh to them and every later day skips that
+ * walk; the results are identical. */
+int solweig_gvf_statics(const SolweigScene* scene, const int32_t* gvf_dxdy, int first_steps, int second_steps,
+                        uint32_t* hits, float* nosh, void* stream);
 /* Byte offsets inside the batched-day work buffer: quads [H][px] float4,
  * first-direction Lup [H][px], GVF [H][3][px] (Lup, albedo, shadow),
  * albedo-without-shadow GVF [px], patch sums (room for [2][2H][px]; the day

@@ -35,6 +35,7 @@ class SolweigScene(ctypes.Structure):
         ("veg_sums", _vp), ("sky_band_counts", _vp), ("gvf_face", _vp), ("svf_dir", _vp),
         ("patches", ctypes.c_int32), ("nbands", ctypes.c_int32), ("landcover", ctypes.c_int32),
         ("has_water", ctypes.c_int32), ("hmax", ctypes.c_double), ("geo32", _vp),
+        ("gvf_hits", _vp), ("gvf_nosh", _vp),
     ]
 
 
@@ -120,6 +121,7 @@ EXPORTED_SYMBOLS = (
     "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex", "solweig_day_batched_part",
     "solweig_day_batched_layout", "solweig_day_grad_work_bytes", "solweig_day_grad_forward",
     "solweig_day_grad_backward", "solweig_svf_ex", "solweig_svf_ex2", "solweig_svf_work_bytes",
+    "solweig_gvf_statics",
 )
 
 _lock = threading.Lock()
@@ -156,6 +158,7 @@ def _declare(lib):
         "solweig_day_batched_ex": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P]),
         "solweig_day_batched_part": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, i32, i32, i32, P]),
         "solweig_day_batched_layout": (i32, [i32, i32, i32, i32, P]),
+        "solweig_gvf_statics": (i32, [P, P, i32, i32, P, P, P]),
         "solweig_day_grad_work_bytes": (i64, [i32, i32, i32]),
         "solweig_day_grad_forward": (i32, [P, P, P, i32, P, i32, i32, P, i32, P, P, i64, P]),
         "solweig_day_grad_backward": (i32, [P, P, P, i32, P, i32, i32, P, i32, P, P, P, P, P, P, P, i64, P]),

@@ -65,6 +65,27 @@ extern "C" int solweig_day_batched_layout(int rows, int cols, int nhours, int ha
     return SOLWEIG_OK;
 }
 
+extern "C" int solweig_gvf_statics(const SolweigScene* scene, const int32_t* gvf_dxdy, int first_steps,
+                                   int second_steps, uint32_t* hits, float* nosh, void* stream) {
+    SOLWEIG_CHECK_ARG(scene && gvf_dxdy && hits && nosh, "solweig_gvf_statics: null argument");
+    SOLWEIG_CHECK_ARG(first_steps == 1 && second_steps == 22,
+                      "solweig_gvf_statics: only the 1 m walk (first 1, second 22), not %d/%d", first_steps,
+                      second_steps);
+    SOLWEIG_CHECK_ARG(!scene->has_water, "solweig_gvf_statics: scenes with water walk per hour");
+    SOLWEIG_CHECK_ARG(scene->rows > 0 && scene->cols > 0 && scene->flags && scene->alb,
+                      "solweig_gvf_statics: bad scene");
+    const SolweigScene& S = *scene;
+    GvfTable<22> tab;
+    fill_day_table(tab, gvf_dxdy, 22, kHvPitch);
+    cudaStream_t st = as_stream(stream);
+    const size_t smem = gvf_statics_smem_bytes();
+    set_smem_attr((const void*)gvf_statics_kernel, smem);
+    dim3 grid(blocks_for(S.cols, kHvTile), blocks_for(S.rows, kHvTile));
+    gvf_statics_kernel<<<grid, dim3(kHvTile, kHvTile), smem, st>>>(S, tab, hits, nosh);
+    SOLWEIG_CHECK_LAUNCH("gvf_statics_kernel");
+    return SOLWEIG_OK;
+}
+
 extern "C" int solweig_patch_sums(const uint32_t* masks, int64_t pixels, int patches, const float* weights,
                                   int ncols, float* out, void* work, int64_t work_bytes, void* stream) {
     SOLWEIG_CHECK_ARG(masks && weights && out && work && pixels > 0, "solweig_patch_sums: null argument");

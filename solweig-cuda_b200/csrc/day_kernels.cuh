@@ -389,63 +389,22 @@ constexpr int kHvBitsBytes = (kHvN + 15) & ~15;
 
 size_t hv_smem_bytes() { return (size_t)kHvN * 2 * sizeof(float4) + kHvBitsBytes + 64 * sizeof(int); }
 
-__global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
-                                                                  int nhours, GvfTable<22> tab,
-                                                                  const float4* __restrict__ quads,
-                                                                  float* __restrict__ gvf, float* __restrict__ nosh) {
+// The hour-independent part of the hour-vectorized GVF for the pixel at tile
+// offset `own` (tile staged with its ground bits and albedo): the walk-length
+// code of every direction (5 per word: lim, frozen-tail bit) and the
+// albedo-without-shadow GVF sum (before / 18).  Shared by day_gvf_hv_kernel
+// and gvf_statics_kernel.
+__device__ __forceinline__ float hv_static_walks(const uint8_t* bits, const float* albs, int own, bool own_ground,
+                                                 bool interior, int r, int c, int rows, int cols,
+                                                 const GvfTable<22>& tab, uint32_t (&hits)[4]) {
     constexpr int FIRST = 1, SECOND = 22;
-    const int tr = blockIdx.y, tc = blockIdx.x;
-    const bool interior = hv_tile_interior(S.rows, S.cols, tr, tc);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float4* LA = reinterpret_cast<float4*>(smem_raw);  // Lup, albsh of pass hours 0, 1
-    float4* LB = LA + kHvN;                            // pass hours 2, 3
-    uint8_t* bits = reinterpret_cast<uint8_t*>(LB + kHvN);    // ground bit, then sunlit-wall bits
-    float* albs = reinterpret_cast<float*>(LB);                // albedo (walk-length pass only)
-    int* dayh = reinterpret_cast<int*>(bits + kHvBitsBytes);   // daytime hour indices
-    __shared__ int nday;
-    const int tid = threadIdx.y * kHvTile + threadIdx.x;
-    const long long n = (long long)S.rows * S.cols;
-    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
-    if (tid == 0) {
-        int k = 0;
-        for (int h = 0; h < nhours && k < 64; ++h)
-            if (hours[h].daytime) dayh[k++] = h;
-        nday = k;
-    }
-    __syncthreads();
-    const int nd = nday;
-    if (nd == 0) return;
-    {
-        const float4* q0 = quads + (long long)dayh[0] * n;
-        for (int i = tid; i < kHvN; i += kHvThreads) {
-            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
-            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
-            const float4 q = in ? q0[(long long)rr * S.cols + cc] : make_float4(0.f, 0.f, 0.f, 0.f);
-            bits[i] = (uint8_t)(__float_as_int(q.w) & kQuadGround);
-            albs[i] = q.z;
-        }
-    }
-    __syncthreads();
-    // each warp walks an 8 x 4 (columns x rows) piece of the tile: walk lengths
-    // of nearby pixels are alike in both directions (24% fewer warp steps than
-    // a row of 32 on the synthetic city), and a warp's shared loads still take
-    // 4 wavefronts (rows of the piece 296 words, 8 banks, apart)
-    const int lw = tid >> 5, ll = tid & 31;
-    const int tx = (lw & 3) * 8 + (ll & 7), ty = (lw >> 2) * 4 + (ll >> 3);
-    const int r = tr * kHvTile + ty, c = tc * kHvTile + tx;
-    const bool valid = r < S.rows && c < S.cols;  // partial tiles at the far edges
-    const long long p = valid ? (long long)r * S.cols + c : 0;
-    const int own = (ty + kHvHalo) * kHvPitch + tx + kHvHalo;
-    const bool own_ground = valid && (bits[own] & 1u) != 0;
-    const float ob = own_ground ? 1.f : 0.f;
-    const uint32_t face = valid ? S.gvf_face[p] : 0u;
     constexpr float albedo_b = 0.2f;
     constexpr float inv_first = 1.f / FIRST, inv_first1 = 1.f / (FIRST + 1);
-    constexpr float inv_second = 1.f / SECOND, inv_second1 = 1.f / (SECOND + 1);
-    // walk lengths (5 directions x 6 bits per word: lim, frozen-tail bit) and
-    // the static plane
-    uint32_t hits[4] = {0u, 0u, 0u, 0u};
+    constexpr float inv_second = 1.f / SECOND;
+    const float ob = own_ground ? 1.f : 0.f;
     float nsh = 0.f;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) hits[w] = 0u;
     for (int j = 0; j < SOLWEIG_GVF_DIRECTIONS; ++j) {
         int hit = 0, lim = 0;
         float s_alb = 0.f, n_alb = 0.f;
@@ -454,7 +413,7 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
             for (int m = 0; m < SECOND; ++m) {
                 if (!interior) {
                     const int2 o = tab.offs[j * SECOND + m];
-                    if (!in_raster(r + o.x, c + o.y, S.rows, S.cols)) {
+                    if (!in_raster(r + o.x, c + o.y, rows, cols)) {
                         if (m == 0) {
                             hit = lim = 0;
                         } else {  // frozen tail: step m and the rest repeat step m - 1
@@ -484,7 +443,77 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
     }
     nsh *= ob;
     nsh += 18.f * (albs[own] * (1.f - ob));
-    if (valid) nosh[p] = nsh / 18.f;
+    return nsh;
+}
+
+__global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene S, const SolweigHour* __restrict__ hours,
+                                                                  int nhours, GvfTable<22> tab,
+                                                                  const float4* __restrict__ quads,
+                                                                  float* __restrict__ gvf, float* __restrict__ nosh) {
+    constexpr int FIRST = 1, SECOND = 22;
+    const int tr = blockIdx.y, tc = blockIdx.x;
+    const bool interior = hv_tile_interior(S.rows, S.cols, tr, tc);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* LA = reinterpret_cast<float4*>(smem_raw);  // Lup, albsh of pass hours 0, 1
+    float4* LB = LA + kHvN;                            // pass hours 2, 3
+    uint8_t* bits = reinterpret_cast<uint8_t*>(LB + kHvN);    // ground bit, then sunlit-wall bits
+    float* albs = reinterpret_cast<float*>(LB);                // albedo (walk-length pass only)
+    int* dayh = reinterpret_cast<int*>(bits + kHvBitsBytes);   // daytime hour indices
+    __shared__ int nday;
+    const int tid = threadIdx.y * kHvTile + threadIdx.x;
+    const long long n = (long long)S.rows * S.cols;
+    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
+    if (tid == 0) {
+        int k = 0;
+        for (int h = 0; h < nhours && k < 64; ++h)
+            if (hours[h].daytime) dayh[k++] = h;
+        nday = k;
+    }
+    __syncthreads();
+    const int nd = nday;
+    if (nd == 0) return;
+    const bool statics = S.gvf_hits != nullptr && S.gvf_nosh != nullptr;
+    if (!statics) {
+        const float4* q0 = quads + (long long)dayh[0] * n;
+        for (int i = tid; i < kHvN; i += kHvThreads) {
+            const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
+            const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
+            const float4 q = in ? q0[(long long)rr * S.cols + cc] : make_float4(0.f, 0.f, 0.f, 0.f);
+            bits[i] = (uint8_t)(__float_as_int(q.w) & kQuadGround);
+            albs[i] = q.z;
+        }
+        __syncthreads();
+    }
+    // each warp walks an 8 x 4 (columns x rows) piece of the tile: walk lengths
+    // of nearby pixels are alike in both directions (24% fewer warp steps than
+    // a row of 32 on the synthetic city), and a warp's shared loads still take
+    // 4 wavefronts (rows of the piece 296 words, 8 banks, apart)
+    const int lw = tid >> 5, ll = tid & 31;
+    const int tx = (lw & 3) * 8 + (ll & 7), ty = (lw >> 2) * 4 + (ll >> 3);
+    const int r = tr * kHvTile + ty, c = tc * kHvTile + tx;
+    const bool valid = r < S.rows && c < S.cols;  // partial tiles at the far edges
+    const long long p = valid ? (long long)r * S.cols + c : 0;
+    const int own = (ty + kHvHalo) * kHvPitch + tx + kHvHalo;
+    // the ground bit of the sweep's quads is the scene's (flags bit 0)
+    const bool own_ground = valid && (statics ? (S.flags[p] & 1) != 0 : (bits[own] & 1u) != 0);
+    const float ob = own_ground ? 1.f : 0.f;
+    const uint32_t face = valid ? S.gvf_face[p] : 0u;
+    constexpr float albedo_b = 0.2f;
+    constexpr float inv_first = 1.f / FIRST, inv_first1 = 1.f / (FIRST + 1);
+    constexpr float inv_second = 1.f / SECOND, inv_second1 = 1.f / (SECOND + 1);
+    // walk lengths and the static plane: prepared with the scene
+    // (gvf_statics_kernel) or walked here from the first daytime hour's quads
+    uint32_t hits[4] = {0u, 0u, 0u, 0u};
+    if (statics) {
+        if (valid) {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) hits[w] = S.gvf_hits[(long long)w * n + p];
+            nosh[p] = S.gvf_nosh[p];
+        }
+    } else {
+        const float nsh = hv_static_walks(bits, albs, own, own_ground, interior, r, c, S.rows, S.cols, tab, hits);
+        if (valid) nosh[p] = nsh / 18.f;
+    }
     const double ambient_e = valid ? kSBC * (double)S.emis[p] : 0.0;
 
     for (int g0 = 0; g0 < nd; g0 += kHvCh) {
@@ -612,6 +641,45 @@ __global__ void __launch_bounds__(kHvThreads, 1) day_gvf_hv_kernel(SolweigScene 
             }
         }
     }
+}
+
+// Scene statics of the hour-vectorized GVF (1 m walk, no water): per pixel
+// the walk-length codes [4][px] and the albedo-without-shadow GVF [px], from
+// the scene's ground bits and albedo -- what day_gvf_hv_kernel would walk
+// from the first daytime hour's quads each day.  32 x 32 tiles, 1024 threads.
+size_t gvf_statics_smem_bytes() { return (size_t)kHvBitsBytes + (size_t)kHvN * sizeof(float); }
+
+__global__ void __launch_bounds__(kHvThreads, 1) gvf_statics_kernel(SolweigScene S, GvfTable<22> tab,
+                                                                   uint32_t* __restrict__ hits_out,
+                                                                   float* __restrict__ nosh_out) {
+    const int tr = blockIdx.y, tc = blockIdx.x;
+    const bool interior = hv_tile_interior(S.rows, S.cols, tr, tc);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* albs = reinterpret_cast<float*>(smem_raw);
+    uint8_t* bits = reinterpret_cast<uint8_t*>(albs + kHvN);
+    const int tid = threadIdx.y * kHvTile + threadIdx.x;
+    const long long n = (long long)S.rows * S.cols;
+    const int row0 = tr * kHvTile - kHvHalo, col0 = tc * kHvTile - kHvHalo;
+    for (int i = tid; i < kHvN; i += kHvThreads) {
+        const int rr = row0 + i / kHvPitch, cc = col0 + i % kHvPitch;
+        const bool in = interior || in_raster(rr, cc, S.rows, S.cols);
+        const long long q = in ? (long long)rr * S.cols + cc : 0;
+        bits[i] = in ? (uint8_t)(S.flags[q] & 1) : (uint8_t)0;
+        albs[i] = in ? S.alb[q] : 0.f;
+    }
+    __syncthreads();
+    const int lw = tid >> 5, ll = tid & 31;
+    const int tx = (lw & 3) * 8 + (ll & 7), ty = (lw >> 2) * 4 + (ll >> 3);
+    const int r = tr * kHvTile + ty, c = tc * kHvTile + tx;
+    if (r >= S.rows || c >= S.cols) return;
+    const long long p = (long long)r * S.cols + c;
+    const int own = (ty + kHvHalo) * kHvPitch + tx + kHvHalo;
+    const bool own_ground = (bits[own] & 1u) != 0;
+    uint32_t hits[4];
+    const float nsh = hv_static_walks(bits, albs, own, own_ground, interior, r, c, S.rows, S.cols, tab, hits);
+#pragma unroll
+    for (int w = 0; w < 4; ++w) hits_out[(long long)w * n + p] = hits[w];
+    nosh_out[p] = nsh / 18.f;
 }
 
 // ------------------------------------------------------------- kernels 3, 4, 5

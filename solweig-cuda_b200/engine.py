@@ -416,6 +416,7 @@ class Scene:
             device_ptr(self.tan_asvf), device_ptr(self.gvf_face), st), "solweig_scene_finalize")
         self.planes = planes if keep_planes else None
         self.struct = self._make_struct()
+        self._gvf_statics(st)
 
     @classmethod
     def from_inputs(cls, inputs, device="cuda", stream=None):
@@ -509,7 +510,25 @@ class Scene:
         self.gvf_dxdy = _upload(self.gvf_dxdy_host, np.int32, dev)
         self.gvf_host_ptr = self.gvf_dxdy_host.ctypes.data_as(ctypes.c_void_p)
         self.struct = self._make_struct()
+        self._gvf_statics(st)
         return self
+
+    def _gvf_statics(self, st):
+        """The hour-independent part of the batched day's GVF (walk length of
+        every direction, albedo-without-shadow plane) for the 1 m walk of a
+        scene without water, prepared once here (``solweig_gvf_statics``) so
+        the days skip that walk; other scenes leave the pointers NULL."""
+        self.gvf_hits = self.gvf_nosh = None
+        if self.first_steps != 1 or self.second_steps != 22 or self.has_water:
+            return
+        dev = self.dsm.device
+        self.gvf_hits = torch.empty((4,) + self.shape, dtype=torch.int32, device=dev)
+        self.gvf_nosh = torch.empty(self.shape, dtype=torch.float32, device=dev)
+        _lib.check(_lib.lib().solweig_gvf_statics(
+            ctypes.byref(self.struct), self.gvf_host_ptr, self.first_steps, self.second_steps,
+            device_ptr(self.gvf_hits), device_ptr(self.gvf_nosh), st), "solweig_gvf_statics")
+        self.struct.gvf_hits = self.gvf_hits.data_ptr()
+        self.struct.gvf_nosh = self.gvf_nosh.data_ptr()
 
     def _make_struct(self):
         s = _lib.SolweigScene()

@@ -371,3 +371,39 @@ def test_window_sweep_is_bit_identical(cuda, shape, doy, lat, shift):
                     assert torch.equal(q1[h], q0[h]), (window, no_ceiling, h)
             for k in o0:
                 assert torch.equal(o1[k].view(torch.int32), o0[k].view(torch.int32)), (window, no_ceiling, k)
+
+
+def test_gvf_statics_prepared_with_the_scene_are_identical(cuda):
+    """Days that read the GVF walk lengths and albedo-without-shadow plane
+    prepared with the scene (solweig_gvf_statics) equal, bit for bit, days
+    that walk them from the first daytime hour's quads (border and interior
+    tiles)."""
+    import torch
+    from solweig_cuda_b200 import batched, engine, synthetic
+    s = synthetic.make_scene(150, 134, seed=17)
+    scene = engine.Scene(s.dsm, s.trees, s.dem, 1.0, landcover=s.landcover)
+    assert scene.gvf_hits is not None and scene.struct.gvf_hits
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, seed=2)
+    outs = ("tmrt", "utci", "kup", "lup")
+    res = []
+    for with_statics in (True, False):
+        if not with_statics:
+            scene.struct.gvf_hits = None
+            scene.struct.gvf_nosh = None
+        day = batched.ChosenDay(scene, 53.0, 0.0, 3.0, 0.0, outputs=outs)
+        out = {k: v.clone() for k, v in day.run_day(met).items()}
+        torch.cuda.synchronize()
+        o = day.work_offsets()
+        n = scene.pixels
+        gvf = day.work[o["gvf"]:o["gvf"] + 12 * 24 * n].view(torch.float32).view(24, 3, n).clone()
+        nosh = day.work[o["nosh"]:o["nosh"] + 4 * n].view(torch.float32).clone()
+        res.append((out, gvf, nosh, [h.daytime for h, _, _ in day.plan(met)]))
+    scene.struct.gvf_hits = scene.gvf_hits.data_ptr()
+    scene.struct.gvf_nosh = scene.gvf_nosh.data_ptr()
+    (a, ga, na, flags), (b, gb, nb, _) = res
+    assert torch.equal(na, nb)
+    for h, d in enumerate(flags):  # the GVF planes of daytime hours (night ones are not written)
+        if d:
+            assert torch.equal(ga[h], gb[h]), h
+    for k in outs:
+        torch.testing.assert_close(a[k], b[k], rtol=0, atol=0, equal_nan=True)
