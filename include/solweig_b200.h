@@ -20,6 +20,8 @@
  * Reference interfaces replaced (paths relative to the reference root):
  *   solweig_wall_heights      src/walls.py:59-69, src/kernels/geometry.cu:15-34
  *   solweig_wall_aspect       src/walls.py:83-121, src/kernels/geometry.cu:36-63
+ *   solweig_wall_segments_burn, solweig_geometry_walls
+ *                             src/walls.py:270-332 (calculate_geometry_walls)
  *   solweig_shadow            src/model.py:689-708 (cast_shadow),
  *                             src/kernels/geometry.cu:185-253
  *   solweig_svf               src/svf.py:81-114, src/kernels/geometry.cu:77-159
@@ -28,6 +30,8 @@
  *   solweig_gvf               src/model.py:569-622, src/kernels/gvf.cu:79-292
  *   solweig_step(_shadow,_radiation)
  *                             src/model.py:15-256 (Solweig_2022a_calc, device part)
+ *   solweig_step64            the same step under the float64 switch (run.py:27,
+ *                             src/runtime.py:43-49)
  *   solweig_day               src/series.py:445-491 (the hour loop of _run_day)
  *   solweig_day_batched       src/series.py:445-491 (same loop, batched form)
  *   solweig_scene_build/finalize src/series.py:252-349 (_prepare_spatial, per pixel)
@@ -181,6 +185,23 @@ int solweig_wall_aspect(const double* dsm, const double* walls, double* aspect,
                         const int32_t* side2_off, const int32_t* side2_start,
                         void* stream);
 
+/* Walls from building footprints (src/walls.py:270-332, the geometry wall
+ * method).  segments: device float64 [nseg][4] = (u0, v0, u1, v1) in pixel
+ * coordinates (the inverse geotransform of the edge's end points; column u,
+ * row v), 16-byte aligned.  solweig_wall_segments_burn sets owner[pixels] to
+ * the index of the last segment touching each cell (-1: none), where a
+ * segment touches every half-open cell [col, col+1) x [row, row+1) holding one
+ * of its points (rasterio's all_touched burn with later shapes replacing
+ * earlier ones).  solweig_geometry_walls turns owners into float32 planes:
+ * walls = the GHSL height where it is >= minimum (float32 compare; NaN/inf
+ * read as 0; ghsl may be NULL), else the segment's height; aspect = the
+ * segment's aspect mod 360; 0 where no segment touches. */
+int solweig_wall_segments_burn(const double* segments, int64_t nseg, int rows, int cols, int32_t* owner,
+                               void* stream);
+int solweig_geometry_walls(const int32_t* owner, const double* seg_height, const double* seg_aspect,
+                           const float* ghsl, int64_t pixels, double minimum, float* walls, float* aspect,
+                           void* stream);
+
 /* Shadows ---------------------------------------------------------------- */
 /* out: 8 planes [8][pixels] float64 in the reference order
  * (vegsh, sh, vbshvegsh, wallsh, wallsun, wallshve, facesh, facesun);
@@ -277,6 +298,53 @@ int solweig_day(const SolweigScene* scene, const SolweigSkyLayout* layout,
                 const SolweigHour* hours, int nhours, const SolweigState* state,
                 const SolweigOutputs* base, int64_t hour_stride, const int32_t* gvf_dxdy,
                 int first_steps, int second_steps, float* scratch, void* stream);
+
+/* The hourly step with float64 radiation --------------------------------------
+ * The reference's precision switch (run.py:27 --dtype float64; src/runtime.py:
+ * 43-49 recompiles gvf.cu, shortwave.cu, longwave.cu and flux.cu with Real =
+ * double; src/model.py:15-256 then returns float64 planes).  The same hour as
+ * solweig_step with every per-pixel radiation quantity in float64: the shadow
+ * sh - (1 - vegsh)(1 - psi) unrounded, the Lup excess, the 15 ground view
+ * factors, the wave-delay state, the patch sums over every patch in patch
+ * order, Kdown/Kup/Kside, Ldown/Lside, Tmrt.  The shadow sweep and the
+ * visibility masks are the float32 step's (they are exact).  UTCI stays
+ * float32, evaluated from the float32-rounded Tmrt (src/utci.py:8-12).
+ * svfbuveg: device float64 [pixels], svf - (1 - svfveg)(1 - transmissivity)
+ * of the float32-rounded SVF planes; layout and sky: DEVICE structs; hours64:
+ * device array beside hours (same index); scratch: device float64
+ * [SOLWEIG_SCRATCH64_PLANES][pixels]. */
+#define SOLWEIG_SCRATCH64_PLANES 20
+typedef struct SolweigSky64 {
+    double omega[SOLWEIG_MAX_PATCHES];          /* steradian */
+    double cos_alt[SOLWEIG_MAX_PATCHES];
+    double sin_alt[SOLWEIG_MAX_PATCHES];
+    double cardinal[4][SOLWEIG_MAX_PATCHES];    /* E,S,W,N longwave direction cosines (0 = off) */
+    double diffsh_veg;  /* shmat - (1 - vegshmat)(1 - transmissivity) of a vegetation patch,
+                           evaluated in float32 as src/svf.py:117-131 does */
+} SolweigSky64;
+typedef struct SolweigHour64 {
+    double lum[SOLWEIG_MAX_PATCHES];      /* Perez luminance of each patch */
+    double band_lsky[SOLWEIG_MAX_BANDS];  /* emissivity * SBC * Tk^4 / pi per band */
+} SolweigHour64;
+typedef struct SolweigOutputs64 {
+    double* tmrt;
+    float* utci;
+    double* kdown; double* kup; double* ldown; double* lup;
+    double* shadow; double* tg;
+    double* keast; double* ksouth; double* kwest; double* knorth;
+    double* least; double* lsouth; double* lwest; double* lnorth;
+    double* kside_i; double* kside_d; double* kside; double* lside;
+    double* d_rad; double* tg_out;
+} SolweigOutputs64;
+typedef struct SolweigState64 {
+    double* tgmap1; double* tgmap1e; double* tgmap1s; double* tgmap1w; double* tgmap1n;
+    double* tgout1;
+} SolweigState64;
+int solweig_step64(const SolweigScene* scene, const double* svfbuveg, const SolweigSkyLayout* layout,
+                   const SolweigSky64* sky, const SolweigHour* hours, const SolweigHour64* hours64,
+                   int hour, const SolweigState64* state, const SolweigOutputs64* out,
+                   const int32_t* gvf_dxdy /* host [18][second_steps][2] */, int first_steps,
+                   int second_steps, double* scratch, void* stream);
 
 /* Batched day ----------------------------------------------------------------
  * All nhours (<= 64) hours of one day (src/series.py:445-491) in seven
@@ -471,6 +539,8 @@ int solweig_utci_collapse(double ta, double rh, double va, double* coefficients)
 
 /* sizeof(SolweigScene, SolweigSkyLayout, SolweigHour, SolweigOutputs, SolweigState). */
 int solweig_struct_sizes(int64_t* out);
+/* sizeof(SolweigSky64, SolweigHour64, SolweigOutputs64, SolweigState64). */
+int solweig_struct_sizes64(int64_t* out);
 
 #ifdef __cplusplus
 }

@@ -1,6 +1,6 @@
 """Command line of the B200 engine, mirroring the reference's ``run.py``.
 
-    python run.py [--case case.json] [--output DIR] [--dtype float32]
+    python run.py [--case case.json] [--output DIR] [--dtype float32|float64]
                   [--output-core ROW COL ROWS COLS] [--output-chunk-steps N]
                   [--sync-output] [--output-queue-size N] [--no-write] [--progress]
                   [--check] [--form chosen|batched]
@@ -12,8 +12,9 @@ installed).  ``case_type: open_data`` needs network downloads and is not
 supported; ``core_area_m`` / ``buffer_area_m`` tile the rasters with halos and
 every group of tiles runs day by day in one captured graph per day
 (``series.run_tiles``).  Under ``torchrun`` each rank takes a share of the
-days (one tile) or of the tiles (tiled cases).  Only ``--dtype float32`` runs:
-the reference's float64 radiation switch is not provided.
+days (one tile) or of the tiles (tiled cases).  ``--dtype float64`` is the
+reference's radiation precision switch: every hour runs through the float64
+step instead of the batched float32/BF16 form.
 """
 from __future__ import annotations
 
@@ -82,8 +83,8 @@ def main(argv=None):
     parser.add_argument("--case", type=Path, default=Path(ROOT) / "examples" / "case.json",
                         help="JSON case file (default: examples/case.json beside run.py); paths are relative to it")
     parser.add_argument("--output", type=Path)
-    parser.add_argument("--dtype", choices=("float32",), default="float32",
-                        help="radiation precision (float32 only; the float64 switch is not provided)")
+    parser.add_argument("--dtype", choices=("float32", "float64"), default="float32",
+                        help="radiation precision")
     parser.add_argument("--form", choices=("chosen", "batched"), default="chosen",
                         help="chosen: batched day with tensor-core patch sums; batched: per-hour kernels in a graph")
     parser.add_argument("--output-core", type=int, nargs=4, metavar=("ROW", "COL", "ROWS", "COLS"))
@@ -134,7 +135,9 @@ def main(argv=None):
                  "landcover_path", "utc_offset_hours", "site_altitude_m", "output_core",
                  "output_chunk_steps", "async_output", "output_queue_size", "save_tmrt", "save_svf",
                  "save_kup", "save_kdown", "save_lup", "save_ldown", "save_shadow", "dsm_wall_threshold_m",
-                 "output_valid_mask"}
+                 "output_valid_mask", "wall_method", "building_geometry_path", "building_height_path",
+                 "minimum_wall_height_m", "default_building_height_m", "level_height_m",
+                 "minimum_building_height_m", "crs", "geotransform"}
         kwargs = {k: v for k, v in case.items() if k in known}
         run_timeseries(output_path=output, dtype=np.dtype(args.dtype), no_write=args.no_write,
                        progress=args.progress, pixel_size=pixel_size, form=args.form, **kwargs)

@@ -11,7 +11,7 @@ import os
 import threading
 
 __all__ = ["lib", "check", "SolweigScene", "SolweigSkyLayout", "SolweigHour", "SolweigOutputs",
-           "SolweigState", "MAX_PATCHES", "MASK_WORDS", "MAX_BANDS", "GVF_DIRECTIONS",
+           "SolweigState", "SolweigSky64", "SolweigHour64", "SolweigOutputs64", "SolweigState64", "MAX_PATCHES", "MASK_WORDS", "MAX_BANDS", "GVF_DIRECTIONS",
            "GVF_MAX_STEPS", "EXPORTED_SYMBOLS", "library_path"]
 
 MAX_PATCHES = 160
@@ -20,6 +20,7 @@ MAX_BANDS = 8
 GVF_DIRECTIONS = 18
 GVF_MAX_STEPS = 64
 SCRATCH_PLANES = 20  # quad (4) + first-direction Lup (1) + 15 GVF planes
+SCRATCH64_PLANES = 20  # float64 step: 5 per-pixel GVF inputs + 15 GVF planes
 STATIC_SCRATCH_MAX_PIXELS = 512 * 512  # capacity of solweig_step_static_scratch
 
 _c_double_p = ctypes.POINTER(ctypes.c_double)
@@ -90,6 +91,27 @@ class SolweigState(ctypes.Structure):
     _fields_ = [(name, _vp) for name in STATE_FIELDS]
 
 
+class SolweigSky64(ctypes.Structure):
+    """Float64 per-patch constants of the float64 step (device copy per layout)."""
+    _fields_ = [("omega", ctypes.c_double * MAX_PATCHES), ("cos_alt", ctypes.c_double * MAX_PATCHES),
+                ("sin_alt", ctypes.c_double * MAX_PATCHES),
+                ("cardinal", (ctypes.c_double * MAX_PATCHES) * 4), ("diffsh_veg", ctypes.c_double)]
+
+
+class SolweigHour64(ctypes.Structure):
+    """Float64 per-patch weights of one hour (beside its SolweigHour)."""
+    _fields_ = [("lum", ctypes.c_double * MAX_PATCHES), ("band_lsky", ctypes.c_double * MAX_BANDS)]
+
+
+class SolweigOutputs64(ctypes.Structure):
+    """SolweigOutputs of the float64 step: float64 planes, float32 UTCI."""
+    _fields_ = [(name, _vp) for name in OUTPUT_FIELDS]
+
+
+class SolweigState64(ctypes.Structure):
+    _fields_ = [(name, _vp) for name in STATE_FIELDS]
+
+
 class SolweigGradParams(ctypes.Structure):
     """Per-pixel parameters of the day gradient (device float32 pointers)."""
     _fields_ = [("albedo", _vp), ("emissivity", _vp), ("transmissivity", _vp)]
@@ -121,7 +143,8 @@ EXPORTED_SYMBOLS = (
     "solweig_patch_sums", "solweig_day_batched_timed", "solweig_day_batched_ex", "solweig_day_batched_part",
     "solweig_day_batched_layout", "solweig_day_grad_work_bytes", "solweig_day_grad_forward",
     "solweig_day_grad_backward", "solweig_svf_ex", "solweig_svf_ex2", "solweig_svf_work_bytes",
-    "solweig_gvf_statics",
+    "solweig_gvf_statics", "solweig_step64", "solweig_struct_sizes64", "solweig_wall_segments_burn",
+    "solweig_geometry_walls",
 )
 
 _lock = threading.Lock()
@@ -139,6 +162,8 @@ def _declare(lib):
         "solweig_version": (i32, []),
         "solweig_wall_heights": (i32, [P, P, i32, i32, dbl, P]),
         "solweig_wall_aspect": (i32, [P, P, P, i32, i32, i32, P, P, P, P, P, P, P]),
+        "solweig_wall_segments_burn": (i32, [P, i64, i32, i32, P, P]),
+        "solweig_geometry_walls": (i32, [P, P, P, P, i64, dbl, P, P, P]),
         "solweig_shadow": (i32, [P, P, P, i32, dbl, dbl, i32, i32, P, P]),
         "solweig_svf": (i32, [P, P, P, P, i32, i32, i32, i32, P, P, P, dbl, P, P, P, dbl, P, P, P, P,
                               P]),
@@ -152,6 +177,7 @@ def _declare(lib):
         "solweig_gvf": (i32, [P, P, P, P, dbl, dbl, dbl, dbl, dbl, P, i32, i32, P, P, P]),
         "solweig_step": (i32, [P, P, P, i32, P, P, P, i32, i32, P, P]),
         "solweig_step_static_scratch": (i32, [P, P, P, i32, P, P, P, i32, i32, P]),
+        "solweig_step64": (i32, [P, P, P, P, P, P, i32, P, P, P, i32, i32, P, P]),
         "solweig_day_batched": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P]),
         "solweig_day_batched_work_bytes": (i64, [i32, i32, i32, i32]),
         "solweig_day_batched_timed": (i32, [P, P, P, i32, P, P, i64, P, i32, i32, P, i64, P, P, P]),
@@ -171,6 +197,7 @@ def _declare(lib):
                                       P, P, P]),
         "solweig_scene_finalize": (i32, [P, P, P, i64, dbl, P, P, P, P, P, P, P, P, P]),
         "solweig_struct_sizes": (i32, [P]),
+        "solweig_struct_sizes64": (i32, [P]),
         "solweig_utci_scalar": (i32, [dbl, dbl, dbl, P, P, i64, P]),
         "solweig_svf_pack": (i32, [P, P, P, i64, i32, P, P]),
         "solweig_svf_reduce": (i32, [P, P, i64, P, P, P, dbl, P, P, P, P]),
@@ -201,9 +228,13 @@ def lib():
                 handle.solweig_struct_sizes(sizes)
                 mine = [ctypes.sizeof(t) for t in (SolweigScene, SolweigSkyLayout, SolweigHour,
                                                   SolweigOutputs, SolweigState)]
-                if list(sizes) != mine:
-                    raise RuntimeError(f"ABI struct size mismatch: library {list(sizes)} "
-                                       f"vs binding {mine}")
+                sizes64 = (ctypes.c_int64 * 4)()
+                handle.solweig_struct_sizes64(sizes64)
+                mine64 = [ctypes.sizeof(t) for t in (SolweigSky64, SolweigHour64, SolweigOutputs64,
+                                                    SolweigState64)]
+                if list(sizes) != mine or list(sizes64) != mine64:
+                    raise RuntimeError(f"ABI struct size mismatch: library {list(sizes)} {list(sizes64)} "
+                                       f"vs binding {mine} {mine64}")
                 _lib = handle
     return _lib
 

@@ -31,3 +31,13 @@ extern "C" int solweig_struct_sizes(int64_t* out) {
     out[4] = sizeof(SolweigState);
     return SOLWEIG_OK;
 }
+
+// out[0..3] = SolweigSky64, SolweigHour64, SolweigOutputs64, SolweigState64.
+extern "C" int solweig_struct_sizes64(int64_t* out) {
+    if (!out) return SOLWEIG_ERR_INVALID;
+    out[0] = sizeof(SolweigSky64);
+    out[1] = sizeof(SolweigHour64);
+    out[2] = sizeof(SolweigOutputs64);
+    out[3] = sizeof(SolweigState64);
+    return SOLWEIG_OK;
+}

@@ -117,6 +117,31 @@ class SkyLayout:
             self._device[key] = torch.from_numpy(raw.copy()).to(dev)
         return self._device[key]
 
+    def struct64(self):
+        """The float64 per-patch constants of the float64 step (``SolweigSky64``)."""
+        L = self.host
+        s = _lib.SolweigSky64()
+        P = L.count
+        np.ctypeslib.as_array(s.omega)[:P] = L.steradian
+        np.ctypeslib.as_array(s.cos_alt)[:P] = L.cos_alt
+        np.ctypeslib.as_array(s.sin_alt)[:P] = L.sin_alt
+        card = np.ctypeslib.as_array(s.cardinal)
+        for d in range(4):
+            card[d, :P] = L.cardinal[:, d]
+        # diffsh of a vegetation patch (shmat 1, vegshmat 0) in float32, as
+        # compute_diffsh evaluates it (src/svf.py:117-131)
+        one, tv = np.float32(1.0), np.float32(CONSTANTS["transVeg"])
+        s.diffsh_veg = float(one - (one - np.float32(0.0)) * (one - tv))
+        return s
+
+    def device64(self, dev):
+        """``struct64`` in device memory (uploaded once per device)."""
+        key = "f64:" + str(dev)
+        if key not in self._device:
+            raw = np.frombuffer(_lib.struct_bytes(self.struct64()), dtype=np.uint8)
+            self._device[key] = torch.from_numpy(raw.copy()).to(dev)
+        return self._device[key]
+
 
 def _upload(arr, dtype, device):
     return torch.from_numpy(np.ascontiguousarray(arr, dtype=dtype)).to(device, non_blocking=False)
@@ -472,6 +497,7 @@ class Scene:
         self.dsm_max = float(self.dsm.max().item())
         self.hmax = float(max(self.dsm_max, self.vegdem.max().item(), self.vegdem2.max().item()))
         self.svfbuveg = f32(inputs["svfbuveg"])
+        self._svfbuveg64 = f64(inputs["svfbuveg"])
         self.svfalfa = f64(inputs["svfalfa"])
         self.tan_asvf = torch.tan(f64(inputs["asvf"])).contiguous()
         P = self.layout.struct.patches
@@ -560,6 +586,17 @@ class Scene:
         geo = torch.zeros(self.shape + (4,), dtype=torch.float32, device=self.dsm.device)
         geo[..., :3] = packed
         return geo
+
+    def svfbuveg64(self):
+        """svf - (1 - svfveg)(1 - transVeg) in float64 from the float32-rounded
+        SVF planes (``src/series.py:337-341``), for the float64 step."""
+        t = getattr(self, "_svfbuveg64", None)
+        if t is None:
+            svf = self.svf32[self.SVF_ORDER.index("svf")].to(torch.float64)
+            veg = self.svf32[self.SVF_ORDER.index("svfveg")].to(torch.float64)
+            t = (svf - (1.0 - veg) * (1.0 - CONSTANTS["transVeg"])).contiguous()
+            self._svfbuveg64 = t
+        return t
 
     @property
     def walls_host(self):
@@ -853,6 +890,18 @@ class DayRunner:
             sc.first_steps, sc.second_steps, device_ptr(self.scratch), stream_handle(stream)),
             "solweig_step")
 
+    def _alloc_outputs(self, outputs, nrows):
+        return {k: torch.empty((nrows,) + self.scene.shape, dtype=torch.float32, device=self.scene.device)
+                for k in outputs}
+
+    def _put(self, slot, hour, ray, scal):
+        """Stage hour record ``slot`` and copy it to the device."""
+        self.buffers.put(slot, hour, ray)
+        self.buffers.upload(slot, 1, ray.steps if ray is not None else 1)
+
+    def _outputs_struct(self, res, index):
+        return outputs_struct(res, index)
+
     def run_day(self, met, outputs=("tmrt", "utci"), stream=None):
         """Run the rows of one calendar day; returns {name: tensor [H, rows, cols]}."""
         met = np.asarray(met, dtype=np.float64)
@@ -862,8 +911,7 @@ class DayRunner:
         dectime = sol.dectime
         timestepdec = (dectime[1] - dectime[0]) if len(met) > 1 else 1 / 24.
         twater = float(np.mean(met[:, 11])) if self.scene.landcover else None
-        res = {k: torch.empty((len(met),) + self.scene.shape, dtype=torch.float32,
-                              device=self.scene.device) for k in outputs}
+        res = self._alloc_outputs(outputs, len(met))
         self.buffers.wait_free()
         self.reset_state()
         firstdaytime, timeadd, CI = 1, 0.0, 1.0
@@ -877,9 +925,8 @@ class DayRunner:
                 dectime[i], sol.altmax[i], met[i, 11], met[i, 10], met[i, 14], met[i, 21],
                 met[i, 22], met[i, 12], met[i, 9], psi, CI, firstdaytime, timeadd, timestepdec,
                 twater)
-            self.buffers.put(i, h, ray)
-            self.buffers.upload(i, 1, ray.steps if ray is not None else 1)
-            self._launch(i, outputs_struct(res, i), stream)
+            self._put(i, h, ray, scal)
+            self._launch(i, self._outputs_struct(res, i), stream)
             scalars.append(scal)
         self.buffers.mark()
         self.last_scalars = scalars
@@ -945,3 +992,73 @@ class DayRunner:
 SHADOW_BYTES_PER_PIXEL = 77
 GVF_BYTES_PER_PIXEL = 84
 RADIATION_BYTES_PER_PIXEL = 221
+
+
+def hour64_record(scene, hour, scal):
+    """The float64 per-patch weights of one hour (``SolweigHour64``): the Perez
+    luminances (daytime) and the band sky emittances of ``hour_plan``."""
+    h64 = _lib.SolweigHour64()
+    if hour.daytime:
+        np.ctypeslib.as_array(h64.lum)[:scene.layout.host.count] = scal.lv[:, 2]
+    np.ctypeslib.as_array(h64.band_lsky)[:len(scal.band_lsky)] = scal.band_lsky
+    return h64
+
+
+class DayRunner64(DayRunner):
+    """Plain form with float64 radiation, the reference's ``dtype=float64``
+    (``run.py:27``, ``src/runtime.py:43-49``): one ``solweig_step64`` per hour
+    (shadow fields, ground view factors and radiation in float64), float64
+    thermal state and output planes; UTCI stays float32."""
+
+    def __init__(self, scene, latitude, longitude, site_altitude=3.0, utc=0.0, hours=24):
+        self.scene = scene
+        self.latitude, self.longitude, self.site_altitude, self.utc = latitude, longitude, site_altitude, utc
+        dev = scene.device
+        self.state = {k: torch.zeros(scene.shape, dtype=torch.float64, device=dev)
+                      for k in _lib.STATE_FIELDS}
+        self.scratch = torch.empty((_lib.SCRATCH64_PLANES, scene.rows, scene.cols), dtype=torch.float64,
+                                   device=dev)
+        slots = max(24, int(hours))
+        self.buffers = HourBuffers(scene, slots)
+        self.h64size = ctypes.sizeof(_lib.SolweigHour64)
+        self.h64_host = torch.empty(slots * self.h64size, dtype=torch.uint8, pin_memory=True)
+        self.h64_dev = torch.empty(slots * self.h64size, dtype=torch.uint8, device=dev)
+        self.layout_dev = scene.layout.device(dev)
+        self.sky64_dev = scene.layout.device64(dev)
+        self.svfbuveg = scene.svfbuveg64()
+
+    def state_struct(self):
+        s = _lib.SolweigState64()
+        for k in _lib.STATE_FIELDS:
+            setattr(s, k, self.state[k].data_ptr())
+        return s
+
+    def _alloc_outputs(self, outputs, nrows):
+        return {k: torch.empty((nrows,) + self.scene.shape,
+                               dtype=torch.float32 if k == "utci" else torch.float64, device=self.scene.device)
+                for k in outputs}
+
+    def _outputs_struct(self, res, index):
+        out = _lib.SolweigOutputs64()
+        for k, t in res.items():
+            setattr(out, k, (t[index] if index is not None else t).data_ptr())
+        return out
+
+    def _put(self, slot, hour, ray, scal):
+        super()._put(slot, hour, ray, scal)
+        n = self.h64size
+        raw = np.frombuffer(_lib.struct_bytes(hour64_record(self.scene, hour, scal)), dtype=np.uint8)
+        self.h64_host.numpy()[slot * n:(slot + 1) * n] = raw
+        self.h64_dev[slot * n:(slot + 1) * n].copy_(self.h64_host[slot * n:(slot + 1) * n], non_blocking=True)
+
+    def _launch(self, slot, out_struct, stream=None):
+        sc = self.scene
+        _lib.check(_lib.lib().solweig_step64(
+            ctypes.byref(sc.struct), device_ptr(self.svfbuveg), device_ptr(self.layout_dev),
+            device_ptr(self.sky64_dev), self.buffers.ptr(), device_ptr(self.h64_dev), slot,
+            ctypes.byref(self.state_struct()), ctypes.byref(out_struct), sc.gvf_host_ptr,
+            sc.first_steps, sc.second_steps, device_ptr(self.scratch), stream_handle(stream)),
+            "solweig_step64")
+
+    def profile_day(self, met):
+        raise NotImplementedError("profile_day times the float32 kernels; time a DayRunner64 day with events")

@@ -33,7 +33,10 @@ _OPTIONAL = frozenset({"minimum_wall_height_m", "dsm_wall_threshold_m", "default
                        "level_height_m", "minimum_building_height_m", "save_tmrt", "save_svf", "save_kup",
                        "save_kdown", "save_lup", "save_ldown", "save_shadow", "wall_method",
                        "utc_offset_hours", "site_altitude_m", "output_core", "output_chunk_steps",
-                       "async_output", "output_queue_size"})
+                       "async_output", "output_queue_size",
+                       # georeferencing of .npy rasters for wall_method=geometry (a GeoTIFF
+                       # carries them; these keys have no counterpart in the reference)
+                       "crs", "geotransform"})
 _SAVE_FLAGS = ("save_tmrt", "save_svf", "save_kup", "save_kdown", "save_lup", "save_ldown", "save_shadow")
 _POSITIVE_LENGTHS = ("minimum_wall_height_m", "dsm_wall_threshold_m", "default_building_height_m",
                      "level_height_m", "minimum_building_height_m")

@@ -77,13 +77,30 @@ def prepare_model(*, dtype=np.float32, **inputs):
 
 
 class _StepRunner:
-    """Per-scene buffers for single-hour calls."""
+    """Per-scene buffers for single-hour calls (the float32 or float64 step's
+    scratch is allocated on first use)."""
 
     def __init__(self, scene):
+        self.scene = scene
         self.buffers = engine.HourBuffers(scene, 1)
-        self.scratch = torch.empty((_lib.SCRATCH_PLANES,) + scene.shape, dtype=torch.float32,
-                                   device=scene.device)
         self.layout_dev = scene.layout.device(scene.device)
+        self._scratch = {}
+        self.h64_host = self.h64_dev = None
+
+    def scratch(self, dtype):
+        if dtype not in self._scratch:
+            planes = _lib.SCRATCH64_PLANES if dtype == torch.float64 else _lib.SCRATCH_PLANES
+            self._scratch[dtype] = torch.empty((planes,) + self.scene.shape, dtype=dtype, device=self.scene.device)
+        return self._scratch[dtype]
+
+    def put64(self, hour, scal):
+        """Stage and upload the hour's float64 patch weights (after ``buffers.put``)."""
+        raw = np.frombuffer(_lib.struct_bytes(engine.hour64_record(self.scene, hour, scal)), dtype=np.uint8)
+        if self.h64_host is None:
+            self.h64_host = torch.empty(raw.size, dtype=torch.uint8, pin_memory=True)
+            self.h64_dev = torch.empty(raw.size, dtype=torch.uint8, device=self.scene.device)
+        self.h64_host.numpy()[:] = raw
+        self.h64_dev.copy_(self.h64_host, non_blocking=True)
 
 
 _RUNNERS = {}
@@ -129,9 +146,9 @@ def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, s
     Without ``prepared`` the device geometry is built on the first call and
     reused by later calls given the same static array objects (the two most
     recent sets are kept); arrays changed in place between calls need a new
-    ``prepare_model``.  ``dtype`` float64 returns float64 planes computed by
-    the float32 step (the reference's float64 radiation switch is not
-    provided)."""
+    ``prepare_model``.  ``dtype`` float64 runs the float64 step
+    (``solweig_step64``: the reference's float64 radiation switch) and returns
+    float64 planes and state."""
     args = dict(locals())
     _check_switches(args)
     constants = dict(albedo_b=0.2, absK=0.7, absL=0.95, ewall=0.9, Fside=0.22, Fup=0.06, Fcyl=0.28,
@@ -152,23 +169,34 @@ def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, s
         float(dectime), float(altmax), float(Ta), float(RH), float(radG), float(radD), float(radI),
         float(P), 0.0, float(psi), float(CI), int(firstdaytime), float(timeadd), float(timestepdec),
         None if Twater is None else float(Twater))
+    f64 = dt == np.float64
+    tdt = torch.float64 if f64 else torch.float32
     run.buffers.wait_free()
     run.buffers.put(0, h, ray)
     run.buffers.upload(0, 1, ray.steps if ray is not None else 1)
+    if f64:
+        run.put64(h, scal)
     state = {}
-    st = _lib.SolweigState()
+    st = _lib.SolweigState64() if f64 else _lib.SolweigState()
     for arg, abi in zip(_STATE_ARGS, _STATE_ABI):
-        t = _as_device(args[arg], torch.float32, scene.device, scene.shape).clone()
+        t = _as_device(args[arg], tdt, scene.device, scene.shape).clone()
         state[arg] = t
         setattr(st, abi, t.data_ptr())
-    planes = {name: torch.empty(scene.shape, dtype=torch.float32, device=scene.device) for name in _PLANES}
-    out = _lib.SolweigOutputs()
+    planes = {name: torch.empty(scene.shape, dtype=tdt, device=scene.device) for name in _PLANES}
+    out = _lib.SolweigOutputs64() if f64 else _lib.SolweigOutputs()
     for name, abi in _PLANES.items():
         setattr(out, abi, planes[name].data_ptr())
-    _lib.check(_lib.lib().solweig_step(
-        ctypes.byref(scene.struct), device_ptr(run.layout_dev), run.buffers.ptr(), 0, ctypes.byref(st),
-        ctypes.byref(out), scene.gvf_host_ptr, scene.first_steps, scene.second_steps,
-        device_ptr(run.scratch), stream_handle()), "solweig_step")
+    if f64:
+        _lib.check(_lib.lib().solweig_step64(
+            ctypes.byref(scene.struct), device_ptr(scene.svfbuveg64()), device_ptr(run.layout_dev),
+            device_ptr(scene.layout.device64(scene.device)), run.buffers.ptr(), device_ptr(run.h64_dev), 0,
+            ctypes.byref(st), ctypes.byref(out), scene.gvf_host_ptr, scene.first_steps, scene.second_steps,
+            device_ptr(run.scratch(torch.float64)), stream_handle()), "solweig_step64")
+    else:
+        _lib.check(_lib.lib().solweig_step(
+            ctypes.byref(scene.struct), device_ptr(run.layout_dev), run.buffers.ptr(), 0, ctypes.byref(st),
+            ctypes.byref(out), scene.gvf_host_ptr, scene.first_steps, scene.second_steps,
+            device_ptr(run.scratch(torch.float32)), stream_handle()), "solweig_step")
     run.buffers.mark()
     torch.cuda.current_stream().synchronize()
     if altitude > 0:
@@ -176,7 +204,6 @@ def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, s
     else:
         lay = scene.layout.host
         L_patches = np.column_stack((lay.altitude, lay.azimuth, np.zeros(lay.count)))
-    conv = (lambda t: t) if dt == np.float32 else (lambda t: t.to(torch.float64))
     values = {
         'ea': float(scal.ea), 'esky': float(scal.esky), 'I0': float(scal.I0), 'CI': float(ci_next),
         'firstdaytime': fd_next, 'timestepdec': float(timestepdec), 'timeadd': timeadd_next,
@@ -184,7 +211,7 @@ def Solweig_2022a_calc(i, dsm, scale, rows, cols, svf, svfN, svfW, svfE, svfS, s
         'CI_Tg': float(scal.CI_Tg), 'CI_TgG': float(scal.CI_TgG),
     }
     for name in _PLANES:
-        values[name] = conv(planes[name])
+        values[name] = planes[name]
     for arg in _STATE_ARGS:
-        values[arg] = conv(state[arg])
+        values[arg] = state[arg]
     return tuple(values[n] for n in OUTPUT_NAMES)

@@ -12,7 +12,9 @@ arguments and day grouping (``src/series.py:91-194``).  Differences, by design:
   outputs are copied to pinned host memory on a separate stream while the
   next day computes; a bounded writer thread stores them
   (``src/output.py:11-102``, ``src/runtime.py:79-163``);
-* calendar days can be split over ranks (one process per GPU, no exchange).
+* calendar days can be split over ranks (one process per GPU, no exchange);
+* ``dtype=float64`` (the reference's radiation precision switch) runs every
+  hour through the float64 step (:class:`engine.DayRunner64`) instead.
 """
 from __future__ import annotations
 
@@ -31,7 +33,7 @@ from . import engine, shard
 from .batched import BatchedDay, ChosenDay
 
 __all__ = ["DayForcing", "Meteorology", "load_meteorology", "run_timeseries", "load_raster",
-           "OutputWriter", "rank_and_world"]
+           "OutputWriter", "rank_and_world", "Float64Day"]
 
 
 @dataclass(frozen=True)
@@ -188,7 +190,7 @@ class _HostCopy:
         copy_stream.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(copy_stream):
             for k, v in planes.items():
-                h = torch.empty(v.shape, dtype=torch.float32, pin_memory=True)
+                h = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
                 h.copy_(v, non_blocking=True)
                 self.host[k] = h.numpy()
             self.event = torch.cuda.Event()
@@ -234,6 +236,30 @@ def _make_runner(scene, latitude, longitude, site_altitude, utc, hours, outputs,
     return BatchedDay(scene, latitude, longitude, site_altitude, utc, hours=hours, outputs=outputs)
 
 
+class Float64Day:
+    """Day runner of the float64 switch (``dtype=float64``, ``run.py:27``):
+    every hour through the float64 step (:class:`engine.DayRunner64`), for
+    any day length; the requested planes come back as float64 (UTCI float32)."""
+
+    def __init__(self, scene, latitude, longitude, site_altitude, utc, hours, outputs):
+        self.runner = engine.DayRunner64(scene, latitude, longitude, site_altitude, utc, hours=hours)
+        self.outputs = tuple(outputs)
+
+    def run_day(self, met):
+        return self.runner.run_day(met, self.outputs)
+
+
+def _make_runner64(scene, latitude, longitude, site_altitude, utc, hours, outputs, form):
+    return Float64Day(scene, latitude, longitude, site_altitude, utc, hours, outputs)
+
+
+def _check_dtype(dtype):
+    dt = np.dtype(dtype)
+    if dt not in (np.float32, np.float64):
+        raise NotImplementedError(f"dtype must be float32 or float64 (the reference's choices), not {dt}")
+    return dt == np.float64
+
+
 def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path,
                    longitude, latitude, *, landcover_path=None, utc_offset_hours=None,
                    site_altitude_m=3., wall_method='dsm', building_geometry_path=None,
@@ -244,7 +270,7 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
                    no_write=False, output_core=None, output_chunk_steps=24,
                    async_output=True, output_queue_size=2, output_valid_mask=None, progress=False,
                    pixel_size=1.0, device=None, form="chosen", rank=None, world_size=None,
-                   scene_factory=None, runner_factory=None):
+                   scene_factory=None, runner_factory=None, crs=None, geotransform=None):
     """Simulate every day of the forcing on one tile (``src/series.py:91-156``).
 
     Days run in the batched form (``form="chosen"``, :class:`batched.ChosenDay`)
@@ -253,19 +279,29 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
     runs a contiguous share of the calendar days on its own GPU
     (``LOCAL_RANK``) and writes those days' folders; rank 0 also writes the
     static rasters.  Days are independent (the thermal state resets every
-    day), so ranks exchange nothing.  ``dtype`` must be float32: the float64
-    radiation switch of the reference is not provided.  ``scene_factory`` and
+    day), so ranks exchange nothing.  ``dtype=float64`` runs every hour
+    through the float64 step (:class:`Float64Day`; ``form`` is then not
+    used: the batched forms compute in float32 and BF16).  ``scene_factory`` and
     ``runner_factory`` replace :class:`engine.Scene` and the day runner (for
     tests of the host logic).
+
+    ``wall_method="geometry"`` takes the walls from building footprints
+    (``building_geometry_path``: GeoJSON in EPSG:4326; ``building_height_path``:
+    the GHSL height raster) as ``src/series.py:218-233`` does; the ``.npy``
+    rasters carry no georeferencing, so ``crs`` (the rasters' coordinate
+    system) and ``geotransform`` (GDAL order) must then be given.
 
     Returns ``{"static": {...}, "days": {date: {variable: [paths]}}}`` with the
     days this rank ran.
     """
-    if str(wall_method).strip().lower() != "dsm":
-        raise NotImplementedError("only wall_method='dsm' is supported")
-    if np.dtype(dtype) != np.float32:
-        raise NotImplementedError("only dtype=float32 is supported: the float64 radiation switch of "
-                                  "the reference is not provided by this engine")
+    method = str(wall_method).strip().lower()
+    if method not in ("dsm", "geometry"):
+        raise ValueError(f"wall_method must be 'dsm' or 'geometry', not {wall_method!r}")
+    if method == "geometry" and not (building_geometry_path and building_height_path):
+        raise ValueError("wall_method='geometry' requires building_geometry_path and building_height_path")
+    if method == "geometry" and (crs is None or geotransform is None):
+        raise ValueError("wall_method='geometry' needs the rasters' crs and geotransform (GDAL order)")
+    f64 = _check_dtype(dtype)
     if form not in ("chosen", "batched"):
         raise ValueError(f"form must be 'chosen' or 'batched', not {form!r}")
     rank, world = rank_and_world(rank, world_size)
@@ -295,8 +331,18 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
     if device is None:
         device = _default_device(rank, world)
     make_scene = scene_factory or engine.Scene
+    wall_args = {}
+    if method == "geometry":
+        from . import walls as _walls
+        buildings = _walls.load_buildings(building_geometry_path, crs, default_height_m=default_building_height_m,
+                                          level_height_m=level_height_m,
+                                          minimum_height_m=minimum_building_height_m)
+        ghsl = load_raster(building_height_path).astype(np.float32)
+        w, a = _walls.calculate_geometry_walls(buildings, ghsl, dsm.shape, _walls.affine_from_gdal(geotransform),
+                                               minimum_wall_height_m, device=device)
+        wall_args = dict(walls=w.astype(np.float64), aspect=a.astype(np.float64))
     scene = make_scene(dsm, trees, dem, pixel_size, landcover=lc, wall_threshold=dsm_wall_threshold_m,
-                       device=device, keep_planes=save_svf)
+                       device=device, keep_planes=save_svf, **wall_args)
     files = {"static": {}, "days": {}}
     writer = OutputWriter(enabled=bool(async_output and not no_write), max_inflight=output_queue_size)
     if not no_write and rank == 0:
@@ -314,7 +360,7 @@ def run_timeseries(building_dsm_path, tree_path, dem_path, met_file, output_path
                                             ("Shadow", save_shadow)) if on]
     abi = {"UTCI": "utci", "TMRT": "tmrt", "Kup": "kup", "Kdown": "kdown", "Lup": "lup",
            "Ldown": "ldown", "Shadow": "shadow"}
-    make = runner_factory or _make_runner
+    make = runner_factory or (_make_runner64 if f64 else _make_runner)
     runners = {}
     on_gpu = torch.device(scene.device).type == "cuda"
     copy_stream = torch.cuda.Stream(device=scene.device) if on_gpu and not no_write else None
@@ -374,14 +420,13 @@ def run_tiles(tiles, met_file, output_path, longitude, latitude, *, utc_offset_h
     ranks each takes a contiguous share of the tiles.  Outputs go to
     ``output_path/<tile_id>/<date>/<VAR>.npy`` (cropped to the core) and
     ``output_path/<tile_id>/static``.  Days longer than 64 rows run tile by
-    tile in the per-hour graph form.
+    tile in the per-hour graph form.  ``dtype=float64`` runs every tile-day
+    through the float64 step (:class:`Float64Day`), tile by tile.
 
     Returns ``{tile_id: {"static": {...}, "days": {date: {variable: [paths]}}}}``.
     """
     from .batched import TileBatch
-    if np.dtype(dtype) != np.float32:
-        raise NotImplementedError("only dtype=float32 is supported: the float64 radiation switch of "
-                                  "the reference is not provided by this engine")
+    f64 = _check_dtype(dtype)
     rank, world = rank_and_world(rank, world_size)
     forcing = load_meteorology(met_file)
     mine = shard.split(list(tiles), rank, world)
@@ -424,11 +469,18 @@ def run_tiles(tiles, met_file, output_path, longitude, latitude, *, utc_offset_h
                     np.save(static / "walls.npy", sc.walls_host.astype(np.float32))
                     np.save(static / "aspect.npy", sc.aspect_host.astype(np.float32))
                     rec["static"] = {"walls": str(static / "walls.npy"), "aspect": str(static / "aspect.npy")}
-            batches = {}
+            batches, runners64 = {}, {}
             for day in forcing.days:
                 writer.check()
                 nh = len(day.values)
-                if nh <= 64:
+                if f64:
+                    results = []
+                    for i, sc in enumerate(scenes):
+                        if (i, nh) not in runners64:
+                            runners64[(i, nh)] = Float64Day(sc, float(latitude), float(longitude),
+                                                            float(site_altitude_m), utc, nh, outs)
+                        results.append(runners64[(i, nh)].run_day(day.values))
+                elif nh <= 64:
                     if nh not in batches:
                         batches[nh] = TileBatch(scenes, [float(latitude)] * len(scenes),
                                                 [float(longitude)] * len(scenes), float(site_altitude_m), utc,
@@ -461,7 +513,7 @@ def run_tiles(tiles, met_file, output_path, longitude, latitude, *, utc_offset_h
             torch.cuda.synchronize(torch.device(device))
             for batch in batches.values():  # device error flags of every tile-day
                 batch.check_errors()
-            del batches, scenes
+            del batches, runners64, scenes
         writer.finish()
         return files
     except BaseException:

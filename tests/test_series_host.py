@@ -126,11 +126,29 @@ def test_run_timeseries_masks_cropped_outputs_after_the_copy(tmp_path):
             assert np.array_equal(y[:, mask], x[:, mask])
 
 
-def test_run_timeseries_rejects_bad_mask_and_float64(tmp_path):
+def test_run_timeseries_rejects_bad_mask_and_dtype(tmp_path):
     with pytest.raises(ValueError, match="cropped output"):
         run_stub(tmp_path / "a", output_core=(0, 0, 4, 4), output_valid_mask=np.ones((12, 10), bool))
-    with pytest.raises(NotImplementedError, match="float64"):
-        run_stub(tmp_path / "b", dtype=np.float64)
+    with pytest.raises(NotImplementedError, match="float32 or float64"):
+        run_stub(tmp_path / "b", dtype=np.float16)
+    # the float64 switch is accepted (the stub runner stands in for the float64 step)
+    assert len(run_stub(tmp_path / "c", dtype=np.float64)["days"]) == 4
+
+
+def test_geometry_wall_method_needs_its_inputs(tmp_path):
+    with pytest.raises(ValueError, match="building_geometry_path"):
+        run_stub(tmp_path / "g1", wall_method="geometry")
+    with pytest.raises(ValueError, match="crs and geotransform"):
+        run_stub(tmp_path / "g2", wall_method="geometry", building_geometry_path="b.geojson",
+                 building_height_path="h.npy")
+    with pytest.raises(ValueError, match="wall_method"):
+        run_stub(tmp_path / "g3", wall_method="lidar")
+
+
+def test_float64_switch_selects_the_float64_step():
+    from solweig_cuda_b200 import series
+    assert series._check_dtype(np.float64) and not series._check_dtype("float32")
+    assert series._make_runner64.__code__.co_varnames[:8] == series._make_runner.__code__.co_varnames[:8]
 
 
 def test_run_timeseries_rank_shares_cover_all_days(tmp_path):
