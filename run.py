@@ -123,6 +123,10 @@ def main(argv=None):
     case["met_file"] = forcing
     pixel_size = float(settings.get("resolution_m", 1))
     if "core_area_m" in settings:
+        if str(case.get("wall_method", "dsm")).strip().lower() != "dsm":
+            # the reference's tile jobs crop the DSM, trees, DEM and land cover
+            # but not the building-height raster (run.py:113-129)
+            raise SystemExit("wall_method='geometry' is not supported for tiled cases")
         from solweig_cuda_b200.series import run_tiles
         known = {"longitude", "latitude", "utc_offset_hours", "site_altitude_m", "output_chunk_steps",
                  "async_output", "output_queue_size", "save_tmrt", "save_kup", "save_kdown", "save_lup",

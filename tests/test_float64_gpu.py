@@ -4,9 +4,10 @@ float64 oracle, through ``engine.DayRunner64``, the drop-in
 ``Solweig_2022a_calc(dtype=float64)`` and ``run_timeseries(dtype=float64)``.
 
 Bars (the float32 step is held to Tmrt 0.1 K): shadow bit-exact, Tmrt within
-1e-8 K and every flux plane within 1e-10 relative (of the plane's largest
+1e-10 K and every flux plane within 1e-12 relative (of the plane's largest
 value) of the oracle over a full day, on a scene with water pixels; UTCI
 (float32, from the float32-rounded Tmrt as the reference) within 1e-3 K.
+Measured on a B200: Tmrt 5.7e-14 K, fluxes <= 1.6e-15 relative.
 """
 import numpy as np
 import pytest
@@ -15,8 +16,8 @@ from conftest import small_scene
 
 pytestmark = pytest.mark.gpu
 
-TMRT_TOL = 1e-8
-REL_TOL = 1e-10
+TMRT_TOL = 1e-10
+REL_TOL = 1e-12
 PLANES = {"tmrt": "Tmrt", "kdown": "Kdown", "kup": "Kup", "ldown": "Ldown", "lup": "Lup",
           "shadow": "shadow", "tg": "Tg", "keast": "Keast", "ksouth": "Ksouth", "kwest": "Kwest",
           "knorth": "Knorth", "least": "Least", "lsouth": "Lsouth", "lwest": "Lwest", "lnorth": "Lnorth",
@@ -96,7 +97,7 @@ def test_float64_step_is_closer_to_the_oracle_than_float32(water48):
     e32 = float(np.max(np.abs(t32 - want)))
     print(f"Tmrt error: float64 step {e64:.3e} K, float32 step {e32:.3e} K")
     assert e64 <= TMRT_TOL and e32 <= 0.1
-    assert e64 * 100 <= e32
+    assert e64 * 1e5 <= e32
 
 
 def test_solweig_2022a_calc_float64_equals_the_day_runner(water48):
