@@ -49,9 +49,11 @@ def _args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-month", action="store_true",
                    help="skip the 720 h (30 days in one graph) figure of the headline line")
-    p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient"), default="day",
+    p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient", "float64"),
+                   default="day",
                    help="day: the headline 2000^2 x 24 h line; month: 2000^2 x 720 h in one graph; "
-                        "tiles: 64 uneven tiles in one graph; precision: 4000^2 patch-sum error report")
+                        "tiles: 64 uneven tiles in one graph; precision: 4000^2 patch-sum error report; "
+                        "float64: the float64 radiation switch, hour by hour")
     p.add_argument("--no-tune", dest="tune", action="store_false",
                    help="skip the launch-shape autotuner (cached per shape) of the batched form")
     return p.parse_args()
@@ -306,6 +308,36 @@ def run_month(a):
         "clocks": clocks.summary()}), flush=True)
 
 
+def run_float64(a):
+    """The float64 switch (dtype=float64): 2000^2 px x 24 h through the float64
+    step, hour by hour, beside the float32 per-hour form on the same day."""
+    import torch
+    from solweig_cuda_b200 import engine, synthetic
+    dev = torch.device("cuda", 0)
+    n = a.size
+    sc = synthetic.make_scene(n, seed=0)
+    scene = engine.Scene(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, device=dev)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    r64 = engine.DayRunner64(scene, 53.0, 0.0, 3.0, 0.0)
+    r32 = engine.DayRunner(scene, 53.0, 0.0, 3.0, 0.0)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    with ClockSampler(0) as clocks:
+        ms64 = _events_ms(lambda: r64.run_day(met), a.steps, a.warmup, flush)
+    ms32 = _events_ms(lambda: r32.run_day(met), a.steps, a.warmup, flush)
+    t64 = r64.run_day(met, outputs=("tmrt",))["tmrt"]
+    t32 = r32.run_day(met, outputs=("tmrt",))["tmrt"]
+    diff = float((t64 - t32.double()).abs().max())
+    work = n * n * 24
+    print(json.dumps({
+        "metric": "pixel-hours/s Tmrt+UTCI, 2000^2 px x 24 h, float64 radiation (dtype=float64)",
+        "value": work / (ms64 / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms64, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{n}x{n} px at 1 m, 24 hourly steps (DOY 172, 53N), solweig_step64 per hour",
+                   "float32_per_hour_ms": ms32, "max_abs_tmrt_f64_minus_f32_K": diff,
+                   "kernel_launches_per_day": 3 * 24, "l2": "flushed before every day"},
+        "clocks": clocks.summary()}), flush=True)
+
+
 def _tile_specs(count=64):
     import numpy as np
     rng = np.random.default_rng(2024)
@@ -509,7 +541,7 @@ def main():
             import torch
             torch.cuda.set_device(0)
             {"month": run_month, "tiles": run_tiles, "precision": run_precision,
-             "gradient": run_gradient}[a.workload](a)
+             "gradient": run_gradient, "float64": run_float64}[a.workload](a)
         return 0
     import numpy as np
     import torch
