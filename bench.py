@@ -49,11 +49,12 @@ def _args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-month", action="store_true",
                    help="skip the 720 h (30 days in one graph) figure of the headline line")
-    p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient", "float64"),
+    p.add_argument("--workload", choices=("day", "month", "tiles", "precision", "gradient", "float64",
+                                          "geometry_walls"),
                    default="day",
                    help="day: the headline 2000^2 x 24 h line; month: 2000^2 x 720 h in one graph; "
                         "tiles: 64 uneven tiles in one graph; precision: 4000^2 patch-sum error report; "
-                        "float64: the float64 radiation switch, hour by hour")
+                        "float64: the float64 radiation switch, hour by hour; geometry_walls: footprint walls")
     p.add_argument("--no-tune", dest="tune", action="store_false",
                    help="skip the launch-shape autotuner (cached per shape) of the batched form")
     return p.parse_args()
@@ -329,13 +330,68 @@ def run_float64(a):
     diff = float((t64 - t32.double()).abs().max())
     work = n * n * 24
     print(json.dumps({
-        "metric": "pixel-hours/s Tmrt+UTCI, 2000^2 px x 24 h, float64 radiation (dtype=float64)",
+        "metric": f"pixel-hours/s Tmrt+UTCI, {n}^2 px x 24 h, float64 radiation (dtype=float64)",
         "value": work / (ms64 / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms64, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{n}x{n} px at 1 m, 24 hourly steps (DOY 172, 53N), solweig_step64 per hour",
                    "float32_per_hour_ms": ms32, "max_abs_tmrt_f64_minus_f32_K": diff,
                    "kernel_launches_per_day": 3 * 24, "l2": "flushed before every day"},
         "clocks": clocks.summary()}), flush=True)
+
+
+def run_geometry_walls(a):
+    """The geometry wall method on a 2000^2 px, 1 m raster: 20 000 seeded
+    footprints (rectangles and pentagons, 4-40 m) burned into the wall rasters."""
+    import numpy as np
+    import torch
+    from solweig_cuda_b200 import _lib, walls
+    from solweig_cuda_b200.engine import device_ptr
+    n = a.size
+    rng = np.random.default_rng(7)
+    buildings = []
+    for k in range(20000):
+        x, y = rng.uniform(0, n - 40, 2)
+        w, h = rng.uniform(4, 40, 2)
+        ring = [[x, y], [x + w, y], [x + w, y + h], [x + w / 2, y + 1.3 * h], [x, y + h], [x, y]]
+        if k % 2:
+            ring = [ring[0], ring[1], ring[2], ring[4], ring[5]]
+        buildings.append(({"type": "Polygon", "coordinates": [ring]}, float(rng.uniform(3, 30))))
+    ghsl = np.where(rng.random((n, n)) < 0.3, rng.uniform(0, 30, (n, n)), 0).astype(np.float32)
+    transform = (1.0, 0.0, 0.0, 0.0, -1.0, float(n))
+    t0 = time.perf_counter()
+    w_host, _ = walls.calculate_geometry_walls(buildings, ghsl, (n, n), transform, 2.0)
+    call_s = time.perf_counter() - t0
+    # the two device kernels alone, on the segments of that call
+    seg = []
+    for g, h in buildings:
+        hh, aa = walls.wall_segments(g, h)
+        seg += [list(s[0]) + list(s[1]) for s, _ in hh]
+    seg = np.asarray(seg, dtype=np.float64)
+    pix = np.column_stack([seg[:, 0], n - seg[:, 1], seg[:, 2], n - seg[:, 3]])
+    dev = torch.device("cuda", 0)
+    t_seg = torch.from_numpy(np.ascontiguousarray(pix)).to(dev)
+    t_h = torch.ones(len(pix), dtype=torch.float64, device=dev)
+    t_g = torch.from_numpy(ghsl).to(dev)
+    owner = torch.empty((n, n), dtype=torch.int32, device=dev)
+    out_w = torch.empty((n, n), dtype=torch.float32, device=dev)
+    out_a = torch.empty((n, n), dtype=torch.float32, device=dev)
+    L = _lib.lib()
+
+    def kernels():
+        _lib.check(L.solweig_wall_segments_burn(device_ptr(t_seg), len(pix), n, n, device_ptr(owner), None), "burn")
+        _lib.check(L.solweig_geometry_walls(device_ptr(owner), device_ptr(t_h), device_ptr(t_h), device_ptr(t_g),
+                                            n * n, 2.0, device_ptr(out_w), device_ptr(out_a), None), "merge")
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    ms = _events_ms(kernels, a.steps, a.warmup, flush)
+    print(json.dumps({
+        "metric": f"raster pixels/s, geometry wall method (footprint edges burned, GHSL merge), {n}^2 px",
+        "value": n * n / (ms / 1000.0), "unit": "pixels/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": f"{n}x{n} px at 1 m, 20000 footprints (seed 7), {len(pix)} edges",
+                   "kernels": ["segment_burn_kernel", "geometry_walls_kernel"], "gpu_launches_per_step": 2,
+                   "calculate_geometry_walls_s": call_s, "wall_pixels": int((w_host > 0).sum()),
+                   "l2": "flushed before every step"}}), flush=True)
 
 
 def _tile_specs(count=64):
@@ -541,7 +597,8 @@ def main():
             import torch
             torch.cuda.set_device(0)
             {"month": run_month, "tiles": run_tiles, "precision": run_precision,
-             "gradient": run_gradient, "float64": run_float64}[a.workload](a)
+             "gradient": run_gradient, "float64": run_float64,
+             "geometry_walls": run_geometry_walls}[a.workload](a)
         return 0
     import numpy as np
     import torch
