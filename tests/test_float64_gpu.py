@@ -166,3 +166,28 @@ def test_run_timeseries_float64_writes_the_float64_step(water48, tmp_path):
     assert np.array_equal(tm, ref["tmrt"].cpu().numpy().astype(np.float32))
     u = ref["utci"].cpu().numpy()
     assert np.array_equal(np.isnan(ut), np.isnan(u)) and np.array_equal(ut[~np.isnan(u)], u[~np.isnan(u)])
+
+
+def test_run_tiles_float64_equals_run_timeseries_per_tile(cuda, tmp_path):
+    """run_tiles(dtype=float64) writes, for each tile, what run_timeseries
+    (dtype=float64) writes for that tile's window cropped to its core."""
+    from solweig_cuda_b200 import series, synthetic, tiling
+    sc = small_scene(40, seed=6)
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0, seed=2)
+    jobs = []
+    for t in tiling.tile_windows(40, 40, core=24, halo=6):
+        jobs.append({"tile_id": t["tile_id"], "output_core": t["output_core"],
+                     **{k: np.ascontiguousarray(tiling.extract(v, t))
+                        for k, v in (("dsm", sc.dsm), ("trees", sc.trees), ("dem", sc.dem),
+                                     ("landcover", sc.landcover))}})
+    got = series.run_tiles(jobs, met, tmp_path / "tiles", 0.0, 53.0, utc_offset_hours=0.0, dtype=np.float64)
+    for j in jobs:
+        ref = series.run_timeseries(j["dsm"], j["trees"], j["dem"], met, tmp_path / "single" / j["tile_id"],
+                                    0.0, 53.0, landcover_path=j["landcover"], utc_offset_hours=0.0,
+                                    output_core=j["output_core"], dtype=np.float64)
+        (date,) = ref["days"]
+        for var in ("UTCI", "TMRT"):
+            a = np.load(got[j["tile_id"]]["days"][date][var][0])
+            b = np.load(ref["days"][date][var][0])
+            assert a.shape == (24,) + tuple(j["output_core"][2:])
+            assert np.array_equal(a.view(np.int32), b.view(np.int32)), (j["tile_id"], var)
