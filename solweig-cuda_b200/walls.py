@@ -128,7 +128,8 @@ def _polygons(geometry):
     for poly in polys:
         rings = []
         for ring in poly:
-            r = np.asarray(ring, dtype=np.float64).reshape(-1, np.shape(ring)[-1] if len(ring) else 2)[:, :2]
+            r = np.asarray(ring, dtype=np.float64)
+            r = r[:, :2] if r.ndim == 2 else np.zeros((0, 2))  # drop any z coordinate
             if len(r) and not np.array_equal(r[0], r[-1]):
                 r = np.vstack([r, r[:1]])  # close the ring as shapely does
             rings.append(r)
