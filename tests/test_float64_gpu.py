@@ -191,3 +191,33 @@ def test_run_tiles_float64_equals_run_timeseries_per_tile(cuda, tmp_path):
             b = np.load(ref["days"][date][var][0])
             assert a.shape == (24,) + tuple(j["output_core"][2:])
             assert np.array_equal(a.view(np.int32), b.view(np.int32)), (j["tile_id"], var)
+
+
+def test_float64_day_matches_umep_itself(cuda):
+    """The float64 step against UMEP's own Solweig_2022a_calc over a day
+    (tests/golden/day.npz: the reference's numpy path imported in place, on the
+    statics of tests/golden/svf.npz and the golden walls), at the bar the
+    oracle itself is pinned to (1e-9)."""
+    import os
+    from oracle import step as ST
+    from solweig_cuda_b200 import engine, synthetic
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    g = np.load(os.path.join(gold, "day.npz"))
+    sv = np.load(os.path.join(gold, "svf.npz"))
+    P = int(sv["patches"])
+    cubes = [np.unpackbits(sv[k], axis=2)[:, :, :P].astype(np.float64) for k in ("shmat", "vegmat", "vbmat")]
+    order = (0, 10, 1, 11, 6, 4, 14, 9, 2, 12, 7, 5, 3, 13, 8)
+    planes = sv["planes"]
+    svf = tuple(planes[i] for i in order) + (cubes[1], cubes[2], cubes[0], planes[15])
+    sc = synthetic.make_scene(32, seed=6)
+    s = ST.prepare_static(sc.dsm, sc.trees, sc.dem, 1.0, landcover=sc.landcover, walls=g["walls"],
+                          aspect=g["aspect"], svf=svf)
+    scene = engine.Scene.from_inputs(dict(s, **CONSTANTS))
+    names = {"tmrt": "Tmrt", "kdown": "Kdown", "kup": "Kup", "ldown": "Ldown", "lup": "Lup", "kside": "Kside",
+             "lside": "Lside", "shadow": "shadow"}
+    got = engine.DayRunner64(scene, 53.0, 0.0, 3.0, 0.0).run_day(g["met"], outputs=tuple(names))
+    worst = 0.0
+    for k, name in names.items():
+        worst = max(worst, float(np.max(np.abs(got[k].cpu().numpy() - g[name]))))
+    print(f"float64 step vs UMEP day: worst absolute difference {worst:.3e}")
+    assert worst < 1e-9
