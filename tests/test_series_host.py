@@ -196,3 +196,25 @@ def test_run_timeseries_raises_when_a_day_left_invalid_results(tmp_path):
     with pytest.raises(batched.DayError):
         series.run_timeseries(z, z, z, _forcing(2), tmp_path, 0.0, 53.0, scene_factory=StubScene,
                               runner_factory=FlaggedRunner, device="cpu")
+
+
+def test_cli_refuses_geometry_walls_for_tiled_cases(tmp_path):
+    """run.py: a tiled case with wall_method=geometry stops before any device
+    work (the reference's tile jobs do not crop the building-height raster)."""
+    import importlib.util
+    import json
+    from solweig_cuda_b200 import synthetic
+    met = synthetic.make_met(doy=172, latitude=53.0, longitude=0.0)
+    header = "iy id it imin Q* QH QE Qs Qf Wind RH Td press rain Kdn snow ldown fcld wuh xsmd lai_hr Kdiff Kdir Wd"
+    np.savetxt(tmp_path / "met.txt", met, header=header, comments="", fmt="%.6f")
+    case = {"case_name": "t", "building_dsm_path": "dsm.npy", "tree_path": "trees.npy", "dem_path": "dem.npy",
+            "met_file": "met.txt", "output_path": "out", "longitude": 0.0, "latitude": 53.0,
+            "core_area_m": 20, "buffer_area_m": 6, "wall_method": "geometry",
+            "building_geometry_path": "b.geojson", "building_height_path": "h.npy"}
+    (tmp_path / "case.json").write_text(json.dumps(case))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("solweig_run_cli", os.path.join(root, "run.py"))
+    cli = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cli)
+    with pytest.raises(SystemExit, match="geometry"):
+        cli.main(["--case", str(tmp_path / "case.json"), "--no-progress"])
