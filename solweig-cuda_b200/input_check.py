@@ -221,6 +221,20 @@ def check_options(case, *, dtype=np.float32, output_path=None, no_write=False):
         raise ValueError("wall_method must be dsm or geometry")
     if method == "geometry" and not all(case.get(k) for k in ("building_geometry_path", "building_height_path")):
         raise ValueError("wall_method=geometry requires building_geometry_path and building_height_path")
+    # georeferencing of .npy rasters (no counterpart in the reference: a GeoTIFF carries it)
+    gt = case.get("geotransform")
+    if gt is not None:
+        if (not isinstance(gt, (list, tuple)) or len(gt) != 6
+                or not all(_is_real(v) and math.isfinite(v) for v in gt)):
+            raise ValueError("geotransform must be six finite numbers (GDAL order)")
+        if gt[1] * gt[5] - gt[2] * gt[4] == 0:
+            raise ValueError("geotransform must be invertible")
+    if case.get("crs") is not None:
+        from . import crs as _crs
+        try:
+            _crs.project_lonlat([0.0], [0.0], case["crs"])
+        except NotImplementedError as exc:
+            raise ValueError(f"crs: {exc}") from None
     check_output_window(case.get("output_core"), None)
     if output_path is not None and not no_write:
         out = Path(output_path).resolve()

@@ -104,11 +104,20 @@ def test_preparation_defaults():
     ({"wall_method": "lidar"}, "dsm or geometry"),
     ({"wall_method": "geometry"}, "requires building_geometry_path"),
     ({"output_core": [0, 0, 0, 5]}, "output_core"),
+    ({"geotransform": [0, 1, 0, 0, 0]}, "six finite numbers"),
+    ({"geotransform": [0, 1, 0, 0, 0, float("nan")]}, "six finite numbers"),
+    ({"geotransform": [0, 1, 0, 0, 0, 0]}, "invertible"),
+    ({"crs": "EPSG:2154"}, "crs"),
 ])
 def test_run_options_rejected(case, message):
     from solweig_cuda_b200 import input_check
     with pytest.raises(ValueError, match=message):
         input_check.check_options(case)
+
+
+def test_georeferencing_options_accepted():
+    from solweig_cuda_b200 import input_check
+    input_check.check_options({"geotransform": [500000.0, 1.0, 0.0, 5760048.0, 0.0, -1.0], "crs": "EPSG:32633"})
 
 
 def test_output_window_and_mask():
